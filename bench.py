@@ -1,0 +1,400 @@
+"""Benchmark: vertex-steps/s of the deformable-ring hot path on B200.
+
+Workload (default): 1024 rings, nv 32/45 bidisperse 1:1.4 (39,424 vertices),
+smooth vertex-segment Lennard-Jones (rc 2.5 sigma, epsilon 1), calA0 1.05,
+packing fraction 0.85, ka=kl=1, kb=0.01, NVE velocity Verlet at dt 0.002 with
+ring velocities drawn at T 0.01, FP64.  Inputs are synthetic and seeded: rings
+placed without overlap at phi 0.40, compressed to 0.85 with FIRE
+(cudaring_b200.workloads), then thermalised; none of that is timed.
+
+One bench step = ``--md-steps`` NVE steps (default 1000) through one
+``DPM2D.NVELoop`` call, neighbour-list rebuilds included as they fall due.
+``value`` = vertices x MD steps x bench steps / device time (max over ranks);
+``e2e`` adds, every bench step, the upload of positions and velocities from
+pinned host memory and the download of positions, velocities and the
+potential energy through the public API.
+
+Multi-GPU: one independent replica per rank (weak scaling, no collective on
+the data path); rank 0 prints the line.  ``--impl reference`` times the
+reference's own kernels compiled as host code (oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "vertex-steps/s at 1 B200: mixed vs plain FP64 at <=1e-6 force err; HBM GB/s frac"
+UNIT = "vertex-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--md-steps", type=int, default=1000)
+    ap.add_argument("--rings", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def committed_traffic() -> dict | None:
+    path = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_reference_rate(d, threads: int, target_seconds: float = 12.0, rebuild_every: float | None = None) -> dict:
+    """Reference kernels compiled as host code (oracle/_ref): one neighbour build
+    plus NVE steps on the same prepared state; vertex-steps/s with the build
+    amortised over the rebuild interval measured on the GPU run."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    import oracle
+
+    kind = "reference" if oracle.ref_available() else "port"
+    if kind != "reference":
+        return {"value": None, "unit": UNIT, "cores": threads, "kind": "port",
+                "sample": "oracle/_ref not built; CPU baseline skipped"}
+    R = oracle.ref()
+    pos, vel = d.getVertexPositions(), d.getVertexVelocities()
+    rad, l0, a0 = d.getVertexRadii(), d.getRestLengths(), d.getRestAreas()
+    th0 = np.full(d.numVertices, 0.0)
+    nvl = d.numVertexInParticleList
+    th0 = np.repeat(2 * np.pi / nvl, nvl).astype(np.float64)
+    box = d.getBoxSize()
+    R.ref_create(len(nvl), nvl)
+    R.ref_set_box(float(box[0]), float(box[1]))
+    R.ref_set_types(1, 1, 0, 0)
+    R.ref_set_energy_costs(1.0, 1.0, 0.01, 1.0)
+    R.ref_set_lj_cutoff(2.5)
+    R.ref_set_time_step(0.002)
+    R.ref_set_state(pos.ctypes.data, vel.ctypes.data, rad.ctypes.data, l0.ctypes.data, th0.ctypes.data,
+                    a0.ctypes.data)
+    cut = R.ref_set_displacement_cutoff(0.5, 2 * rad.mean())
+    t0 = time.perf_counter()
+    R.ref_calc_neighbor_list(cut)
+    t_build = time.perf_counter() - t0
+    R.ref_reset_last_positions()
+    R.ref_calc_force_energy()
+    n = 5
+    t0 = time.perf_counter()
+    R.ref_nve_loop(n)
+    t_probe = (time.perf_counter() - t0) / n
+    nsteps = max(5, int(max(1.0, target_seconds - t_build) / max(t_probe, 1e-6)))
+    nsteps = min(nsteps, 2000)
+    upd0 = R.ref_update_count()
+    t0 = time.perf_counter()
+    R.ref_nve_loop(nsteps)
+    t_steps = time.perf_counter() - t0
+    upd = R.ref_update_count() - upd0
+    per_step = t_steps / nsteps  # includes any rebuild that fell due in the sample
+    if upd == 0 and rebuild_every:
+        per_step += t_build / rebuild_every
+    rate = d.numVertices / per_step
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": (f"{nsteps} NVE steps of the same {d.numVertices}-vertex state on {threads} threads "
+                       f"({t_steps:.1f} s, {upd} rebuilds in sample; one O(Nv^2) list build {t_build:.1f} s"
+                       + (f", amortised over the GPU run's {rebuild_every:.0f} steps per rebuild" if upd == 0
+                          and rebuild_every else "") + ")")}
+
+
+# ------------------------------------------------------------------- main
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        return run_reference_arm(args, world, rank)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from cudaring_b200 import workloads
+
+    t_prep = time.perf_counter()
+    d, info = workloads.prepared_deformable(1, args.rings, seed=20261203 + rank)
+    nv, npr = d.numVertices, d.numParticles
+    c = info["config"]
+    d.setTimeStep(c["dt"])
+    d.setSeed(1000 + rank)
+    d.initNVE(c["T"], readState=False)
+    t_prep = time.perf_counter() - t_prep
+
+    import ctypes
+
+    sp = ctypes.c_void_p()
+    d._call("cr_get_stream", ctypes.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    M = args.md_steps
+
+    def l2_flush():
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+
+    # warm-up (also compiles and caches the CUDA graphs)
+    for _ in range(args.warmup):
+        d.NVELoop(M)
+        l2_flush()
+    torch.cuda.synchronize()
+    upd0 = d.getUpdateCount()
+    launches0 = d.getLaunchCount()
+    e0 = d.getEnergy()
+
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            d.NVELoop(M)
+            l2_flush()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms_total = max_over_ranks(ev0.elapsed_time(ev1), world)
+    launches = d.getLaunchCount() - launches0
+    updates = d.getUpdateCount() - upd0
+    e1 = d.getEnergy()
+    vertex_steps = nv * M * args.steps * world
+    value = vertex_steps / (ms_total / 1e3)
+
+    # e2e through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        hpos = torch.empty(2 * nv, dtype=torch.float64, pin_memory=True).numpy()
+        hvel = torch.empty(2 * nv, dtype=torch.float64, pin_memory=True).numpy()
+        hpos[:] = d.getVertexPositions()
+        hvel[:] = d.getVertexVelocities()
+        n_e2e = max(1, min(args.steps, 5))
+        barrier(world)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ea.record(stream)
+        for _ in range(n_e2e):
+            d.setVertexPositions(hpos)
+            d.setVertexVelocities(hvel)
+            d.NVELoop(M)
+            hpos[:] = d.getVertexPositions()
+            hvel[:] = d.getVertexVelocities()
+            _ = d.getPotentialEnergy()
+        eb.record(stream)
+        torch.cuda.synchronize()
+        ms_e2e = max_over_ranks(ea.elapsed_time(eb), world)
+        e2e = {"value": nv * M * n_e2e * world / (ms_e2e / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": 2 * 16 * nv, "d2h_bytes_per_step": 2 * 16 * nv + 8}
+
+    # roofline of the dominant kernel: the fused force + NVE step kernel
+    ms_launch = ctypes.c_double()
+    d._call("cr_profile_step_kernel", 200, ctypes.byref(ms_launch))
+    bytes_per_launch = 88 * nv + 8 * npr
+    achieved = bytes_per_launch / (ms_launch.value * 1e-3) / 1e9
+    peaks = measured_peaks()
+    traffic = committed_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                "traffic": traffic.get("bytes_per_launch") if traffic else None,
+                "kernel": "k_tile<LJ, smooth, step>", "ms_per_launch": ms_launch.value,
+                "algorithmic_bytes_per_launch": bytes_per_launch}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        steps_per_rebuild = (M * args.steps / updates) if updates else None
+        cpu = cpu_reference_rate(d, os.cpu_count() or 1, rebuild_every=steps_per_rebuild)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded rings placed at phi 0.40, FIRE-compressed to 0.85, T=0.01 velocities",
+            "config": {"workload": f"{npr} deformable rings nv 32/45 (1:1.4), {nv} vertices, smooth vertex-segment "
+                                   f"LJ rc 2.5, calA0 1.05, phi 0.85, NVE dt 0.002, FP64",
+                       "rings": npr, "vertices": nv, "md_steps_per_bench_step": M,
+                       "l2": "flushed between bench steps (256 MB write)", "parallelism": f"replicas x{world}",
+                       "neighbour_rebuilds_in_timed_region": updates,
+                       "energy_drift_rel": abs(e1 - e0) / abs(e0) if e0 else None,
+                       "prep_seconds": t_prep, "fire_iterations_prep": info["fire_iterations"]},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    d.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    import oracle
+
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libcrref.so was not built "
+                                                              "(needs the reference checkout at build time)"}))
+        return
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    # same prepared state, built on the GPU when one is present, else on the CPU port
+    from cudaring_b200 import workloads
+
+    d, info = workloads.prepared_deformable(1, args.rings, seed=20261203)
+    c = info["config"]
+    R = oracle.ref()
+    nvl = d.numVertexInParticleList
+    pos, rad, l0, a0 = d.getVertexPositions(), d.getVertexRadii(), d.getRestLengths(), d.getRestAreas()
+    rng = np.random.default_rng(1000)
+    vel = np.repeat(rng.normal(0.0, np.sqrt(c["T"]), size=(len(nvl), 2)), nvl, axis=0).reshape(-1)
+    th0 = np.repeat(2 * np.pi / nvl, nvl).astype(np.float64)
+    box = d.getBoxSize()
+    R.ref_create(len(nvl), nvl)
+    R.ref_set_box(float(box[0]), float(box[1]))
+    R.ref_set_types(1, 1, 0, 0)
+    R.ref_set_energy_costs(1.0, 1.0, 0.01, 1.0)
+    R.ref_set_lj_cutoff(2.5)
+    R.ref_set_time_step(c["dt"])
+    R.ref_set_state(pos.ctypes.data, vel.ctypes.data, rad.ctypes.data, l0.ctypes.data, th0.ctypes.data, a0.ctypes.data)
+    cut = R.ref_set_displacement_cutoff(0.5, 2 * rad.mean())
+    t0 = time.perf_counter()
+    R.ref_calc_neighbor_list(cut)
+    t_build = time.perf_counter() - t0
+    R.ref_reset_last_positions()
+    R.ref_calc_force_energy()
+    per = 20  # NVE steps per reference bench step
+    for _ in range(max(0, min(args.warmup, 1))):
+        R.ref_nve_loop(per)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        R.ref_nve_loop(per)
+    t = time.perf_counter() - t0
+    upd = R.ref_update_count()
+    value = d.numVertices * per * args.steps / t
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (same prepared state as the ours arm)",
+            "config": {"workload": f"{d.numParticles} deformable rings, {d.numVertices} vertices, smooth LJ, phi 0.85,"
+                                   f" NVE dt 0.002", "md_steps_per_bench_step": per,
+                       "rebuilds_in_sample": upd, "list_build_seconds": t_build},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{per * args.steps} NVE steps, reference kernels as host code, "
+                                       f"{threads} OpenMP threads"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    d.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,1386 @@
+// Context, op sequencer (CUDA graphs with conditional rebuild nodes) and the
+// C ABI declared in include/cudaring.h.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "cr_launch.h"
+#include "cr_tile.cuh"
+
+using namespace cr;
+
+#define CR_TRY(expr)                                                                     \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) return ctx->fail(CR_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+namespace {
+
+enum OpType { OP_DRIFT = 0, OP_TILE = 1, OP_FIRE_PRE = 2, OP_CHECK = 3 };
+
+struct Op {
+  int type;
+  int in_buf;     // position buffer read
+  int out_buf;    // position buffer written (drift/advance), or in_buf
+  int advance;    // tile: 1 = write next positions, 0 = final (store v, F)
+  int check_after;  // a rebuild conditional follows this op
+  int check_buf;    // buffer whose positions the rebuild would use
+};
+
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+  cudaGraph_t graph = nullptr;
+};
+
+long long pow2ceil(long long x) {
+  long long p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+}  // namespace
+
+struct cr_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // capture stream for conditional bodies
+  std::string err;
+  long long launches = 0;
+
+  int np = 0, nv = 0;
+  std::vector<int> ring_first_h, ring_nv_h, ring_of_h;
+  std::vector<int4> tiles_h;
+  int lanes = 2;
+
+  SysParams p{};
+  int potential = 0, interaction = 0, monomer = 0, particle = 0, noise_type = 0, shape = 0, geometry = 0;
+  double dt = 1e-3, driving = 0.0, taup = 0.0;
+  unsigned long long seed = 0x5EEDC0DEULL;
+  unsigned long long rng_calls = 0;
+  double cutoff = 0.0, cut_distance = 1.0;
+  long long list_size_ref = 0;
+  double rmax = 0.0;
+
+  // device state
+  double2* pos[2] = {nullptr, nullptr};
+  int cur = 0;
+  double2 *vel = nullptr, *force = nullptr, *last_pos = nullptr, *ppos = nullptr;
+  double *rad = nullptr, *l0 = nullptr, *theta0 = nullptr, *a0 = nullptr;
+  double *energy = nullptr, *p_energy = nullptr, *theta = nullptr, *length = nullptr, *area = nullptr,
+         *perimeter = nullptr, *p_angle = nullptr, *vertex_area = nullptr;
+  int *ring_of = nullptr, *ring_first = nullptr, *ring_nv = nullptr, *zero_cnt = nullptr;
+  int2* pp_of = nullptr;
+  int4* tiles = nullptr;
+  int* nbr = nullptr;
+  int* nbr_cnt = nullptr;
+  int cap = 0;
+  bool nbr_built = false;
+  // cell scratch
+  CellGrid grid{0, 0, 0.0, 0.0};
+  int ncells_alloc = 0;
+  int *cell_of = nullptr, *slot = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_vid = nullptr,
+      *cell_ring = nullptr;
+  double2* cell_pos = nullptr;
+  double* cell_rad = nullptr;
+  double* partials = nullptr;
+  int partials_n = 0;
+  DevStatus* status = nullptr;
+  DevStatus* status_h = nullptr;  // pinned
+  double* fire_state = nullptr;   // [2][4]
+
+  // integrators
+  int sim_kind = -1;  // Kind
+  double T = 0.0, gamma = 1.0, noise = 0.0, gamma_factor = 1.0;
+  bool fire_ready = false;
+  FireParams fp{};
+  bool use_graphs = true;
+
+  std::map<std::tuple<int, long, int, int, unsigned long long>, GraphEntry> graphs;
+
+  int fail(int code, const std::string& msg) {
+    err = msg;
+    return code;
+  }
+};
+
+namespace {
+
+template <typename T>
+int dalloc(cr_ctx* ctx, T** p, size_t n) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) return ctx->fail(CR_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  e = cudaMemset(*p, 0, n * sizeof(T));
+  if (e != cudaSuccess) return ctx->fail(CR_ECUDA, std::string("cudaMemset: ") + cudaGetErrorString(e));
+  return CR_OK;
+}
+
+void drop_graphs(cr_ctx* ctx) {
+  for (auto& kv : ctx->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->graphs.clear();
+}
+
+void refresh_params(cr_ctx* ctx) {
+  SysParams& p = ctx->p;
+  p.nv = ctx->nv;
+  p.np = ctx->np;
+  p.inv_lx = 1.0 / p.lx;
+  p.inv_ly = 1.0 / p.ly;
+  p.monomer = ctx->monomer;
+  p.potential = ctx->potential;
+}
+
+SysArrays arrays(cr_ctx* ctx, int buf, bool zero_list = false) {
+  SysArrays a;
+  a.pos = ctx->pos[buf];
+  a.rad = ctx->rad;
+  a.l0 = ctx->l0;
+  a.theta0 = ctx->theta0;
+  a.a0 = ctx->a0;
+  a.ring_of = ctx->ring_of;
+  a.ring_first = ctx->ring_first;
+  a.ring_nv = ctx->ring_nv;
+  a.pp_of = ctx->pp_of;
+  a.nbr = ctx->nbr;
+  a.nbr_cnt = (zero_list || !ctx->nbr_built) ? ctx->zero_cnt : ctx->nbr_cnt;
+  a.tiles = ctx->tiles;
+  a.nbr_cap = ctx->cap;
+  return a;
+}
+
+StepArgs base_args(cr_ctx* ctx) {
+  StepArgs s;
+  memset(&s, 0, sizeof(s));
+  s.vel = ctx->vel;
+  s.force = ctx->force;
+  s.last_pos = ctx->last_pos;
+  s.energy = ctx->energy;
+  s.p_energy = ctx->p_energy;
+  s.theta_out = ctx->theta;
+  s.length_out = ctx->length;
+  s.area_out = ctx->area;
+  s.perim_out = ctx->perimeter;
+  s.ppos_out = ctx->ppos;
+  s.p_angle = ctx->p_angle;
+  s.partials = ctx->partials;
+  s.status = ctx->status;
+  s.fire_state = ctx->fire_state;
+  s.dt = ctx->dt;
+  s.hdt = 0.5 * ctx->dt;
+  s.gamma = ctx->gamma;
+  s.noise = ctx->noise;
+  s.gamma_factor = ctx->gamma_factor;
+  s.driving = ctx->driving;
+  s.sp_amp = ctx->taup != 0.0 ? std::sqrt(2.0 * ctx->dt / ctx->taup) : 0.0;
+  s.active = ctx->particle == CR_PARTICLE_ACTIVE;
+  s.disp_cutoff = ctx->cutoff;
+  s.seed = ctx->seed;
+  s.fire_tol = -1.0;
+  return s;
+}
+
+int inter_kind(cr_ctx* ctx) {
+  return (ctx->interaction == CR_INTERACTION_VERTEX_VERTEX || ctx->interaction == CR_INTERACTION_ALL) ? INT_VV
+                                                                                                      : INT_SMOOTH;
+}
+
+LaunchCfg tile_cfg(cr_ctx* ctx) { return LaunchCfg{ctx->stream, (int)ctx->tiles_h.size(), ctx->lanes}; }
+
+int ensure_partials(cr_ctx* ctx) {
+  int need = std::max<int>((int)ctx->tiles_h.size(), 2048) * NSUM;
+  if (ctx->partials_n >= need) return CR_OK;
+  ctx->partials_n = need;
+  return dalloc(ctx, &ctx->partials, need);
+}
+
+// Cell grid for the current box, radii and cutDistance (see cr_nbr.cu).
+int setup_grid(cr_ctx* ctx, double cut) {
+  const double cmin = (1.0 + cut) * 2.0 * ctx->rmax * (1.0 + 1e-9);
+  int ncx = cmin > 0 ? (int)std::floor(ctx->p.lx / cmin) : 0;
+  int ncy = cmin > 0 ? (int)std::floor(ctx->p.ly / cmin) : 0;
+  ncx = std::min(ncx, 4096);
+  ncy = std::min(ncy, 4096);
+  if (ncx < 3 || ncy < 3) {
+    ctx->grid = CellGrid{0, 0, 0.0, 0.0};
+    return CR_OK;
+  }
+  ctx->grid = CellGrid{ncx, ncy, ctx->p.lx / ncx, ctx->p.ly / ncy};
+  const int ncells = ncx * ncy;
+  if (ncells > ctx->ncells_alloc) {
+    drop_graphs(ctx);
+    int rc;
+    if ((rc = dalloc(ctx, &ctx->cell_cnt, ncells))) return rc;
+    if ((rc = dalloc(ctx, &ctx->cell_start, ncells + 1))) return rc;
+    ctx->ncells_alloc = ncells;
+  }
+  return CR_OK;
+}
+
+NbrArgs nbr_args(cr_ctx* ctx, int buf, double cut) {
+  NbrArgs n;
+  n.pos = ctx->pos[buf];
+  n.rad = ctx->rad;
+  n.ring_of = ctx->ring_of;
+  n.nbr = ctx->nbr;
+  n.nbr_cnt = ctx->nbr_cnt;
+  n.cap = ctx->cap;
+  n.cut_distance = cut;
+  n.last_pos = ctx->last_pos;
+  n.cell_of = ctx->cell_of;
+  n.slot = ctx->slot;
+  n.cell_cnt = ctx->cell_cnt;
+  n.cell_start = ctx->cell_start;
+  n.cell_vid = ctx->cell_vid;
+  n.cell_pos = ctx->cell_pos;
+  n.cell_rad = ctx->cell_rad;
+  n.cell_ring = ctx->cell_ring;
+  n.status = ctx->status;
+  n.count_op = 0;
+  return n;
+}
+
+int read_status(cr_ctx* ctx) {
+  CR_TRY(cudaMemcpyAsync(ctx->status_h, ctx->status, sizeof(DevStatus), cudaMemcpyDeviceToHost, ctx->stream));
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+int clear_flags(cr_ctx* ctx) {
+  // abort, overflow, rebuild, converged, nonfinite <- 0 (counters kept)
+  int rc = read_status(ctx);
+  if (rc) return rc;
+  DevStatus s = *ctx->status_h;
+  s.abort = 0;
+  s.overflow = 0;
+  s.rebuild = 0;
+  s.converged = 0;
+  s.nonfinite = 0;
+  s.done_ctr = 0;
+  *ctx->status_h = s;
+  CR_TRY(cudaMemcpyAsync(ctx->status, ctx->status_h, sizeof(DevStatus), cudaMemcpyHostToDevice, ctx->stream));
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+// Build the list from positions buffer `buf`; grows capacity like the
+// reference (two passes when the first overflowed).
+int build_list(cr_ctx* ctx, int buf, double cut) {
+  int rc;
+  if ((rc = setup_grid(ctx, cut))) return rc;
+  for (int pass = 0; pass < 3; pass++) {
+    launch_nbr_build(ctx->stream, ctx->p, ctx->grid, nbr_args(ctx, buf, cut));
+    ctx->launches += (ctx->grid.ncx ? 6 : 2);
+    CR_TRY(cudaGetLastError());
+    if ((rc = read_status(ctx))) return rc;
+    const int mc = ctx->status_h->max_count;
+    if (!ctx->status_h->overflow) {
+      ctx->list_size_ref = std::max<long long>(ctx->list_size_ref, mc > 0 ? pow2ceil(mc) : 0);
+      ctx->nbr_built = true;
+      if (mc * 2 > ctx->cap) {
+        // keep headroom for rebuilds inside step sequences
+        int newcap = (int)std::max<long long>(16, pow2ceil(2LL * mc));
+        if ((rc = dalloc(ctx, &ctx->nbr, (size_t)newcap * ctx->nv))) return rc;
+        ctx->cap = newcap;
+        drop_graphs(ctx);
+        if ((rc = clear_flags(ctx))) return rc;
+        continue;  // rebuild into the larger list
+      }
+      return CR_OK;
+    }
+    int newcap = (int)std::max<long long>(16, pow2ceil(2LL * mc));
+    if ((rc = dalloc(ctx, &ctx->nbr, (size_t)newcap * ctx->nv))) return rc;
+    ctx->cap = newcap;
+    drop_graphs(ctx);
+    if ((rc = clear_flags(ctx))) return rc;
+  }
+  return ctx->fail(CR_ENBR_OVERFLOW, "neighbour list did not fit after growing");
+}
+
+void update_rmax(cr_ctx* ctx, const double* rad_h) {
+  double m = 0.0;
+  for (int i = 0; i < ctx->nv; i++) m = std::max(m, rad_h[i]);
+  ctx->rmax = m;
+}
+
+int force_pass(cr_ctx* ctx, bool zero_list) {
+  StepArgs s = base_args(ctx);
+  s.kind = KIND_NONE;
+  s.write_out = 1;
+  s.active = 0;
+  if (ctx->particle == CR_PARTICLE_ACTIVE && !zero_list) {
+    // addSelfPropulsion advances the ring angles, then adds f0 (cos, sin)
+    launch_advance_angles(ctx->stream, ctx->np, ctx->p_angle, s.sp_amp, ctx->seed, (1ull << 62) + ctx->rng_calls++);
+    ctx->launches++;
+    s.active = 1;
+  }
+  launch_tile(tile_cfg(ctx), ctx->potential, inter_kind(ctx), MODE_FORCE, ctx->p, arrays(ctx, ctx->cur, zero_list), s);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  return CR_OK;
+}
+
+int reduce_now(cr_ctx* ctx) {
+  int rc;
+  if ((rc = ensure_partials(ctx))) return rc;
+  const int nb = std::min(2048, std::max(1, (ctx->nv + 255) / 256));
+  launch_reduce(ctx->stream, ctx->nv, ctx->np, ctx->vel, ctx->force, ctx->energy, ctx->p_energy,
+                inter_kind(ctx) == INT_SMOOTH, ctx->partials, ctx->status, nb);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  return read_status(ctx);
+}
+
+// ------------------------------------------------------------- op sequences
+
+// Ops of one call.  NVE / Langevin / BAOAB: drift, then nsteps tile ops (the
+// last one final); Brownian: a displacement check, then nsteps advancing tile
+// ops; FIRE: nsteps x (pre, tile).
+std::vector<Op> make_ops(cr_ctx* ctx, int kind, long nsteps) {
+  std::vector<Op> ops;
+  int b = ctx->cur;
+  if (kind == KIND_FIRE) {
+    for (long i = 0; i < nsteps; i++) {
+      ops.push_back(Op{OP_FIRE_PRE, b, b, 0, 1, b});
+      ops.push_back(Op{OP_TILE, b, b, 0, 0, b});
+    }
+  } else if (kind == KIND_BROWNIAN || kind == KIND_DRIVEN_BROWNIAN) {
+    ops.push_back(Op{OP_CHECK, b, b, 0, 1, b});
+    for (long i = 0; i < nsteps; i++) {
+      ops.push_back(Op{OP_TILE, b, b ^ 1, 1, 1, b ^ 1});
+      b ^= 1;
+    }
+  } else {
+    ops.push_back(Op{OP_DRIFT, b, b ^ 1, 0, 1, b ^ 1});
+    b ^= 1;
+    for (long i = 0; i < nsteps; i++) {
+      const bool last = (i == nsteps - 1);
+      if (last) {
+        ops.push_back(Op{OP_TILE, b, b, 0, 0, b});
+      } else {
+        ops.push_back(Op{OP_TILE, b, b ^ 1, 1, 1, b ^ 1});
+        b ^= 1;
+      }
+    }
+  }
+  return ops;
+}
+
+void enqueue_op(cr_ctx* ctx, cudaStream_t st, const Op& op, int kind, bool use_cond, cudaGraphConditionalHandle h) {
+  StepArgs s = base_args(ctx);
+  s.kind = kind;
+  s.use_cond = use_cond ? 1 : 0;
+  s.cond = h;
+  s.pos_out = ctx->pos[op.out_buf];
+  s.advance = op.advance;
+  s.accumulate = 1;
+  s.write_out = (kind == KIND_FIRE || !op.advance) ? 1 : 0;
+  s.fire_tol = ctx->fp.tol;
+  const SysArrays a = arrays(ctx, op.in_buf);
+  const int nb = (ctx->nv + 255) / 256;
+  switch (op.type) {
+    case OP_DRIFT:
+      s.kind = kind;
+      launch_drift(st, ctx->p, a, s, nb);
+      break;
+    case OP_CHECK:
+      // a drift with dt = 0 is exactly the displacement check of current positions
+      s.kind = KIND_NVE;
+      s.dt = 0.0;
+      s.hdt = 0.0;
+      s.pos_out = ctx->pos[op.out_buf];
+      launch_drift(st, ctx->p, a, s, nb);
+      break;
+    case OP_FIRE_PRE:
+      launch_fire_pre(st, ctx->p, a, s, ctx->fp, ctx->fire_state, nb);
+      break;
+    case OP_TILE: {
+      LaunchCfg c = tile_cfg(ctx);
+      c.stream = st;
+      launch_tile(c, ctx->potential, inter_kind(ctx), MODE_STEP, ctx->p, a, s);
+      break;
+    }
+  }
+  ctx->launches++;
+}
+
+int capture_graph(cr_ctx* ctx, const std::vector<Op>& ops, int kind, GraphEntry& ge) {
+  cudaGraph_t graph;
+  CR_TRY(cudaGraphCreate(&graph, 0));
+  CR_TRY(cudaStreamBeginCaptureToGraph(ctx->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  for (const Op& op : ops) {
+    cudaGraphConditionalHandle h = 0;
+    if (op.check_after) {
+      cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
+      if (e != cudaSuccess) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(ctx->stream, &dummy);
+        cudaGraphDestroy(graph);
+        return ctx->fail(CR_ECUDA, std::string("cudaGraphConditionalHandleCreate: ") + cudaGetErrorString(e));
+      }
+    }
+    enqueue_op(ctx, ctx->stream, op, kind, op.check_after != 0, h);
+    if (op.check_after) {
+      cudaStreamCaptureStatus cs;
+      cudaGraph_t cg;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t ndeps = 0;
+      CR_TRY(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &cg, &deps, &ndeps));
+      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      CR_TRY(cudaGraphAddNode(&node, cg, deps, ndeps, &cp));
+      CR_TRY(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      CR_TRY(cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      launch_nbr_build(ctx->side, ctx->p, ctx->grid, nbr_args(ctx, op.check_buf, ctx->cut_distance));
+      cudaGraph_t body_out;
+      CR_TRY(cudaStreamEndCapture(ctx->side, &body_out));
+    }
+  }
+  cudaGraph_t out;
+  CR_TRY(cudaStreamEndCapture(ctx->stream, &out));
+  CR_TRY(cudaGraphInstantiate(&ge.exec, out, 0));
+  ge.graph = out;
+  return CR_OK;
+}
+
+// Direct launches with a host check after every op that may arm a rebuild:
+// the fallback when graphs are off, and the resume path after an abort.
+int run_direct(cr_ctx* ctx, const std::vector<Op>& ops, size_t first, int kind) {
+  int rc;
+  for (size_t i = first; i < ops.size(); i++) {
+    const Op& op = ops[i];
+    enqueue_op(ctx, ctx->stream, op, kind, false, 0);
+    CR_TRY(cudaGetLastError());
+    if ((rc = read_status(ctx))) return rc;
+    if (ctx->status_h->abort) return CR_OK;  // caller inspects
+    if (op.check_after && ctx->status_h->rebuild) {
+      if ((rc = build_list(ctx, op.check_buf, ctx->cut_distance))) return rc;
+    }
+  }
+  return CR_OK;
+}
+
+int launch_chunk(cr_ctx* ctx, const std::vector<Op>& ops, int kind, long n) {
+  if (ctx->use_graphs) {
+    auto key = std::make_tuple(kind, n, ops.front().in_buf, ctx->cap, 0ULL);
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+      GraphEntry ge;
+      if (capture_graph(ctx, ops, kind, ge) != CR_OK) {
+        cudaGetLastError();
+        ctx->use_graphs = false;  // direct launches for the life of the context
+      } else {
+        it = ctx->graphs.emplace(key, ge).first;
+      }
+    }
+    if (ctx->use_graphs) {
+      CR_TRY(cudaGraphLaunch(it->second.exec, ctx->stream));
+      ctx->launches += (long long)ops.size();
+      return CR_OK;
+    }
+  }
+  return run_direct(ctx, ops, 0, kind);
+}
+
+// Runs nsteps integrator steps (or FIRE iterations) as chunks of captured
+// graphs.  Non-FIRE chunks are launched back to back with one status read at
+// the end; FIRE reads the status after every chunk to stop at convergence.
+// A neighbour-list overflow inside a chunk aborts the remaining ops (they
+// become no-ops); the host then grows the list and resumes from the op after
+// which the failed build ran.
+int run_ops(cr_ctx* ctx, int kind, long nsteps) {
+  int rc;
+  if ((rc = ensure_partials(ctx))) return rc;
+  if (!ctx->nbr_built) {
+    if ((rc = build_list(ctx, ctx->cur, ctx->cut_distance))) return rc;
+  } else if ((rc = setup_grid(ctx, ctx->cut_distance))) {
+    return rc;
+  }
+  if ((rc = clear_flags(ctx))) return rc;
+  const long long upd0 = ctx->status_h->update_count;
+  const long chunk = 128;
+  std::vector<std::vector<Op>> plan;
+  std::vector<long> sizes;
+  {
+    int b = ctx->cur;
+    for (long done = 0; done < nsteps;) {
+      const long n = std::min(chunk, nsteps - done);
+      const int keep = ctx->cur;
+      ctx->cur = b;
+      plan.push_back(make_ops(ctx, kind, n));
+      ctx->cur = keep;
+      sizes.push_back(n);
+      b = plan.back().back().out_buf;
+      done += n;
+    }
+  }
+  size_t c = 0;
+  while (c < plan.size()) {
+    const long long ops0 = ctx->status_h->ops_done;
+    size_t c_end = c;
+    if (kind == KIND_FIRE) {
+      if ((rc = launch_chunk(ctx, plan[c], kind, sizes[c]))) return rc;
+      c_end = c + 1;
+    } else {
+      for (c_end = c; c_end < plan.size(); c_end++)
+        if ((rc = launch_chunk(ctx, plan[c_end], kind, sizes[c_end]))) return rc;
+    }
+    if ((rc = read_status(ctx))) return rc;
+    if (ctx->status_h->abort) {
+      if (ctx->status_h->nonfinite) return ctx->fail(CR_ENONFINITE, "non-finite force during the step sequence");
+      if (!ctx->status_h->overflow) return ctx->fail(CR_ECUDA, "step sequence aborted");
+      // locate the op after which the failed build ran (builds are not ops)
+      long long k = ctx->status_h->ops_done - ops0;
+      size_t j = c;
+      while (j < c_end && k >= (long long)plan[j].size()) k -= (long long)plan[j++].size();
+      if (j >= c_end || k == 0) return ctx->fail(CR_ECUDA, "inconsistent op counter after abort");
+      if ((rc = clear_flags(ctx))) return rc;
+      ctx->cap = 0;  // build_list grows from the measured count
+      if ((rc = build_list(ctx, plan[j][(size_t)k - 1].check_buf, ctx->cut_distance))) return rc;
+      if ((rc = clear_flags(ctx))) return rc;
+      if ((rc = run_direct(ctx, plan[j], (size_t)k, kind))) return rc;
+      if (ctx->status_h->abort) return ctx->fail(CR_ENBR_OVERFLOW, "neighbour list overflow during resume");
+      c = j + 1;
+      continue;
+    }
+    c = c_end;
+    if (kind == KIND_FIRE && ctx->status_h->converged) break;
+  }
+  ctx->cur = plan[std::min(c, plan.size()) - 1].back().out_buf;
+  if (ctx->status_h->max_ever > 0)
+    ctx->list_size_ref = std::max<long long>(ctx->list_size_ref, pow2ceil(ctx->status_h->max_ever));
+  // kernels of the rebuilds that ran inside conditional nodes
+  ctx->launches += (ctx->status_h->update_count - upd0) * (ctx->grid.ncx ? 6 : 2);
+  return CR_OK;
+}
+
+int check_ctx(const cr_ctx* ctx) { return ctx ? CR_OK : CR_EINVAL; }
+
+int set_current_device(cr_ctx* ctx) {
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return ctx->fail(CR_ECUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  return CR_OK;
+}
+
+int upload(cr_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (!src) return ctx->fail(CR_EINVAL, "NULL host pointer");
+  CR_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+int download(const cr_ctx* cctx, void* dst, const void* src, size_t bytes) {
+  cr_ctx* ctx = const_cast<cr_ctx*>(cctx);
+  if (!dst) return ctx->fail(CR_EINVAL, "NULL host pointer");
+  CR_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+// double AoS <-> double2 internal: identical memory layout.
+static_assert(sizeof(double2) == 2 * sizeof(double), "double2 layout");
+
+}  // namespace
+
+// =========================================================================== C ABI
+extern "C" {
+
+int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
+  if (!out || numParticles <= 0 || !nvList) return CR_EINVAL;
+  *out = nullptr;
+  cr_ctx* ctx = new cr_ctx();
+  int rc;
+  cudaError_t e = cudaGetDevice(&ctx->device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return CR_ECUDA;
+  }
+  ctx->np = (int)numParticles;
+  long total = 0;
+  int maxnv = 0;
+  for (long q = 0; q < numParticles; q++) {
+    if (nvList[q] < 3) {
+      delete ctx;
+      return CR_EINVAL;
+    }
+    ctx->ring_first_h.push_back((int)total);
+    ctx->ring_nv_h.push_back((int)nvList[q]);
+    total += nvList[q];
+    maxnv = std::max(maxnv, (int)nvList[q]);
+  }
+  if (total >= (1L << 30)) {
+    delete ctx;
+    return CR_EINVAL;
+  }
+  ctx->nv = (int)total;
+  ctx->lanes = maxnv > tile_vertices(2) ? 1 : 2;
+  if (maxnv > tile_vertices(1)) {
+    delete ctx;
+    return CR_ENOTSUP;
+  }
+  ctx->ring_of_h.resize(total);
+  std::vector<int2> pp(total);
+  for (int q = 0; q < ctx->np; q++) {
+    const int f = ctx->ring_first_h[q], n = ctx->ring_nv_h[q];
+    for (int k = 0; k < n; k++) {
+      ctx->ring_of_h[f + k] = q;
+      const int prev = f + (k == 0 ? n - 1 : k - 1);
+      const int k2 = (k - 2 + 2 * n) % n;
+      pp[f + k] = make_int2(prev, f + k2);
+    }
+  }
+  // tiles: consecutive whole rings up to the tile capacity
+  const int tv = tile_vertices(ctx->lanes);
+  int r = 0;
+  while (r < ctx->np) {
+    int r1 = r, cnt = 0;
+    while (r1 < ctx->np && cnt + ctx->ring_nv_h[r1] <= tv) cnt += ctx->ring_nv_h[r1++];
+    ctx->tiles_h.push_back(make_int4(r, r1, ctx->ring_first_h[r], ctx->ring_first_h[r] + cnt));
+    r = r1;
+  }
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete ctx;
+    return CR_ECUDA;
+  }
+  const size_t nv = total, np = numParticles;
+  if ((rc = dalloc(ctx, &ctx->pos[0], nv)) || (rc = dalloc(ctx, &ctx->pos[1], nv)) ||
+      (rc = dalloc(ctx, &ctx->vel, nv)) || (rc = dalloc(ctx, &ctx->force, nv)) ||
+      (rc = dalloc(ctx, &ctx->last_pos, nv)) || (rc = dalloc(ctx, &ctx->ppos, np)) ||
+      (rc = dalloc(ctx, &ctx->rad, nv)) || (rc = dalloc(ctx, &ctx->l0, nv)) || (rc = dalloc(ctx, &ctx->theta0, nv)) ||
+      (rc = dalloc(ctx, &ctx->a0, np)) || (rc = dalloc(ctx, &ctx->energy, nv)) ||
+      (rc = dalloc(ctx, &ctx->p_energy, np)) || (rc = dalloc(ctx, &ctx->theta, nv)) ||
+      (rc = dalloc(ctx, &ctx->length, nv)) || (rc = dalloc(ctx, &ctx->area, np)) ||
+      (rc = dalloc(ctx, &ctx->perimeter, np)) || (rc = dalloc(ctx, &ctx->p_angle, np)) ||
+      (rc = dalloc(ctx, &ctx->vertex_area, np)) || (rc = dalloc(ctx, &ctx->ring_of, nv)) ||
+      (rc = dalloc(ctx, &ctx->ring_first, np)) || (rc = dalloc(ctx, &ctx->ring_nv, np)) ||
+      (rc = dalloc(ctx, &ctx->zero_cnt, nv)) || (rc = dalloc(ctx, &ctx->pp_of, nv)) ||
+      (rc = dalloc(ctx, &ctx->tiles, ctx->tiles_h.size())) || (rc = dalloc(ctx, &ctx->nbr_cnt, nv)) ||
+      (rc = dalloc(ctx, &ctx->cell_of, nv)) || (rc = dalloc(ctx, &ctx->slot, nv)) ||
+      (rc = dalloc(ctx, &ctx->cell_vid, nv)) || (rc = dalloc(ctx, &ctx->cell_ring, nv)) ||
+      (rc = dalloc(ctx, &ctx->cell_pos, nv)) || (rc = dalloc(ctx, &ctx->cell_rad, nv)) ||
+      (rc = dalloc(ctx, &ctx->status, 1)) || (rc = dalloc(ctx, &ctx->fire_state, 8))) {
+    cr_destroy(ctx);
+    return rc;
+  }
+  ctx->cap = 16;
+  if ((rc = dalloc(ctx, &ctx->nbr, (size_t)ctx->cap * nv))) {
+    cr_destroy(ctx);
+    return rc;
+  }
+  if (cudaMallocHost((void**)&ctx->status_h, sizeof(DevStatus)) != cudaSuccess) {
+    cr_destroy(ctx);
+    return CR_ENOMEM;
+  }
+  memset(ctx->status_h, 0, sizeof(DevStatus));
+  if (upload(ctx, ctx->ring_of, ctx->ring_of_h.data(), nv * sizeof(int)) ||
+      upload(ctx, ctx->ring_first, ctx->ring_first_h.data(), np * sizeof(int)) ||
+      upload(ctx, ctx->ring_nv, ctx->ring_nv_h.data(), np * sizeof(int)) ||
+      upload(ctx, ctx->pp_of, pp.data(), nv * sizeof(int2)) ||
+      upload(ctx, ctx->tiles, ctx->tiles_h.data(), ctx->tiles_h.size() * sizeof(int4))) {
+    cr_destroy(ctx);
+    return CR_ECUDA;
+  }
+  // reference defaults (src/DPM2D.cu:41-95)
+  ctx->p.lx = ctx->p.ly = 1.0;
+  ctx->p.ea = 1e5;
+  ctx->p.el = 20;
+  ctx->p.eb = 10;
+  ctx->p.ec = 1;
+  ctx->dt = 1e-3;
+  refresh_params(ctx);
+  if (ensure_partials(ctx)) {
+    cr_destroy(ctx);
+    return CR_ENOMEM;
+  }
+  *out = ctx;
+  return CR_OK;
+}
+
+int cr_destroy(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  drop_graphs(ctx);
+  void* ptrs[] = {ctx->pos[0], ctx->pos[1], ctx->vel, ctx->force, ctx->last_pos, ctx->ppos, ctx->rad, ctx->l0,
+                  ctx->theta0, ctx->a0, ctx->energy, ctx->p_energy, ctx->theta, ctx->length, ctx->area,
+                  ctx->perimeter, ctx->p_angle, ctx->vertex_area, ctx->ring_of, ctx->ring_first, ctx->ring_nv,
+                  ctx->zero_cnt, ctx->pp_of, ctx->tiles, ctx->nbr, ctx->nbr_cnt, ctx->cell_of, ctx->slot,
+                  ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
+                  ctx->partials, ctx->status, ctx->fire_state};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (ctx->status_h) cudaFreeHost(ctx->status_h);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (ctx->side) cudaStreamDestroy(ctx->side);
+  delete ctx;
+  return CR_OK;
+}
+
+const char* cr_last_error(const cr_ctx* ctx) { return ctx ? ctx->err.c_str() : "NULL context"; }
+
+int cr_get_num_vertices(const cr_ctx* ctx, long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  *out = ctx->nv;
+  return CR_OK;
+}
+int cr_get_num_particles(const cr_ctx* ctx, long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  *out = ctx->np;
+  return CR_OK;
+}
+
+#define CR_ENUM_SETTER(name, field, lo, hi)                                   \
+  int name(cr_ctx* ctx, int v) {                                             \
+    if (!ctx) return CR_EINVAL;                                              \
+    if (v < (lo) || v > (hi)) return ctx->fail(CR_EINVAL, #name ": bad value"); \
+    ctx->field = v;                                                          \
+    refresh_params(ctx);                                                     \
+    drop_graphs(ctx);                                                        \
+    return CR_OK;                                                            \
+  }
+CR_ENUM_SETTER(cr_set_potential_type, potential, 0, 3)
+CR_ENUM_SETTER(cr_set_monomer_type, monomer, 0, 1)
+CR_ENUM_SETTER(cr_set_noise_type, noise_type, 0, 3)
+CR_ENUM_SETTER(cr_set_shape_type, shape, 0, 1)
+
+int cr_set_interaction_type(cr_ctx* ctx, int v) {
+  if (!ctx) return CR_EINVAL;
+  if (v < 0 || v > 3) return ctx->fail(CR_EINVAL, "cr_set_interaction_type: bad value");
+  if (v == CR_INTERACTION_ALL)
+    return ctx->fail(CR_ENOTSUP, "interactionEnum::all (O(N^2) debug path) is served by the neighbour list path");
+  ctx->interaction = v;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_particle_type(cr_ctx* ctx, int v) {
+  if (!ctx) return CR_EINVAL;
+  if (v < 0 || v > 2) return ctx->fail(CR_EINVAL, "cr_set_particle_type: bad value");
+  if (v == CR_PARTICLE_ACTIVE_SHAPE)
+    return ctx->fail(CR_ENOTSUP, "activeShape (rest-length noise) is not on the accelerated path");
+  ctx->particle = v;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_geometry_type(cr_ctx* ctx, int v) {
+  if (!ctx) return CR_EINVAL;
+  if (v != CR_GEOMETRY_NORMAL) return ctx->fail(CR_ENOTSUP, "only periodic geometry is supported");
+  ctx->geometry = v;
+  return CR_OK;
+}
+
+int cr_set_box_size(cr_ctx* ctx, const double* box) {
+  if (!ctx || !box || !(box[0] > 0) || !(box[1] > 0)) return ctx ? ctx->fail(CR_EINVAL, "bad box") : CR_EINVAL;
+  ctx->p.lx = box[0];
+  ctx->p.ly = box[1];
+  refresh_params(ctx);
+  drop_graphs(ctx);
+  return CR_OK;
+}
+int cr_get_box_size(const cr_ctx* ctx, double* box) {
+  if (!ctx || !box) return CR_EINVAL;
+  box[0] = ctx->p.lx;
+  box[1] = ctx->p.ly;
+  return CR_OK;
+}
+
+int cr_set_energy_costs(cr_ctx* ctx, double ea, double el, double eb, double ec) {
+  if (!ctx) return CR_EINVAL;
+  ctx->p.ea = ea;
+  ctx->p.el = el;
+  ctx->p.eb = eb;
+  ctx->p.ec = ec;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_lj_cutoff(cr_ctx* ctx, double c) {
+  if (!ctx || !(c > 0)) return ctx ? ctx->fail(CR_EINVAL, "bad LJ cutoff") : CR_EINVAL;
+  ctx->p.lj_cutoff = c;
+  const double ratio6 = 1 / std::pow(c, 6);
+  ctx->p.lj_ecut = 4 * ctx->p.ec * (ratio6 * ratio6 - ratio6);
+  ctx->p.lj_fshift = 24 * ctx->p.ec * (2 * ratio6 - 1) * ratio6 / c;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_attraction_constants(cr_ctx* ctx, double l1, double l2) {
+  if (!ctx) return CR_EINVAL;
+  ctx->p.l1 = l1;
+  ctx->p.l2 = l2;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_fene_constants(cr_ctx* ctx, double stiff, double ext) {
+  if (!ctx) return CR_EINVAL;
+  ctx->p.stiff = stiff;
+  ctx->p.ext_sq = ext * ext;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_time_step(cr_ctx* ctx, double dt) {
+  if (!ctx || !(dt > 0)) return ctx ? ctx->fail(CR_EINVAL, "bad dt") : CR_EINVAL;
+  ctx->dt = dt;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_self_propulsion_params(cr_ctx* ctx, double driving, double taup) {
+  if (!ctx) return CR_EINVAL;
+  ctx->driving = driving;
+  ctx->taup = taup;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_set_seed(cr_ctx* ctx, unsigned long long seed) {
+  if (!ctx) return CR_EINVAL;
+  ctx->seed = seed;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+#define CR_NV2 ((size_t)ctx->nv * sizeof(double2))
+#define CR_NV1 ((size_t)ctx->nv * sizeof(double))
+#define CR_NP1 ((size_t)ctx->np * sizeof(double))
+
+int cr_set_vertex_positions(cr_ctx* ctx, const double* pos) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->pos[ctx->cur], pos, CR_NV2);
+}
+int cr_get_vertex_positions(const cr_ctx* ctx, double* pos) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, pos, ctx->pos[ctx->cur], CR_NV2);
+}
+int cr_set_vertex_velocities(cr_ctx* ctx, const double* vel) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->vel, vel, CR_NV2);
+}
+int cr_get_vertex_velocities(const cr_ctx* ctx, double* vel) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, vel, ctx->vel, CR_NV2);
+}
+int cr_get_vertex_forces(const cr_ctx* ctx, double* f) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, f, ctx->force, CR_NV2);
+}
+int cr_set_vertex_forces(cr_ctx* ctx, const double* f) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->force, f, CR_NV2);
+}
+int cr_get_vertex_energies(const cr_ctx* ctx, double* e) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, e, ctx->energy, CR_NV1);
+}
+int cr_get_particle_energies(const cr_ctx* ctx, double* e) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, e, ctx->p_energy, CR_NP1);
+}
+int cr_set_vertex_radii(cr_ctx* ctx, const double* rad) {
+  if (!ctx) return CR_EINVAL;
+  int rc = upload(ctx, ctx->rad, rad, CR_NV1);
+  if (rc == CR_OK) {
+    update_rmax(ctx, rad);
+    drop_graphs(ctx);
+  }
+  return rc;
+}
+int cr_get_vertex_radii(const cr_ctx* ctx, double* rad) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, rad, ctx->rad, CR_NV1);
+}
+int cr_set_rest_areas(cr_ctx* ctx, const double* a0) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->a0, a0, CR_NP1);
+}
+int cr_get_rest_areas(const cr_ctx* ctx, double* a0) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, a0, ctx->a0, CR_NP1);
+}
+int cr_set_rest_lengths(cr_ctx* ctx, const double* l0) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->l0, l0, CR_NV1);
+}
+int cr_get_rest_lengths(const cr_ctx* ctx, double* l0) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, l0, ctx->l0, CR_NV1);
+}
+int cr_set_rest_angles(cr_ctx* ctx, const double* t0) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->theta0, t0, CR_NV1);
+}
+int cr_get_areas(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->area, CR_NP1);
+}
+int cr_get_perimeters(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->perimeter, CR_NP1);
+}
+int cr_get_segment_lengths(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->length, CR_NV1);
+}
+int cr_get_segment_angles(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->theta, CR_NV1);
+}
+int cr_calc_particle_shape(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  // geometry pass only: the force outputs are restored afterwards by keeping
+  // them out of this pass (a zero-length neighbour list and a scratch force)
+  double2* keep_force = ctx->force;
+  double* keep_energy = ctx->energy;
+  double* keep_pe = ctx->p_energy;
+  double2* tmpf = nullptr;
+  double* tmpe = nullptr;
+  double* tmpp = nullptr;
+  CR_TRY(cudaMallocAsync((void**)&tmpf, CR_NV2, ctx->stream));
+  CR_TRY(cudaMallocAsync((void**)&tmpe, CR_NV1, ctx->stream));
+  CR_TRY(cudaMallocAsync((void**)&tmpp, CR_NP1, ctx->stream));
+  ctx->force = tmpf;
+  ctx->energy = tmpe;
+  ctx->p_energy = tmpp;
+  int particle = ctx->particle;
+  ctx->particle = CR_PARTICLE_PASSIVE;
+  int rc = force_pass(ctx, true);
+  ctx->particle = particle;
+  ctx->force = keep_force;
+  ctx->energy = keep_energy;
+  ctx->p_energy = keep_pe;
+  cudaFreeAsync(tmpf, ctx->stream);
+  cudaFreeAsync(tmpe, ctx->stream);
+  cudaFreeAsync(tmpp, ctx->stream);
+  if (rc) return rc;
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+int cr_calc_particle_positions(cr_ctx* ctx) { return cr_calc_particle_shape(ctx); }
+int cr_get_particle_positions(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->ppos, (size_t)ctx->np * sizeof(double2));
+}
+int cr_set_particle_positions(cr_ctx* ctx, const double* pp) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->ppos, pp, (size_t)ctx->np * sizeof(double2));
+}
+
+int cr_set_displacement_cutoff(cr_ctx* ctx, double cutoff, double size, double* cut_out) {
+  if (!ctx) return CR_EINVAL;
+  // DPM2D::setDisplacementCutoff (src/DPM2D.cu:1300-1329)
+  double base = 1.0;
+  switch (ctx->potential) {
+    case CR_POTENTIAL_HARMONIC: base = 1.0; break;
+    case CR_POTENTIAL_LENNARD_JONES: base = ctx->p.lj_cutoff; break;
+    case CR_POTENTIAL_WCA: base = kWCAcut; break;
+    case CR_POTENTIAL_ADHESIVE: base = 1.0 + ctx->p.l2; break;
+  }
+  ctx->cut_distance = base + cutoff;
+  ctx->cutoff = cutoff * size;
+  drop_graphs(ctx);
+  if (cut_out) *cut_out = ctx->cut_distance;
+  return CR_OK;
+}
+
+int cr_calc_neighbor_list(cr_ctx* ctx, double cut) {
+  if (!ctx) return CR_EINVAL;
+  int rc = clear_flags(ctx);
+  if (rc) return rc;
+  return build_list(ctx, ctx->cur, cut);
+}
+
+int cr_reset_last_positions(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  CR_TRY(cudaMemcpyAsync(ctx->last_pos, ctx->pos[ctx->cur], CR_NV2, cudaMemcpyDeviceToDevice, ctx->stream));
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+int cr_check_neighbors(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  int rc;
+  if ((rc = clear_flags(ctx))) return rc;
+  std::vector<Op> ops{Op{OP_CHECK, ctx->cur, ctx->cur, 0, 1, ctx->cur}};
+  if ((rc = run_direct(ctx, ops, 0, KIND_NVE))) return rc;
+  return CR_OK;
+}
+
+int cr_get_neighbor_list_size(const cr_ctx* ctx, long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  *out = (long)ctx->list_size_ref;
+  return CR_OK;
+}
+
+int cr_get_max_neighbor_list(const cr_ctx* ctx, long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  std::vector<int> cnt(ctx->nv);
+  int rc = download(ctx, cnt.data(), ctx->nbr_built ? ctx->nbr_cnt : ctx->zero_cnt, ctx->nv * sizeof(int));
+  if (rc) return rc;
+  for (int i = 0; i < ctx->nv; i++) out[i] = cnt[i];
+  return CR_OK;
+}
+
+int cr_get_neighbors(const cr_ctx* ctx, long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  const long ls = ctx->list_size_ref;
+  if (ls == 0) return CR_OK;
+  std::vector<int> cnt(ctx->nv), nb((size_t)ctx->cap * ctx->nv);
+  int rc;
+  if ((rc = download(ctx, cnt.data(), ctx->nbr_built ? ctx->nbr_cnt : ctx->zero_cnt, ctx->nv * sizeof(int)))) return rc;
+  if ((rc = download(ctx, nb.data(), ctx->nbr, nb.size() * sizeof(int)))) return rc;
+  std::vector<int> row;
+  for (int i = 0; i < ctx->nv; i++) {
+    row.clear();
+    for (int s = 0; s < std::min(cnt[i], ctx->cap); s++) row.push_back(nb[(size_t)s * ctx->nv + i]);
+    std::sort(row.begin(), row.end());
+    for (long s = 0; s < ls; s++) out[(size_t)i * ls + s] = s < (long)row.size() ? row[s] : -1;
+  }
+  return CR_OK;
+}
+
+int cr_get_update_count(const cr_ctx* ctx, long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  cr_ctx* c = const_cast<cr_ctx*>(ctx);
+  int rc = read_status(c);
+  if (rc) return rc;
+  *out = (long)c->status_h->update_count;
+  return CR_OK;
+}
+
+int cr_reset_update_count(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  int rc = read_status(ctx);
+  if (rc) return rc;
+  ctx->status_h->update_count = 0;
+  return upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus));
+}
+
+int cr_calc_force_energy(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  int rc = force_pass(ctx, false);
+  if (rc) return rc;
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+int cr_get_potential_energy(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = reduce_now(ctx);
+  if (rc) return rc;
+  *out = ctx->status_h->sums[S_PE];
+  return CR_OK;
+}
+int cr_get_kinetic_energy(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = reduce_now(ctx);
+  if (rc) return rc;
+  *out = 0.5 * ctx->status_h->sums[S_VV];
+  return CR_OK;
+}
+int cr_get_energy(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = reduce_now(ctx);
+  if (rc) return rc;
+  *out = ctx->status_h->sums[S_PE] + 0.5 * ctx->status_h->sums[S_VV];
+  return CR_OK;
+}
+int cr_get_temperature(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = reduce_now(ctx);
+  if (rc) return rc;
+  *out = 2.0 * (0.5 * ctx->status_h->sums[S_VV]) / (ctx->nv * 2.0);
+  return CR_OK;
+}
+int cr_get_max_unbalanced_force(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = reduce_now(ctx);
+  if (rc) return rc;
+  *out = std::sqrt(ctx->status_h->sums[S_FMAX2]);
+  return CR_OK;
+}
+int cr_get_total_force_magnitude(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = reduce_now(ctx);
+  if (rc) return rc;
+  *out = std::sqrt(ctx->status_h->sums[S_FF] / (ctx->nv * 2.0));
+  return CR_OK;
+}
+
+static int phi_common(cr_ctx* ctx, const double* ring_area_dev, double* out) {
+  std::vector<double> ar(ctx->np), va(ctx->np);
+  launch_vertex_area(ctx->stream, ctx->np, ctx->ring_first, ctx->ring_nv, ctx->rad, ctx->vertex_area);
+  ctx->launches++;
+  int rc;
+  if ((rc = download(ctx, ar.data(), ring_area_dev, CR_NP1))) return rc;
+  if ((rc = download(ctx, va.data(), ctx->vertex_area, CR_NP1))) return rc;
+  double s = 0.0, v = 0.0;
+  for (int q = 0; q < ctx->np; q++) s += ar[q];
+  for (int q = 0; q < ctx->np; q++) v += va[q];
+  *out = (s + kPi * v) / (ctx->p.lx * ctx->p.ly);
+  return CR_OK;
+}
+int cr_get_phi(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  return phi_common(ctx, ctx->area, out);
+}
+int cr_get_preferred_phi(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  return phi_common(ctx, ctx->a0, out);
+}
+int cr_get_mean_vertex_radius(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  std::vector<double> r(ctx->nv);
+  int rc = download(ctx, r.data(), ctx->rad, CR_NV1);
+  if (rc) return rc;
+  double s = 0;
+  for (double x : r) s += x;
+  *out = s / ctx->nv;
+  return CR_OK;
+}
+int cr_get_mean_particle_size(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  std::vector<double> a(ctx->np);
+  int rc = download(ctx, a.data(), ctx->a0, CR_NP1);
+  if (rc) return rc;
+  double s = 0;
+  for (double x : a) s += x;
+  *out = 2 * std::sqrt(s / (kPi * ctx->np));  // src/DPM2D.cu:781-783
+  return CR_OK;
+}
+
+int cr_scale_vertices(cr_ctx* ctx, double scale) {
+  if (!ctx || !(scale > 0)) return ctx ? ctx->fail(CR_EINVAL, "bad scale") : CR_EINVAL;
+  launch_scale_vertices(ctx->stream, ctx->nv, ctx->np, ctx->ring_of, ctx->ppos, ctx->pos[ctx->cur], ctx->a0,
+                        ctx->area, ctx->l0, ctx->rad, scale);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->rmax *= scale;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+static int reset_rng_step(cr_ctx* ctx) {
+  int rc = read_status(ctx);
+  if (rc) return rc;
+  ctx->status_h->rng_step = 0;
+  return upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus));
+}
+
+int cr_init_nve(cr_ctx* ctx, double T, int readState) {
+  if (!ctx) return CR_EINVAL;
+  // DPM2D::initNVE (src/DPM2D.cu:3760-3771): lastPos = pos, KE injection
+  int rc = cr_reset_last_positions(ctx);
+  if (rc) return rc;
+  if ((rc = reset_rng_step(ctx))) return rc;
+  ctx->sim_kind = KIND_NVE;
+  ctx->T = T;
+  if (!readState) {
+    launch_inject_ke(ctx->stream, ctx->nv, ctx->ring_of, ctx->vel, std::sqrt(T), ctx->seed, (1ull << 61) + ctx->rng_calls++);
+    ctx->launches++;
+    CR_TRY(cudaGetLastError());
+    CR_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_nve_loop(cr_ctx* ctx, long nsteps) {
+  if (!ctx || nsteps < 0) return CR_EINVAL;
+  if (ctx->sim_kind != KIND_NVE) return ctx->fail(CR_ESTATE, "cr_nve_loop before cr_init_nve");
+  if (nsteps == 0) return CR_OK;
+  return run_ops(ctx, KIND_NVE, nsteps);
+}
+
+int cr_init_langevin(cr_ctx* ctx, double T, double gamma, int readState) {
+  if (!ctx) return CR_EINVAL;
+  // DPM2D::initLangevin (src/DPM2D.cu:3713-3753)
+  ctx->T = T;
+  switch (ctx->noise_type) {
+    case CR_NOISE_LANGEVIN:
+      ctx->sim_kind = KIND_LANGEVIN;
+      ctx->gamma = gamma;
+      ctx->noise = std::sqrt(2.0 * T * gamma / ctx->dt);
+      break;
+    case CR_NOISE_BAOAB:
+      ctx->sim_kind = KIND_BAOAB;
+      ctx->gamma_factor = std::exp(-gamma * ctx->dt);
+      ctx->noise = std::sqrt(1 - std::exp(-2 * gamma * ctx->dt)) * std::sqrt(T);
+      break;
+    case CR_NOISE_BROWNIAN:
+      ctx->sim_kind = KIND_BROWNIAN;
+      ctx->gamma = gamma;
+      ctx->noise = std::sqrt(2.0 * T * gamma / ctx->dt);
+      break;
+    default:
+      ctx->sim_kind = KIND_DRIVEN_BROWNIAN;
+      ctx->gamma = gamma;
+      ctx->noise = std::sqrt(2.0 * T * gamma / ctx->dt);
+      break;
+  }
+  int rc = cr_reset_last_positions(ctx);
+  if (rc) return rc;
+  if ((rc = reset_rng_step(ctx))) return rc;
+  if (!readState) {
+    launch_inject_ke(ctx->stream, ctx->nv, ctx->ring_of, ctx->vel, std::sqrt(T), ctx->seed, (1ull << 61) + ctx->rng_calls++);
+    ctx->launches++;
+    CR_TRY(cudaGetLastError());
+    CR_TRY(cudaStreamSynchronize(ctx->stream));
+  }
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_langevin_loop(cr_ctx* ctx, long nsteps) {
+  if (!ctx || nsteps < 0) return CR_EINVAL;
+  if (ctx->sim_kind < KIND_LANGEVIN || ctx->sim_kind > KIND_DRIVEN_BROWNIAN)
+    return ctx->fail(CR_ESTATE, "cr_langevin_loop before cr_init_langevin");
+  if (nsteps == 0) return CR_OK;
+  return run_ops(ctx, ctx->sim_kind, nsteps);
+}
+
+int cr_init_fire(cr_ctx* ctx, const double* prm, long minStep, long numStep, long numDOF) {
+  if (!ctx || !prm) return CR_EINVAL;
+  (void)numDOF;
+  ctx->fp.a_start = prm[0];
+  ctx->fp.f_dec = prm[1];
+  ctx->fp.f_inc = prm[2];
+  ctx->fp.f_a = prm[3];
+  ctx->fp.dt_max = prm[5];
+  ctx->fp.min_step = minStep;
+  ctx->fp.tol = -1.0;
+  double st[8] = {prm[4], prm[6], (double)numStep, 0, prm[4], prm[6], (double)numStep, 0};
+  int rc = upload(ctx, ctx->fire_state, st, sizeof(st));
+  if (rc) return rc;
+  if ((rc = read_status(ctx))) return rc;
+  ctx->status_h->fire_iters = 0;
+  if ((rc = upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus)))) return rc;
+  ctx->fire_ready = true;
+  ctx->sim_kind = KIND_FIRE;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+static int fire_run(cr_ctx* ctx, long nsteps, double tol) {
+  int rc;
+  ctx->fp.tol = tol;
+  drop_graphs(ctx);
+  if ((rc = reduce_now(ctx))) return rc;  // P, |v|^2, |F|^2 of the current state
+  if ((rc = clear_flags(ctx))) return rc;
+  if (tol >= 0 && ctx->status_h->sums[S_FMAX2] <= tol * tol) return CR_OK;
+  return run_ops(ctx, KIND_FIRE, nsteps);
+}
+
+int cr_vertex_fire_loop(cr_ctx* ctx, long nsteps) {
+  if (!ctx || nsteps < 0) return CR_EINVAL;
+  if (!ctx->fire_ready) return ctx->fail(CR_ESTATE, "cr_vertex_fire_loop before cr_init_fire");
+  if (nsteps == 0) return CR_OK;
+  return fire_run(ctx, nsteps, -1.0);
+}
+
+int cr_fire_minimize(cr_ctx* ctx, double tol, long maxIter, long* iterations, double* maxForce) {
+  if (!ctx || maxIter < 0) return CR_EINVAL;
+  if (!ctx->fire_ready) return ctx->fail(CR_ESTATE, "cr_fire_minimize before cr_init_fire");
+  int rc = read_status(ctx);
+  if (rc) return rc;
+  const long long it0 = ctx->status_h->fire_iters;
+  rc = fire_run(ctx, maxIter, tol);
+  if (rc) return rc;
+  if ((rc = read_status(ctx))) return rc;
+  if (iterations) *iterations = (long)(ctx->status_h->fire_iters - it0);
+  double m;
+  if ((rc = cr_get_max_unbalanced_force(ctx, &m))) return rc;
+  if (maxForce) *maxForce = m;
+  return CR_OK;
+}
+
+int cr_get_fire_state(cr_ctx* ctx, double* out3) {
+  if (!ctx || !out3) return CR_EINVAL;
+  int rc = read_status(ctx);
+  if (rc) return rc;
+  double st[8];
+  if ((rc = download(ctx, st, ctx->fire_state, sizeof(st)))) return rc;
+  const int b = (int)(ctx->status_h->fire_iters & 1);
+  out3[0] = st[b * 4];
+  out3[1] = st[b * 4 + 1];
+  out3[2] = st[b * 4 + 2];
+  return CR_OK;
+}
+
+int cr_get_stream(const cr_ctx* ctx, void** out) {
+  if (!ctx || !out) return CR_EINVAL;
+  *out = (void*)ctx->stream;
+  return CR_OK;
+}
+
+int cr_profile_step_kernel(cr_ctx* ctx, long reps, double* ms_per_launch) {
+  if (!ctx || reps <= 0 || !ms_per_launch) return CR_EINVAL;
+  if (!ctx->nbr_built) return ctx->fail(CR_ESTATE, "cr_profile_step_kernel before a neighbour list exists");
+  int rc;
+  if ((rc = ensure_partials(ctx))) return rc;
+  // scratch copies so the context state is untouched
+  double2 *pos_s = nullptr, *vel_s = nullptr, *frc_s = nullptr;
+  DevStatus* st_s = nullptr;
+  CR_TRY(cudaMallocAsync((void**)&pos_s, CR_NV2, ctx->stream));
+  CR_TRY(cudaMallocAsync((void**)&vel_s, CR_NV2, ctx->stream));
+  CR_TRY(cudaMallocAsync((void**)&frc_s, CR_NV2, ctx->stream));
+  CR_TRY(cudaMallocAsync((void**)&st_s, sizeof(DevStatus), ctx->stream));
+  CR_TRY(cudaMemcpyAsync(vel_s, ctx->vel, CR_NV2, cudaMemcpyDeviceToDevice, ctx->stream));
+  CR_TRY(cudaMemsetAsync(st_s, 0, sizeof(DevStatus), ctx->stream));
+  StepArgs s = base_args(ctx);
+  s.kind = ctx->sim_kind >= 0 && ctx->sim_kind != KIND_FIRE ? ctx->sim_kind : KIND_NVE;
+  s.advance = 1;
+  s.accumulate = 1;
+  s.active = 0;  // ring angles are state; the self-propulsion term is not timed here
+  s.pos_out = pos_s;
+  s.vel = vel_s;
+  s.force = frc_s;
+  s.status = st_s;
+  const SysArrays a = arrays(ctx, ctx->cur);
+  cudaEvent_t e0, e1;
+  CR_TRY(cudaEventCreate(&e0));
+  CR_TRY(cudaEventCreate(&e1));
+  for (int w = 0; w < 3; w++) launch_tile(tile_cfg(ctx), ctx->potential, inter_kind(ctx), MODE_STEP, ctx->p, a, s);
+  CR_TRY(cudaEventRecord(e0, ctx->stream));
+  for (long r = 0; r < reps; r++) launch_tile(tile_cfg(ctx), ctx->potential, inter_kind(ctx), MODE_STEP, ctx->p, a, s);
+  CR_TRY(cudaEventRecord(e1, ctx->stream));
+  CR_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  CR_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  *ms_per_launch = ms / (double)reps;
+  ctx->launches += reps + 3;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFreeAsync(pos_s, ctx->stream);
+  cudaFreeAsync(vel_s, ctx->stream);
+  cudaFreeAsync(frc_s, ctx->stream);
+  cudaFreeAsync(st_s, ctx->stream);
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+int cr_get_launch_count(const cr_ctx* ctx, long long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  *out = ctx->launches;
+  return CR_OK;
+}
+
+}  // extern "C"

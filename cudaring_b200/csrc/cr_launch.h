@@ -1,0 +1,70 @@
+// Host-side declarations of the kernel launchers (internal to libcudaring).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "cr_common.cuh"
+
+namespace cr {
+
+struct StepArgs;
+
+struct LaunchCfg {
+  cudaStream_t stream;
+  int grid;    // number of tiles / CTAs
+  int lanes;   // lanes per vertex in the pair phase (1, 2, 4)
+};
+
+// cr_tile.cu
+void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
+                 const StepArgs& s);
+int tile_vertices(int lanes);
+
+// cr_misc.cu
+struct FireParams {
+  double a_start, f_dec, f_inc, f_a, dt_max;
+  long long min_step;
+  double tol;
+};
+void launch_drift(cudaStream_t st, const SysParams& p, const SysArrays& a, const StepArgs& s, int nblocks);
+void launch_fire_pre(cudaStream_t st, const SysParams& p, const SysArrays& a, const StepArgs& s,
+                     const FireParams& fp, double* fire_state, int nblocks);
+void launch_reduce(cudaStream_t st, int nv, int np, const double2* vel, const double2* force, const double* energy,
+                   const double* p_energy, int use_p_energy, double* partials, DevStatus* status, int nblocks);
+void launch_inject_ke(cudaStream_t st, int nv, const int* ring_of, double2* vel, double amplitude,
+                      unsigned long long seed, unsigned long long stream);
+void launch_scale_vertices(cudaStream_t st, int nv, int np, const int* ring_of, const double2* ppos, double2* pos,
+                           double* a0, double* area, double* l0, double* rad, double scale);
+void launch_advance_angles(cudaStream_t st, int np, double* angle, double amp, unsigned long long seed,
+                           unsigned long long stream);
+void launch_vertex_area(cudaStream_t st, int np, const int* ring_first, const int* ring_nv, const double* rad,
+                        double* out);
+
+// cr_nbr.cu
+struct CellGrid {
+  int ncx, ncy;       // cells per dimension (>= 3 each), or 0 for brute force
+  double cx, cy;      // cell sizes
+};
+struct NbrArgs {
+  const double2* pos;
+  const double* rad;
+  const int* ring_of;
+  int* nbr;           // [cap][nv]
+  int* nbr_cnt;
+  int cap;
+  double cut_distance;
+  double2* last_pos;  // set to pos by the build
+  // cell scratch
+  int* cell_of;
+  int* slot;
+  int* cell_cnt;      // [ncells], zero between builds
+  int* cell_start;    // [ncells + 1]
+  int* cell_vid;      // [nv]
+  double2* cell_pos;  // [nv]
+  double* cell_rad;   // [nv]
+  int* cell_ring;     // [nv]
+  DevStatus* status;
+  int count_op;       // 1: the build is one op of a step sequence (ops_done += 1)
+};
+void launch_nbr_build(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n);
+
+}  // namespace cr

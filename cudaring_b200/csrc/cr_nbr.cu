@@ -1,0 +1,223 @@
+// Neighbour-list build on a periodic cell grid.
+//
+// Rule (kernelCalcNeighborList, include/cudaKernel.cuh:1735-1763): j is a
+// neighbour of i iff ring(j) != ring(i) and -(1 - d_ij/(r_i + r_j)) <
+// cutDistance, d_ij the minimum-image distance.  The host picks cells no
+// smaller than (1 + cutDistance) * 2 * max(rad) (plus a relative margin), so
+// every such pair lies in the 3x3 cell stencil and the set equals the
+// reference's O(Nv^2) scan; the test itself is evaluated with the same
+// expression.  Systems with fewer than 3 cells per side use the brute-force
+// kernel.
+//
+// Kernels (all graph-capturable, no host synchronisation):
+//   k_cell_count   cell of each vertex + slot inside the cell (atomic)
+//   k_cell_scan    exclusive scan of the cell counts (one CTA), zeroes counts
+//   k_cell_fill    scatter vertex ids by cell
+//   k_cell_sort    sort each cell's ids ascending and copy pos/rad/ring (SoA)
+//   k_nbr_cells    stencil search -> slot-major list, counts, overflow flag,
+//                  lastPos = pos; the last CTA publishes the build to status
+#include "cr_launch.h"
+#include "cr_tile.cuh"
+
+namespace cr {
+
+__device__ __forceinline__ int cell_coord(double x, double L, double invL, int nc) {
+  double w = x - L * floor(x * invL);          // wrap into [0, L]
+  int c = (int)(w * (nc * invL));
+  return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+}
+
+__global__ void k_cell_count(const __grid_constant__ SysParams p, int ncx, int ncy, const double2* pos, int* cell_of,
+                             int* slot, int* cell_cnt) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < p.nv) {
+    const double2 x = pos[v];
+    const int cx = cell_coord(x.x, p.lx, p.inv_lx, ncx);
+    const int cy = cell_coord(x.y, p.ly, p.inv_ly, ncy);
+    const int c = cy * ncx + cx;
+    cell_of[v] = c;
+    slot[v] = atomicAdd(cell_cnt + c, 1);
+  }
+}
+
+// One CTA of 1024 threads: chunked exclusive scan over ncells counts.
+__global__ void __launch_bounds__(1024) k_cell_scan(int ncells, int* cell_cnt, int* cell_start) {
+  __shared__ int s_tot[1024];
+  const int t = threadIdx.x;
+  const int chunk = (ncells + 1023) / 1024;
+  const int b = t * chunk, e = min(ncells, b + chunk);
+  int sum = 0;
+  for (int c = b; c < e; c++) sum += cell_cnt[c];
+  s_tot[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    int y = (t >= off) ? s_tot[t - off] : 0;
+    __syncthreads();
+    s_tot[t] += y;
+    __syncthreads();
+  }
+  int run = s_tot[t] - sum;  // exclusive prefix of this chunk
+  for (int c = b; c < e; c++) {
+    const int n = cell_cnt[c];
+    cell_start[c] = run;
+    run += n;
+    cell_cnt[c] = 0;
+  }
+  if (t == 1023) cell_start[ncells] = s_tot[1023];
+}
+
+__global__ void k_cell_fill(int nv, const int* cell_of, const int* slot, const int* cell_start, int* cell_vid) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nv) cell_vid[cell_start[cell_of[v]] + slot[v]] = v;
+}
+
+__global__ void k_cell_sort(int ncells, const int* cell_start, int* cell_vid, const double2* pos, const double* rad,
+                            const int* ring_of, double2* cell_pos, double* cell_rad, int* cell_ring) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncells) {
+    const int b = cell_start[c], e = cell_start[c + 1];
+    for (int i = b + 1; i < e; i++) {  // insertion sort: cells hold a handful of vertices
+      const int key = cell_vid[i];
+      int j = i - 1;
+      while (j >= b && cell_vid[j] > key) {
+        cell_vid[j + 1] = cell_vid[j];
+        j--;
+      }
+      cell_vid[j + 1] = key;
+    }
+    for (int i = b; i < e; i++) {
+      const int v = cell_vid[i];
+      cell_pos[i] = pos[v];
+      cell_rad[i] = rad[v];
+      cell_ring[i] = ring_of[v];
+    }
+  }
+}
+
+__device__ __forceinline__ bool is_neighbor(const SysParams& p, double2 xi, double2 xj, double rsum, double cut) {
+  // -calcOverlap(thisPos, otherPos, radSum) < cutDistance (include/cudaKernel.cuh:1752)
+  const double d = dist_of(pbc2(p, xi, xj));
+  return -(1.0 - d / rsum) < cut;
+}
+
+__device__ __forceinline__ void publish_build(const NbrArgs& n, int my_max, int my_overflow) {
+  DevStatus* st = n.status;
+  if (my_overflow) atomicOr(&st->overflow, 1);
+  if (my_max > 0) atomicMax(&st->max_count, my_max);
+  if (is_last_block(st)) {
+    if (threadIdx.x == 0) {
+      __threadfence();
+      if (st->max_count > st->max_ever) st->max_ever = st->max_count;
+      if (st->abort) {
+        // an earlier op of this sequence failed; leave its state alone
+      } else if (st->overflow) {
+        st->abort = 1;
+      } else {
+        st->rebuild = 0;
+        st->update_count += 1;
+        if (n.count_op) st->ops_done += 1;
+      }
+      st->done_ctr = 0;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_nbr_cells(const __grid_constant__ SysParams p, int ncx, int ncy,
+                                                   const __grid_constant__ NbrArgs n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int cnt = 0;
+  if (i < p.nv) {
+    const double2 xi = n.pos[i];
+    const double ri = n.rad[i];
+    const int ring = n.ring_of[i];
+    const int c = n.cell_of[i];
+    const int cx = c % ncx, cy = c / ncx;
+    for (int dy = -1; dy <= 1; dy++) {
+      int yy = cy + dy;
+      yy += (yy < 0) ? ncy : 0;
+      yy -= (yy >= ncy) ? ncy : 0;
+      for (int dx = -1; dx <= 1; dx++) {
+        int xx = cx + dx;
+        xx += (xx < 0) ? ncx : 0;
+        xx -= (xx >= ncx) ? ncx : 0;
+        const int cc = yy * ncx + xx;
+        const int b = n.cell_start[cc], e = n.cell_start[cc + 1];
+        for (int k = b; k < e; k++) {
+          if (n.cell_ring[k] == ring) continue;
+          if (is_neighbor(p, xi, n.cell_pos[k], ri + n.cell_rad[k], n.cut_distance)) {
+            if (cnt < n.cap) n.nbr[(size_t)cnt * p.nv + i] = n.cell_vid[k];
+            cnt++;
+          }
+        }
+      }
+    }
+    n.nbr_cnt[i] = cnt;
+    n.last_pos[i] = xi;
+  }
+  // CTA max and overflow, then publish
+  int m = cnt;
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ int s_max[8];
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  int bm = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) bm = max(bm, s_max[w]);
+  publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap);
+}
+
+// Brute force for boxes with fewer than three cells per side.
+__global__ void __launch_bounds__(256) k_nbr_brute(const __grid_constant__ SysParams p,
+                                                   const __grid_constant__ NbrArgs n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int cnt = 0;
+  if (i < p.nv) {
+    const double2 xi = n.pos[i];
+    const double ri = n.rad[i];
+    const int ring = n.ring_of[i];
+    for (int j = 0; j < p.nv; j++) {
+      if (n.ring_of[j] == ring) continue;
+      if (is_neighbor(p, xi, n.pos[j], ri + n.rad[j], n.cut_distance)) {
+        if (cnt < n.cap) n.nbr[(size_t)cnt * p.nv + i] = j;
+        cnt++;
+      }
+    }
+    n.nbr_cnt[i] = cnt;
+    n.last_pos[i] = xi;
+  }
+  int m = cnt;
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  __shared__ int s_max[8];
+  if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+  __syncthreads();
+  int bm = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) bm = max(bm, s_max[w]);
+  publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap);
+}
+
+// The build skips itself when an earlier op aborted the sequence.
+__global__ void k_nbr_guard_reset(DevStatus* st) {
+  if (threadIdx.x == 0) {
+    st->overflow = 0;
+    st->max_count = 0;
+  }
+}
+
+void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g, const NbrArgs& n) {
+  const int nb = (p.nv + 255) / 256;
+  k_nbr_guard_reset<<<1, 32, 0, stream>>>(n.status);
+  if (g.ncx >= 3 && g.ncy >= 3) {
+    const int ncells = g.ncx * g.ncy;
+    k_cell_count<<<nb, 256, 0, stream>>>(p, g.ncx, g.ncy, n.pos, n.cell_of, n.slot, n.cell_cnt);
+    k_cell_scan<<<1, 1024, 0, stream>>>(ncells, n.cell_cnt, n.cell_start);
+    k_cell_fill<<<nb, 256, 0, stream>>>(p.nv, n.cell_of, n.slot, n.cell_start, n.cell_vid);
+    k_cell_sort<<<(ncells + 255) / 256, 256, 0, stream>>>(ncells, n.cell_start, n.cell_vid, n.pos, n.rad, n.ring_of,
+                                                          n.cell_pos, n.cell_rad, n.cell_ring);
+    k_nbr_cells<<<nb, 256, 0, stream>>>(p, g.ncx, g.ncy, n);
+  } else {
+    k_nbr_brute<<<nb, 256, 0, stream>>>(p, n);
+  }
+}
+
+}  // namespace cr

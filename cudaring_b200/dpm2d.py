@@ -1,0 +1,234 @@
+"""``DPM2D``: the reference's model API (include/DPM2D.h) over libcudaring.
+
+Method names, argument meaning and units follow farceri/cudaRing's ``DPM2D``
+class so code written against it reads the same; every call goes through the
+C ABI in include/cudaring.h.  Host arrays are numpy float64 / int64 in the
+reference's layout (AoS ``[x0, y0, x1, y1, ...]``).  Loop methods take an
+optional step count (the reference advances one step per call).
+
+Errors raise :class:`CudaRingError` with the library's status and message
+(the reference prints and carries on; a drop-in that silently continues on a
+bad size would hide the same bugs).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import CudaRingError, lib
+
+
+class simControl:
+    """simControlStruct enums (include/DPM2D.h:22-32)."""
+
+    class potentialEnum:
+        harmonic, lennardJones, adhesive, wca = 0, 1, 2, 3
+
+    class interactionEnum:
+        vertexVertex, vertexSmooth, cellSmooth, all = 0, 1, 2, 3
+
+    class monomerEnum:
+        harmonic, FENE = 0, 1
+
+    class particleEnum:
+        passive, active, activeShape = 0, 1, 2
+
+    class noiseEnum:
+        langevin, baoab, brownian, drivenBrownian = 0, 1, 2, 3
+
+    class shapeEnum:
+        deformable, rigid = 0, 1
+
+    class geometryEnum:
+        normal, fixedBox, fixedSides, roundBox = 0, 1, 2, 3
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class DPM2D:
+    """One periodic 2-D system of ring polymers on the current CUDA device."""
+
+    def __init__(self, numVertexInParticleList):
+        self._L = lib()
+        nvl = np.ascontiguousarray(numVertexInParticleList, dtype=np.int64)
+        h = C.c_void_p()
+        rc = self._L.cr_create(len(nvl), nvl.ctypes.data, C.byref(h))
+        if rc != 0:
+            raise CudaRingError("cr_create", rc, "context creation failed")
+        self._h = h
+        self.numVertexInParticleList = nvl
+        self.numParticles = int(len(nvl))
+        self.numVertices = int(nvl.sum())
+
+    # ------------------------------------------------------------ plumbing
+    def _call(self, name, *args):
+        rc = getattr(self._L, name)(self._h, *args)
+        if rc != 0:
+            msg = self._L.cr_last_error(self._h)
+            raise CudaRingError(name, rc, msg.decode() if msg else "")
+
+    def _get(self, name, n, dtype=np.float64):
+        out = np.empty(n, dtype=dtype)
+        self._call(name, out.ctypes.data)
+        return out
+
+    def _scalar(self, name):
+        out = C.c_double()
+        self._call(name, C.byref(out))
+        return out.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.cr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -------------------------------------------------------------- switches
+    def setPotentialType(self, v): self._call("cr_set_potential_type", int(v))
+    def setInteractionType(self, v): self._call("cr_set_interaction_type", int(v))
+    def setMonomerType(self, v): self._call("cr_set_monomer_type", int(v))
+    def setParticleType(self, v): self._call("cr_set_particle_type", int(v))
+    def setNoiseType(self, v): self._call("cr_set_noise_type", int(v))
+    def setShapeType(self, v): self._call("cr_set_shape_type", int(v))
+    def setGeometryType(self, v): self._call("cr_set_geometry_type", int(v))
+
+    # ------------------------------------------------------------ parameters
+    def setBoxSize(self, box): self._call("cr_set_box_size", _f64(box).ctypes.data)
+    def getBoxSize(self): return self._get("cr_get_box_size", 2)
+    def setEnergyCosts(self, ea, el, eb, ec): self._call("cr_set_energy_costs", ea, el, eb, ec)
+    def setLJcutoff(self, c): self._call("cr_set_lj_cutoff", c)
+    def setAttractionConstants(self, l1, l2): self._call("cr_set_attraction_constants", l1, l2)
+    def setFENEconstants(self, stiff, ext): self._call("cr_set_fene_constants", stiff, ext)
+
+    def setTimeStep(self, dt):
+        self._call("cr_set_time_step", dt)
+        return dt
+
+    def setSelfPropulsionParams(self, driving, taup): self._call("cr_set_self_propulsion_params", driving, taup)
+    def setSeed(self, seed): self._call("cr_set_seed", C.c_ulonglong(seed))
+
+    # ----------------------------------------------------------------- state
+    def setVertexPositions(self, a): self._call("cr_set_vertex_positions", _f64(a).ctypes.data)
+    def getVertexPositions(self): return self._get("cr_get_vertex_positions", 2 * self.numVertices)
+    def setVertexVelocities(self, a): self._call("cr_set_vertex_velocities", _f64(a).ctypes.data)
+    def getVertexVelocities(self): return self._get("cr_get_vertex_velocities", 2 * self.numVertices)
+    def setVertexForces(self, a): self._call("cr_set_vertex_forces", _f64(a).ctypes.data)
+    def getVertexForces(self): return self._get("cr_get_vertex_forces", 2 * self.numVertices)
+    def getVertexEnergies(self): return self._get("cr_get_vertex_energies", self.numVertices)
+    def getParticleEnergies(self): return self._get("cr_get_particle_energies", self.numParticles)
+    def setVertexRadii(self, a): self._call("cr_set_vertex_radii", _f64(a).ctypes.data)
+    def getVertexRadii(self): return self._get("cr_get_vertex_radii", self.numVertices)
+    def setRestAreas(self, a): self._call("cr_set_rest_areas", _f64(a).ctypes.data)
+    def getRestAreas(self): return self._get("cr_get_rest_areas", self.numParticles)
+    def setRestLengths(self, a): self._call("cr_set_rest_lengths", _f64(a).ctypes.data)
+    def getRestLengths(self): return self._get("cr_get_rest_lengths", self.numVertices)
+    def setRestAngles(self, a): self._call("cr_set_rest_angles", _f64(a).ctypes.data)
+    def getAreas(self): return self._get("cr_get_areas", self.numParticles)
+    def getPerimeters(self): return self._get("cr_get_perimeters", self.numParticles)
+    def getSegmentLengths(self): return self._get("cr_get_segment_lengths", self.numVertices)
+    def getSegmentAngles(self): return self._get("cr_get_segment_angles", self.numVertices)
+    def calcParticleShape(self): self._call("cr_calc_particle_shape")
+    def calcParticlePositions(self): self._call("cr_calc_particle_positions")
+    def getParticlePositions(self): return self._get("cr_get_particle_positions", 2 * self.numParticles)
+    def setParticlePositions(self, a): self._call("cr_set_particle_positions", _f64(a).ctypes.data)
+
+    # ------------------------------------------------------------ neighbours
+    def setDisplacementCutoff(self, cutoff, size):
+        out = C.c_double()
+        self._call("cr_set_displacement_cutoff", cutoff, size, C.byref(out))
+        return out.value
+
+    def calcNeighborList(self, cutDistance): self._call("cr_calc_neighbor_list", cutDistance)
+    calcNeighbors = calcNeighborList
+    def checkNeighbors(self): self._call("cr_check_neighbors")
+    def resetLastPositions(self): self._call("cr_reset_last_positions")
+
+    def getNeighborListSize(self):
+        out = C.c_long()
+        self._call("cr_get_neighbor_list_size", C.byref(out))
+        return out.value
+
+    def getNeighbors(self):
+        return self._get("cr_get_neighbors", self.numVertices * self.getNeighborListSize(), np.int64)
+
+    def getMaxNeighborList(self): return self._get("cr_get_max_neighbor_list", self.numVertices, np.int64)
+
+    def getUpdateCount(self):
+        out = C.c_long()
+        self._call("cr_get_update_count", C.byref(out))
+        return out.value
+
+    def resetUpdateCount(self): self._call("cr_reset_update_count")
+
+    # ---------------------------------------------------- forces, reductions
+    def calcForceEnergy(self): self._call("cr_calc_force_energy")
+    def getPotentialEnergy(self): return self._scalar("cr_get_potential_energy")
+    def getKineticEnergy(self): return self._scalar("cr_get_kinetic_energy")
+    def getEnergy(self): return self._scalar("cr_get_energy")
+    def getTemperature(self): return self._scalar("cr_get_temperature")
+    def getMaxUnbalancedForce(self): return self._scalar("cr_get_max_unbalanced_force")
+    def getTotalForceMagnitude(self): return self._scalar("cr_get_total_force_magnitude")
+    def getPhi(self): return self._scalar("cr_get_phi")
+    def getPreferredPhi(self): return self._scalar("cr_get_preferred_phi")
+    def getMeanVertexRadius(self): return self._scalar("cr_get_mean_vertex_radius")
+    def getMeanParticleSize(self): return self._scalar("cr_get_mean_particle_size")
+    def scaleVertices(self, scale): self._call("cr_scale_vertices", scale)
+
+    # ------------------------------------------------------------ integrators
+    def initNVE(self, T, readState=False): self._call("cr_init_nve", T, int(bool(readState)))
+    def NVELoop(self, nsteps=1): self._call("cr_nve_loop", int(nsteps))
+    def initLangevin(self, T, gamma, readState=False): self._call("cr_init_langevin", T, gamma, int(bool(readState)))
+    def langevinLoop(self, nsteps=1): self._call("cr_langevin_loop", int(nsteps))
+
+    def initFIRE(self, FIREparams, minStep, numStep, numDOF):
+        self._call("cr_init_fire", _f64(FIREparams).ctypes.data, int(minStep), int(numStep), int(numDOF))
+
+    def vertexFIRELoop(self, nsteps=1): self._call("cr_vertex_fire_loop", int(nsteps))
+
+    def minimizeFIRE(self, tol, maxIter):
+        it, f = C.c_long(), C.c_double()
+        self._call("cr_fire_minimize", tol, int(maxIter), C.byref(it), C.byref(f))
+        return it.value, f.value
+
+    def getFIREState(self): return self._get("cr_get_fire_state", 3)
+
+    def getLaunchCount(self):
+        out = C.c_longlong()
+        self._call("cr_get_launch_count", C.byref(out))
+        return out.value
+
+    # -------------------------------------------------------------- helpers
+    @classmethod
+    def from_packing(cls, pk, potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01,
+                     ec=1.0, LJcutoff=2.5, l1=0.0, l2=0.0, dt=None, **_):
+        """Context holding a :class:`cudaring_b200.synth.Packing` with the given parameters."""
+        d = cls(pk.nv_list)
+        d.setBoxSize(pk.box)
+        d.setPotentialType(getattr(simControl.potentialEnum, potential))
+        d.setInteractionType(getattr(simControl.interactionEnum, interaction))
+        d.setEnergyCosts(ea, el, eb, ec)
+        d.setLJcutoff(LJcutoff)
+        d.setAttractionConstants(l1, l2)
+        if dt is not None:
+            d.setTimeStep(dt)
+        d.setVertexRadii(pk.rad)
+        d.setRestAreas(pk.a0)
+        d.setRestLengths(pk.l0)
+        d.setRestAngles(pk.theta0)
+        d.setVertexPositions(pk.pos)
+        d.setVertexVelocities(pk.vel)
+        return d

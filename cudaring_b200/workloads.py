@@ -1,0 +1,111 @@
+"""Prepared benchmark states built with the library itself.
+
+A dense packing cannot be placed directly: rings are first placed without
+overlap at low packing fraction, then compressed the way the reference's
+compressFIRE driver does it (compressFIRE.cpp:101-205): scale the rings about
+their centroids with ``scaleVertices(sqrt(phi_new / phi))`` (src/DPM2D.cu:1802-1811)
+and relax with FIRE after every step.  At the end the whole system (box,
+positions, radii, rest lengths, rest areas) is rescaled uniformly so the ring
+sizes are the nominal ones again; a uniform rescaling leaves the packing
+fraction unchanged.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import synth
+from .dpm2d import DPM2D
+
+
+def lattice_packing(nv_list, a0_list, calA0, seed: int, spacing_scale: float = 1.02) -> synth.Packing:
+    """Rings on a triangular lattice of discs (no overlap), random site order."""
+    nv_list = np.asarray(nv_list, dtype=np.int64)
+    a0 = np.asarray(a0_list, dtype=np.float64)
+    n = len(nv_list)
+    ring_r = np.sqrt(2.0 * a0 / (nv_list * np.sin(2.0 * np.pi / nv_list)))
+    rads = np.array([synth.ring_rest_shape(int(k), float(a), calA0)[2] for k, a in zip(nv_list, a0)])
+    a = 2.0 * float((ring_r + rads).max()) * spacing_scale
+    nx = int(math.ceil(math.sqrt(n * 2.0 / math.sqrt(3.0))))
+    ny = int(math.ceil(n / nx))
+    ny += ny % 2
+    rng = np.random.Generator(np.random.MT19937(seed))
+    sites = rng.permutation(nx * ny)[:n]
+    ix, iy = sites % nx, sites // nx
+    centres = np.stack([(ix + 0.5 * (iy % 2)) * a, iy * a * math.sqrt(3.0) / 2.0], axis=1)
+    box = np.array([nx * a, ny * a * math.sqrt(3.0) / 2.0])
+    pk = synth.make_packing(nv_list, a0, calA0, 0.5, seed=seed, placement="uniform")
+    # re-place vertices around the lattice centres (make_packing's uniform centres are discarded)
+    pid = np.repeat(np.arange(n), nv_list)
+    offs = pk.pos.reshape(-1, 2) - pk.centres[pid]
+    pos = offs + centres[pid]
+    pk.pos = pos.reshape(-1).copy()
+    pk.centres = centres
+    pk.box = box
+    pk.meta["placement"] = "lattice"
+    return pk
+
+
+def compress(d: DPM2D, phi0: float, phi1: float, dphi: float = 0.05, fire_dt: float = 2e-3,
+             tol_mid: float = 1e-2, tol_end: float = 1e-4, max_iter: int = 20000) -> dict:
+    """Grow rings from preferred packing fraction phi0 to phi1 with FIRE relaxation."""
+    phi = phi0
+    iters = 0
+    cutoff_ = 0.5
+    while True:
+        size = 2.0 * d.getMeanVertexRadius()
+        cut = d.setDisplacementCutoff(cutoff_, size)
+        d.calcNeighborList(cut)
+        d.resetLastPositions()
+        d.calcForceEnergy()
+        d.initFIRE([0.2, 0.5, 1.1, 0.99, fire_dt, 10 * fire_dt, 0.2], 20, 0, d.numVertices)
+        it, fmax = d.minimizeFIRE(tol_end if phi >= phi1 else tol_mid, max_iter)
+        iters += it
+        if phi >= phi1:
+            break
+        new = min(phi1, phi + dphi)
+        d.calcParticlePositions()
+        d.scaleVertices(math.sqrt(new / phi))
+        phi = new
+    return {"fire_iterations": iters, "max_force": fmax}
+
+
+def rescale_lengths(d: DPM2D, f: float) -> None:
+    """Multiply every length of the system by f (areas by f^2)."""
+    d.setBoxSize(d.getBoxSize() * f)
+    d.setVertexPositions(d.getVertexPositions() * f)
+    d.setVertexRadii(d.getVertexRadii() * f)
+    d.setRestLengths(d.getRestLengths() * f)
+    d.setRestAreas(d.getRestAreas() * f * f)
+
+
+def prepared_deformable(index: int = 1, rings: int | None = None, seed: int = 20261203, phi_start: float = 0.40,
+                        placement: str | None = None) -> tuple[DPM2D, dict]:
+    """A relaxed packing of deformable-ring config ``index`` at its target phi.
+
+    index 1: 1024 rings nv 32/45, smooth vertex-segment LJ (rc 2.5), calA0
+    1.05, phi 0.85.  ``rings`` scales the ring count (even small/large split).
+    """
+    c = synth.workload_config(index, rings)
+    n = len(c["nv"])
+    if placement is None:
+        placement = "rsa" if n <= 4096 else "lattice"
+    if placement == "lattice":
+        pk = lattice_packing(c["nv"], c["a0"], c["calA0"], seed)
+        phi_start = synth.preferred_phi(pk.nv_list, pk.a0, pk.rad, pk.box)
+    else:
+        pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], phi_start, seed=seed, placement="rsa")
+    kw = {k: c[k] for k in ("potential", "interaction", "ea", "el", "eb", "ec", "dt") if k in c}
+    if "LJcutoff" in c:
+        kw["LJcutoff"] = c["LJcutoff"]
+    d = DPM2D.from_packing(pk, **kw)
+    info = compress(d, phi_start, c["phi"])
+    rescale_lengths(d, math.sqrt(phi_start / c["phi"]))
+    size = 2.0 * d.getMeanVertexRadius()
+    cut = d.setDisplacementCutoff(0.5, size)
+    d.calcNeighborList(cut)
+    d.resetLastPositions()
+    d.calcForceEnergy()
+    info.update(config=c, placement=placement, phi=d.getPreferredPhi(), cut_distance=cut, seed=seed)
+    return d, info

@@ -1,0 +1,217 @@
+/* cudaring.h -- C ABI of the B200-native cudaRing hot path (libcudaring.so).
+ *
+ * One `cr_ctx` is one 2-D periodic system of deformable (or rigid) ring
+ * polymers, owned on one GPU.  Each entry point replaces the `DPM2D` /
+ * `SimInterface` / `FIRE` member function of the reference (farceri/cudaRing)
+ * cited beside it (file:line within that project), keeps its argument
+ * meaning, and adds an `int` status return (CR_OK on success).  Host arrays
+ * use the reference's layout: AoS [x0,y0,x1,y1,...] float64 for per-vertex
+ * vectors, ring-contiguous counter-clockwise vertex order, int64 (`long`)
+ * indices.  Setters copy synchronously; loop functions are stream-ordered on
+ * the context's own stream and synchronise once before returning.
+ *
+ * Differences from the reference kept deliberately, all at the boundary:
+ *   - loop functions take a step count (the reference advances one step per
+ *     call); `cr_nve_loop(ctx, 1)` is `DPM2D::NVELoop()`;
+ *   - the reference keeps one live model per process in __constant__ memory;
+ *     any number of contexts may coexist here;
+ *   - random numbers come from a counter-based Philox4x32-10 stream keyed by
+ *     `cr_set_seed` instead of Thrust's engine reseeded from lrand48().
+ */
+#ifndef CUDARING_H
+#define CUDARING_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cr_ctx cr_ctx;
+
+/* Status codes. */
+enum {
+  CR_OK = 0,
+  CR_EINVAL = 1,        /* bad argument (size mismatch, unknown enum, NULL) */
+  CR_ENOMEM = 2,        /* device or host allocation failed */
+  CR_ECUDA = 3,         /* CUDA runtime error; see cr_last_error */
+  CR_ENONFINITE = 4,    /* a NaN/Inf force or position was produced */
+  CR_ETIMEOUT = 5,      /* a bounded device wait ran out */
+  CR_ENBR_OVERFLOW = 6, /* neighbour capacity exceeded and could not grow */
+  CR_ESTATE = 7,        /* call out of order (e.g. loop before init) */
+  CR_ENOTSUP = 8        /* option the reference has but this build does not run */
+};
+
+/* simControlStruct enums (include/DPM2D.h:22-32), same numbering. */
+enum { CR_POTENTIAL_HARMONIC = 0, CR_POTENTIAL_LENNARD_JONES = 1, CR_POTENTIAL_ADHESIVE = 2, CR_POTENTIAL_WCA = 3 };
+enum { CR_INTERACTION_VERTEX_VERTEX = 0, CR_INTERACTION_VERTEX_SMOOTH = 1, CR_INTERACTION_CELL_SMOOTH = 2,
+       CR_INTERACTION_ALL = 3 };
+enum { CR_MONOMER_HARMONIC = 0, CR_MONOMER_FENE = 1 };
+enum { CR_PARTICLE_PASSIVE = 0, CR_PARTICLE_ACTIVE = 1, CR_PARTICLE_ACTIVE_SHAPE = 2 };
+enum { CR_SHAPE_DEFORMABLE = 0, CR_SHAPE_RIGID = 1 };
+enum { CR_NOISE_LANGEVIN = 0, CR_NOISE_BAOAB = 1, CR_NOISE_BROWNIAN = 2, CR_NOISE_DRIVEN_BROWNIAN = 3 };
+enum { CR_GEOMETRY_NORMAL = 0, CR_GEOMETRY_FIXED_BOX = 1, CR_GEOMETRY_FIXED_SIDES = 2, CR_GEOMETRY_ROUND_BOX = 3 };
+
+/* ---- lifecycle -------------------------------------------------------- */
+
+/* DPM2D::DPM2D (include/DPM2D.h:47) + setNumVertexInParticleList (:267) +
+ * initParticleIdList (:219): numVertexInParticleList[numParticles] sets the
+ * ring sizes; the context selects the current CUDA device. */
+int cr_create(long numParticles, const long* numVertexInParticleList, cr_ctx** out);
+int cr_destroy(cr_ctx* ctx);
+/* Message of the last failing call on this context ("" if none). */
+const char* cr_last_error(const cr_ctx* ctx);
+/* DPM2D::getNumVertices (include/DPM2D.h:262) */
+int cr_get_num_vertices(const cr_ctx* ctx, long* out);
+int cr_get_num_particles(const cr_ctx* ctx, long* out);
+
+/* ---- control switches (include/DPM2D.h:231-249) -------------------------- */
+int cr_set_potential_type(cr_ctx* ctx, int potentialType);
+int cr_set_interaction_type(cr_ctx* ctx, int interactionType);
+int cr_set_monomer_type(cr_ctx* ctx, int monomerType);
+int cr_set_particle_type(cr_ctx* ctx, int particleType);
+int cr_set_noise_type(cr_ctx* ctx, int noiseType);
+int cr_set_shape_type(cr_ctx* ctx, int shapeType);
+/* Only CR_GEOMETRY_NORMAL (periodic) is run; walls return CR_ENOTSUP. */
+int cr_set_geometry_type(cr_ctx* ctx, int geometryType);
+
+/* ---- parameters ------------------------------------------------------- */
+/* DPM2D::setBoxSize (include/DPM2D.h:275): boxSize[2] */
+int cr_set_box_size(cr_ctx* ctx, const double* boxSize);
+int cr_get_box_size(const cr_ctx* ctx, double* boxSize);
+/* DPM2D::setEnergyCosts (include/DPM2D.h:525) */
+int cr_set_energy_costs(cr_ctx* ctx, double ea, double el, double eb, double ec);
+/* DPM2D::setLJcutoff (include/DPM2D.h:539): LJecut/LJfshift use the ec set
+ * at the time of this call, as in the reference (src/DPM2D.cu:1923-1932). */
+int cr_set_lj_cutoff(cr_ctx* ctx, double LJcutoff);
+/* DPM2D::setAttractionConstants (include/DPM2D.h:535) */
+int cr_set_attraction_constants(cr_ctx* ctx, double l1, double l2);
+/* DPM2D::setFENEconstants (include/DPM2D.h:541) */
+int cr_set_fene_constants(cr_ctx* ctx, double stiff, double ext);
+/* DPM2D::setTimeStep (include/DPM2D.h:545) */
+int cr_set_time_step(cr_ctx* ctx, double dt);
+/* DPM2D::setSelfPropulsionParams (include/DPM2D.h:527) */
+int cr_set_self_propulsion_params(cr_ctx* ctx, double driving, double taup);
+/* Seed of the Philox stream used by every stochastic update. */
+int cr_set_seed(cr_ctx* ctx, unsigned long long seed);
+
+/* ---- state upload / download (host arrays, reference layout) ----------- */
+/* DPM2D::setVertexPositions / getVertexPositions (include/DPM2D.h:357-358): pos[2 Nv] */
+int cr_set_vertex_positions(cr_ctx* ctx, const double* pos);
+int cr_get_vertex_positions(const cr_ctx* ctx, double* pos);
+/* DPM2D::setVertexVelocities / getVertexVelocities (include/DPM2D.h:366-367) */
+int cr_set_vertex_velocities(cr_ctx* ctx, const double* vel);
+int cr_get_vertex_velocities(const cr_ctx* ctx, double* vel);
+/* DPM2D::getVertexForces (include/DPM2D.h:370) */
+int cr_get_vertex_forces(const cr_ctx* ctx, double* force);
+int cr_set_vertex_forces(cr_ctx* ctx, const double* force);
+/* Per-vertex energies (shape + vertex-vertex half-pair terms), d_energy. */
+int cr_get_vertex_energies(const cr_ctx* ctx, double* energy);
+/* DPM2D::getParticleEnergies (include/DPM2D.h:345): smooth-interaction ring energies */
+int cr_get_particle_energies(const cr_ctx* ctx, double* pEnergy);
+/* DPM2D::setVertexRadii (include/DPM2D.h:283) */
+int cr_set_vertex_radii(cr_ctx* ctx, const double* rad);
+int cr_get_vertex_radii(const cr_ctx* ctx, double* rad);
+/* DPM2D::setRestAreas / setRestLengths / setRestAngles (include/DPM2D.h:286-292) */
+int cr_set_rest_areas(cr_ctx* ctx, const double* a0);
+int cr_get_rest_areas(const cr_ctx* ctx, double* a0);
+int cr_set_rest_lengths(cr_ctx* ctx, const double* l0);
+int cr_get_rest_lengths(const cr_ctx* ctx, double* l0);
+int cr_set_rest_angles(cr_ctx* ctx, const double* theta0);
+/* DPM2D::getAreas / getPerimeters / getSegmentLengths / getSegmentAngles
+ * (include/DPM2D.h:295-302), as of the last force evaluation. */
+int cr_get_areas(const cr_ctx* ctx, double* area);
+int cr_get_perimeters(const cr_ctx* ctx, double* perimeter);
+int cr_get_segment_lengths(const cr_ctx* ctx, double* length);
+int cr_get_segment_angles(const cr_ctx* ctx, double* theta);
+/* DPM2D::calcParticlePositions + getParticlePositions (include/DPM2D.h:321, 331) */
+int cr_calc_particle_positions(cr_ctx* ctx);
+int cr_get_particle_positions(const cr_ctx* ctx, double* particlePos);
+int cr_set_particle_positions(cr_ctx* ctx, const double* particlePos);
+/* DPM2D::calcParticleShape (include/DPM2D.h:319) */
+int cr_calc_particle_shape(cr_ctx* ctx);
+
+/* ---- neighbours (src/DPM2D.cu:1300-1423, 3479-3518) -------------------- */
+/* DPM2D::setDisplacementCutoff (include/DPM2D.h:447): returns cutDistance. */
+int cr_set_displacement_cutoff(cr_ctx* ctx, double cutoff, double size, double* cutDistance);
+/* DPM2D::calcNeighborList / calcNeighbors (include/DPM2D.h:638-640): builds
+ * the list {j in another ring : d_ij/(r_i+r_j) - 1 < cutDistance} with a
+ * device cell list; the set equals the reference's brute-force scan. */
+int cr_calc_neighbor_list(cr_ctx* ctx, double cutDistance);
+/* DPM2D::checkNeighbors (include/DPM2D.h:459): rebuild when any vertex moved
+ * more than cutoff/3 since the last rebuild. */
+int cr_check_neighbors(cr_ctx* ctx);
+/* DPM2D::resetLastPositions (include/DPM2D.h:360) */
+int cr_reset_last_positions(cr_ctx* ctx);
+/* The reference's neighborListSize (power of two, only grows). */
+int cr_get_neighbor_list_size(const cr_ctx* ctx, long* listSize);
+/* DPM2D::getNeighbors (include/DPM2D.h:387): out[Nv * listSize] row-major,
+ * ascending neighbour ids, padded with -1. */
+int cr_get_neighbors(const cr_ctx* ctx, long* out);
+/* DPM2D::getMaxNeighborList (include/DPM2D.h:385): out[Nv] */
+int cr_get_max_neighbor_list(const cr_ctx* ctx, long* out);
+/* DPM2D::getUpdateCount / resetUpdateCount (include/DPM2D.h:449-451) */
+int cr_get_update_count(const cr_ctx* ctx, long* out);
+int cr_reset_update_count(cr_ctx* ctx);
+
+/* ---- forces and reductions --------------------------------------------- */
+/* DPM2D::calcForceEnergy (include/DPM2D.h:547): shape + interaction (+ self
+ * propulsion for active rings), overwriting forces and energies. */
+int cr_calc_force_energy(cr_ctx* ctx);
+/* DPM2D::getPotentialEnergy / getKineticEnergy / getEnergy / getTemperature
+ * (include/DPM2D.h:403-409) */
+int cr_get_potential_energy(cr_ctx* ctx, double* out);
+int cr_get_kinetic_energy(cr_ctx* ctx, double* out);
+int cr_get_energy(cr_ctx* ctx, double* out);
+int cr_get_temperature(cr_ctx* ctx, double* out);
+/* DPM2D::getMaxUnbalancedForce / getTotalForceMagnitude (include/DPM2D.h:381-383) */
+int cr_get_max_unbalanced_force(cr_ctx* ctx, double* out);
+int cr_get_total_force_magnitude(cr_ctx* ctx, double* out);
+/* DPM2D::getPhi / getPreferredPhi (include/DPM2D.h:431-433) */
+int cr_get_phi(cr_ctx* ctx, double* out);
+int cr_get_preferred_phi(cr_ctx* ctx, double* out);
+/* DPM2D::getMeanVertexRadius / getMeanParticleSize (include/DPM2D.h:306-312) */
+int cr_get_mean_vertex_radius(cr_ctx* ctx, double* out);
+int cr_get_mean_particle_size(cr_ctx* ctx, double* out);
+/* DPM2D::scaleVertices (include/DPM2D.h:506): scales rings about their
+ * current centroids and multiplies a0 by scale^2, l0 and rad by scale. */
+int cr_scale_vertices(cr_ctx* ctx, double scale);
+
+/* ---- integrators (src/Simulator.cu, src/DPM2D.cu:3713-3775) ------------- */
+/* DPM2D::initNVE (include/DPM2D.h:684): readState != 0 keeps velocities;
+ * otherwise every vertex gets its ring's N(0, sqrt(T)) velocity
+ * (Langevin::injectKineticEnergy, src/Simulator.cu:32-52). */
+int cr_init_nve(cr_ctx* ctx, double T, int readState);
+/* DPM2D::NVELoop (include/DPM2D.h:686), nsteps times. */
+int cr_nve_loop(cr_ctx* ctx, long nsteps);
+/* DPM2D::initLangevin (include/DPM2D.h:680): the noise type selects
+ * Langevin, BAOAB, Brownian or driven Brownian (src/DPM2D.cu:3713-3753). */
+int cr_init_langevin(cr_ctx* ctx, double T, double gamma, int readState);
+/* DPM2D::langevinLoop (include/DPM2D.h:682), nsteps times. */
+int cr_langevin_loop(cr_ctx* ctx, long nsteps);
+
+/* ---- FIRE (src/FIRE.cu:29-41, 302-411) ---------------------------------- */
+/* DPM2D::initFIRE (include/DPM2D.h:665): params[7] = {a_start, f_dec, f_inc,
+ * f_a, dt, dt_max, a}. */
+int cr_init_fire(cr_ctx* ctx, const double* params, long minStep, long numStep, long numDOF);
+/* DPM2D::vertexFIRELoop (include/DPM2D.h:673), nsteps times. */
+int cr_vertex_fire_loop(cr_ctx* ctx, long nsteps);
+/* The driver loop of compressFIRE.cpp:109-117: FIRE iterations until
+ * getMaxUnbalancedForce() <= tol or maxIter iterations; reports both. */
+int cr_fire_minimize(cr_ctx* ctx, double tol, long maxIter, long* iterations, double* maxForce);
+/* FIRE scalars {dt, a, numStep} after the last iteration. */
+int cr_get_fire_state(cr_ctx* ctx, double* out3);
+
+/* ---- run statistics and measurement ------------------------------------ */
+/* Kernels this context has run since creation (direct launches, graph-node
+ * kernels per replay and the rebuild kernels of conditional nodes). */
+int cr_get_launch_count(const cr_ctx* ctx, long long* out);
+/* The context's CUDA stream (cudaStream_t), for recording timing events. */
+int cr_get_stream(const cr_ctx* ctx, void** out);
+/* Average device time of the fused step kernel (the integrator's force +
+ * update op) over `reps` back-to-back launches on scratch copies of the
+ * state, timed with CUDA events on the context stream; state is unchanged. */
+int cr_profile_step_kernel(cr_ctx* ctx, long reps, double* ms_per_launch);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUDARING_H */

@@ -1,0 +1,133 @@
+"""Oracle integrators: numpy restatements of the reference's step functions.
+
+TEST INFRASTRUCTURE ONLY.  Forces come from the C restatement (oracle.c);
+the updates restate:
+
+* ``NVE::integrate`` (src/Simulator.cu:206-212),
+* ``Langevin::integrate`` / ``updateThermalVel`` (src/Simulator.cu:23-30, 54-77),
+* ``BAOAB::integrate`` (src/Simulator.cu:112-144),
+* ``Brownian::integrate`` / ``DrivenBrownian`` (src/Simulator.cu:147-203),
+* ``FIRE::minimizerVertexLoop`` (src/FIRE.cu:302-411),
+* ``DPM2D::checkDisplacement`` with ``shift == false`` (src/DPM2D.cu:1390-1406).
+
+Noise is injected by a callable ``noise(step) -> (Np, 2)`` array so that the
+same draws can be fed to the reference kernels (oracle/_ref) and to this
+restatement; ``philox_noise`` reproduces the library's counter-based stream.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import System, normal2
+
+
+class OracleState:
+    def __init__(self, sys_: System, pk, cutoff_: float = 0.5, size_: float | None = None):
+        self.s = sys_
+        self.pos = pk.pos.copy()
+        self.vel = pk.vel.copy()
+        self.rad = pk.rad.copy()
+        self.a0 = pk.a0.copy()
+        self.l0 = pk.l0.copy()
+        self.theta0 = pk.theta0.copy()
+        size = 2 * self.rad.mean() if size_ is None else size_
+        self.cut_distance = sys_.cut_distance(cutoff_)
+        self.cutoff = cutoff_ * size
+        self.update_count = 0
+        self.rebuild()
+        self.out = None
+        self.forces()
+
+    def rebuild(self):
+        self.s.neighbor_list(self.pos, self.rad, self.cut_distance)
+        self.last_pos = self.pos.copy()
+
+    def check(self):
+        d = (self.pos - self.last_pos).reshape(-1, 2)
+        box = np.array([self.s.s.lx, self.s.s.ly])
+        d -= box * np.round(d / box)
+        if np.any(3 * np.sqrt((d * d).sum(1)) > self.cutoff):
+            self.rebuild()
+            self.update_count += 1
+
+    def forces(self):
+        self.out = self.s.force_energy(self.pos, self.rad, self.a0, self.l0, self.theta0)
+        self.force = self.out["force"]
+        return self.out
+
+    def ring_of(self):
+        return self.s.pid
+
+    # ---------------------------------------------------------------- steps
+    def nve_step(self, dt):
+        self.vel += 0.5 * dt * self.force
+        self.pos += dt * self.vel
+        self.check()
+        self.forces()
+        self.vel += 0.5 * dt * self.force
+
+    def langevin_step(self, dt, gamma, noise_amp, xi):
+        self.vel += 0.5 * dt * self.force
+        self.pos += dt * self.vel
+        self.check()
+        self.forces()
+        r = xi[self.s.pid].reshape(-1)
+        self.force = self.force + noise_amp * r - gamma * self.vel
+        self.vel += 0.5 * dt * self.force
+
+    def baoab_step(self, dt, gamma_factor, noise_amp, xi):
+        self.vel += 0.5 * dt * self.force
+        self.pos += 0.5 * dt * self.vel
+        self.vel = gamma_factor * self.vel + noise_amp * xi[self.s.pid].reshape(-1)
+        self.pos += 0.5 * dt * self.vel
+        self.check()
+        self.forces()
+        self.vel += 0.5 * dt * self.force
+
+    def brownian_step(self, dt, gamma, noise_amp, xi=None):
+        self.check()
+        self.forces()
+        if xi is None:
+            self.vel = self.force / gamma
+        else:
+            self.vel = (self.force + noise_amp * xi[self.s.pid].reshape(-1)) / gamma
+        self.pos += dt * self.vel
+
+
+class OracleFIRE:
+    """FIRE scalars + iteration (src/FIRE.cu:29-41, 338-411)."""
+
+    def __init__(self, params, min_step, num_step):
+        self.a_start, self.f_dec, self.f_inc, self.f_a, self.dt, self.dt_max, self.a = params
+        self.min_step = min_step
+        self.num_step = num_step
+
+    def iterate(self, st: OracleState):
+        p = float(np.dot(st.vel, st.force))
+        if p > 0:
+            self.num_step += 1
+            if self.num_step > self.min_step:
+                self.dt = min(self.dt * self.f_inc, self.dt_max)
+                self.a *= self.f_a
+        else:
+            self.num_step = 0
+            self.dt = max(self.dt * self.f_dec, self.dt_max / 10)
+            self.a = self.a_start
+            st.pos -= 0.5 * self.dt * st.vel
+            st.vel[:] = 0.0
+        st.vel += 0.5 * self.dt * st.force
+        vv = float(np.dot(st.vel, st.vel))
+        ff = float(np.dot(st.force, st.force))
+        if ff > 0:
+            st.vel = (1 - self.a) * st.vel + self.a * st.force * math.sqrt(vv / ff)
+        st.pos += self.dt * st.vel
+        st.check()
+        st.forces()
+        st.vel += 0.5 * self.dt * st.force
+
+
+def philox_noise(seed: int, stream: int, num_rings: int) -> np.ndarray:
+    """(Np, 2) standard normals of one Philox stream, one pair per ring."""
+    return np.stack([normal2(seed, stream, q) for q in range(num_rings)])

@@ -1,0 +1,199 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+The outputs are computed by oracle/_ref/libcrref.so -- farceri/cudaRing's own
+kernels (include/cudaKernel.cuh) compiled as host code by oracle/build_ref.sh
+-- on seeded inputs built with cudaring_b200.synth.  Inputs and outputs are
+stored together, so the tests do not depend on the generator staying
+bit-identical.  Run from the repository root, where the reference checkout
+is available:
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from cudaring_b200 import synth  # noqa: E402
+from oracle.integrators import philox_noise  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+# Force/energy/neighbour cases: (name, rings, potential, interaction, placement, phi, extra)
+FORCE_CASES = [
+    ("harmonic_vv_cfg0", dict(cfg=0), "harmonic", "vertexVertex", "uniform", 0.70, {}),
+    ("harmonic_smooth", dict(cfg=1, n=48), "harmonic", "vertexSmooth", "uniform", 0.80, {}),
+    ("lj_smooth", dict(cfg=1, n=64), "lennardJones", "vertexSmooth", "rsa", 0.40, {}),
+    ("lj_vv", dict(cfg=1, n=64), "lennardJones", "vertexVertex", "rsa", 0.40, {}),
+    ("wca_vv", dict(nv=24, n=64), "wca", "vertexVertex", "rsa", 0.40, {}),
+    ("wca_smooth", dict(nv=24, n=64), "wca", "vertexSmooth", "rsa", 0.40, {}),
+    ("adhesive_vv", dict(cfg=0), "adhesive", "vertexVertex", "uniform", 0.70, dict(l1=0.1, l2=0.3)),
+    ("adhesive_smooth", dict(cfg=0), "adhesive", "vertexSmooth", "uniform", 0.70, dict(l1=0.1, l2=0.3)),
+    ("fene_vv", dict(cfg=0), "harmonic", "vertexVertex", "uniform", 0.70, dict(monomer=1, stiff=1.0, ext=1.5)),
+]
+
+FIELDS = {"pos": 0, "vel": 1, "force": 2, "energy": 3, "p_energy": 4, "area": 5, "perimeter": 6,
+          "theta": 7, "length": 8, "ppos": 9}
+
+
+def packing_for(spec, phi, placement, seed):
+    if "cfg" in spec:
+        c = synth.workload_config(spec["cfg"], spec.get("n"))
+        nv, a0, calA0 = c["nv"], c["a0"], c["calA0"]
+    else:
+        n = spec["n"]
+        nv, a0, calA0 = [spec["nv"]] * n, [1.0] * (n // 2) + [1.4 ** 2] * (n - n // 2), 1.0
+    return synth.make_packing(nv, a0, calA0, phi, seed=seed, placement=placement)
+
+
+def setup_ref(pk, potential, interaction, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj=2.5, l1=0.0, l2=0.0, monomer=0,
+              stiff=0.0, ext=0.0):
+    R = oracle.ref()
+    R.ref_create(pk.num_particles, pk.nv_list)
+    R.ref_set_box(float(pk.box[0]), float(pk.box[1]))
+    R.ref_set_types(oracle.POTENTIALS[potential], oracle.INTERACTIONS[interaction], monomer, 0)
+    R.ref_set_energy_costs(ea, el, eb, ec)
+    R.ref_set_lj_cutoff(lj)
+    R.ref_set_attraction(l1, l2)
+    R.ref_set_fene(stiff, ext)
+    R.ref_set_state(pk.pos.ctypes.data, pk.vel.ctypes.data, pk.rad.ctypes.data, pk.l0.ctypes.data,
+                    pk.theta0.ctypes.data, pk.a0.ctypes.data)
+    cut = R.ref_set_displacement_cutoff(0.5, 2 * pk.rad.mean())
+    return R, cut
+
+
+def grab(R, pk, names):
+    out = {}
+    sizes = dict(pos=2 * pk.num_vertices, vel=2 * pk.num_vertices, force=2 * pk.num_vertices,
+                 energy=pk.num_vertices, p_energy=pk.num_particles, area=pk.num_particles,
+                 perimeter=pk.num_particles, theta=pk.num_vertices, length=pk.num_vertices, ppos=2 * pk.num_particles)
+    for n in names:
+        a = np.zeros(sizes[n])
+        R.ref_get(FIELDS[n], a)
+        out["out_" + n] = a
+    return out
+
+
+def inputs(pk, **params):
+    d = {"nv_list": pk.nv_list, "pos": pk.pos, "vel": pk.vel, "rad": pk.rad, "l0": pk.l0, "theta0": pk.theta0,
+         "a0": pk.a0, "box": pk.box}
+    for k, v in params.items():
+        d["param_" + k] = np.asarray(v)
+    return d
+
+
+def force_cases():
+    for idx, (name, spec, pot, inter, placement, phi, extra) in enumerate(FORCE_CASES):
+        pk = packing_for(spec, phi, placement, seed=20261203 + 100 + idx)
+        kw = dict(l1=extra.get("l1", 0.0), l2=extra.get("l2", 0.0), monomer=extra.get("monomer", 0),
+                  stiff=extra.get("stiff", 0.0), ext=extra.get("ext", 0.0))
+        R, cut = setup_ref(pk, pot, inter, **kw)
+        R.ref_calc_neighbor_list(cut)
+        ls = R.ref_neighbor_list_size()
+        nbr = np.zeros(pk.num_vertices * max(ls, 1), np.int64)
+        cnt = np.zeros(pk.num_vertices, np.int64)
+        R.ref_get_neighbors(nbr)
+        R.ref_get_max_neighbor_list(cnt)
+        R.ref_calc_force_energy()
+        d = inputs(pk, potential=oracle.POTENTIALS[pot], interaction=oracle.INTERACTIONS[inter], ea=1.0, el=1.0,
+                   eb=0.01, ec=1.0, lj_cutoff=2.5, cut_distance=cut, **kw)
+        d.update(grab(R, pk, ["force", "energy", "p_energy", "area", "perimeter", "theta", "length", "ppos"]))
+        d["out_neighbors"] = nbr[: pk.num_vertices * ls]
+        d["out_max_neighbor_list"] = cnt
+        d["out_list_size"] = np.asarray(ls)
+        d["out_potential_energy"] = np.asarray(R.ref_potential_energy())
+        np.savez_compressed(os.path.join(OUT, f"force_{name}.npz"), **d)
+        print(f"force_{name}: nv={pk.num_vertices} listSize={ls} maxF={np.abs(d['out_force']).max():.3e}")
+
+
+def traj_cases():
+    # NVE on config-0 geometry with ring-rigid velocities large enough to trigger rebuilds.
+    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 200)
+    rng = np.random.default_rng(7)
+    pk.vel = np.repeat(rng.normal(0.0, 0.3, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
+    dt, nsteps = 0.005, 200
+    R, cut = setup_ref(pk, "harmonic", "vertexVertex")
+    R.ref_set_time_step(dt)
+    R.ref_calc_neighbor_list(cut)
+    R.ref_reset_last_positions()
+    R.ref_calc_force_energy()
+    R.ref_nve_loop(nsteps)
+    d = inputs(pk, potential=0, interaction=0, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, dt=dt,
+               nsteps=nsteps, cut_distance=cut)
+    d.update(grab(R, pk, ["pos", "vel", "force", "energy"]))
+    d["out_update_count"] = np.asarray(R.ref_update_count())
+    d["out_potential_energy"] = np.asarray(R.ref_potential_energy())
+    d["out_kinetic_energy"] = np.asarray(R.ref_kinetic_energy())
+    np.savez_compressed(os.path.join(OUT, "traj_nve_harmonic_vv.npz"), **d)
+    print(f"traj_nve_harmonic_vv: updates={int(d['out_update_count'])}")
+
+    # NVE, smooth LJ, 64 rings.
+    pk = packing_for(dict(cfg=1, n=64), 0.40, "rsa", seed=20261203 + 201)
+    pk.vel = np.repeat(rng.normal(0.0, 0.3, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
+    dt, nsteps = 0.002, 150
+    R, cut = setup_ref(pk, "lennardJones", "vertexSmooth")
+    R.ref_set_time_step(dt)
+    R.ref_calc_neighbor_list(cut)
+    R.ref_reset_last_positions()
+    R.ref_calc_force_energy()
+    R.ref_nve_loop(nsteps)
+    d = inputs(pk, potential=1, interaction=1, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, dt=dt,
+               nsteps=nsteps, cut_distance=cut)
+    d.update(grab(R, pk, ["pos", "vel", "force", "energy", "p_energy"]))
+    d["out_update_count"] = np.asarray(R.ref_update_count())
+    d["out_potential_energy"] = np.asarray(R.ref_potential_energy())
+    np.savez_compressed(os.path.join(OUT, "traj_nve_lj_smooth.npz"), **d)
+    print(f"traj_nve_lj_smooth: updates={int(d['out_update_count'])}")
+
+    # FIRE on config-0 geometry.
+    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 202)
+    R, cut = setup_ref(pk, "harmonic", "vertexVertex")
+    dt = 0.01
+    params = np.array([0.2, 0.5, 1.1, 0.99, dt, 10 * dt, 0.2])
+    R.ref_calc_neighbor_list(cut)
+    R.ref_reset_last_positions()
+    R.ref_calc_force_energy()
+    R.ref_fire_init(params, 20, 0)
+    nsteps = 300
+    R.ref_fire_loop(nsteps)
+    st = np.zeros(3)
+    R.ref_fire_state(st)
+    d = inputs(pk, potential=0, interaction=0, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, nsteps=nsteps,
+               fire=params, cut_distance=cut)
+    d.update(grab(R, pk, ["pos", "vel", "force", "energy"]))
+    d["out_fire_state"] = st
+    d["out_max_unbalanced_force"] = np.asarray(R.ref_max_unbalanced_force())
+    d["out_potential_energy"] = np.asarray(R.ref_potential_energy())
+    np.savez_compressed(os.path.join(OUT, "traj_fire_harmonic_vv.npz"), **d)
+    print(f"traj_fire_harmonic_vv: maxF={float(d['out_max_unbalanced_force']):.3e} state={st}")
+
+    # Langevin with the library's Philox noise (seed, streams 2s) injected.
+    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 203)
+    pk.vel = np.repeat(rng.normal(0.0, 0.1, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
+    dt, nsteps, T, gamma, seed = 0.005, 60, 0.01, 1.0, 12345
+    R, cut = setup_ref(pk, "harmonic", "vertexVertex")
+    R.ref_set_time_step(dt)
+    R.ref_calc_neighbor_list(cut)
+    R.ref_reset_last_positions()
+    R.ref_calc_force_energy()
+    xi = np.concatenate([philox_noise(seed, 2 * s, pk.num_particles).reshape(-1) for s in range(nsteps)])
+    noise_amp = np.sqrt(2.0 * T * gamma / dt)
+    R.ref_langevin_loop(nsteps, gamma, noise_amp, xi.ctypes.data, 0.0, None)
+    d = inputs(pk, potential=0, interaction=0, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, dt=dt,
+               nsteps=nsteps, T=T, gamma=gamma, seed=seed, cut_distance=cut)
+    d.update(grab(R, pk, ["pos", "vel", "force"]))
+    np.savez_compressed(os.path.join(OUT, "traj_langevin_harmonic_vv.npz"), **d)
+    print("traj_langevin_harmonic_vv: done")
+
+
+if __name__ == "__main__":
+    if not oracle.ref_available():
+        oracle.build()
+    force_cases()
+    traj_cases()
