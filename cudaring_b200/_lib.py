@@ -15,7 +15,7 @@ import re
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 HEADER = os.path.join(ROOT, "include", "cudaring.h")
-LIBPATH = os.path.join(HERE, "lib", "libcudaring.so")
+LIBPATH = os.environ.get("CUDARING_LIBPATH") or os.path.join(HERE, "lib", "libcudaring.so")
 
 _TYPES = {
     "int": C.c_int,

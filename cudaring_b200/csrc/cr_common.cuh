@@ -13,7 +13,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include "../../include/cudaring.h"
+#include "cudaring.h"
 
 namespace cr {
 

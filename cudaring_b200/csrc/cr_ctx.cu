@@ -111,6 +111,8 @@ struct cr_ctx {
 
 namespace {
 
+int upload(cr_ctx* ctx, void* dst, const void* src, size_t bytes);
+
 template <typename T>
 int dalloc(cr_ctx* ctx, T** p, size_t n) {
   if (*p) cudaFree(*p);
@@ -247,6 +249,7 @@ NbrArgs nbr_args(cr_ctx* ctx, int buf, double cut) {
   n.cell_ring = ctx->cell_ring;
   n.status = ctx->status;
   n.count_op = 0;
+  n.count_update = 0;
   return n;
 }
 
@@ -445,7 +448,9 @@ int capture_graph(cr_ctx* ctx, const std::vector<Op>& ops, int kind, GraphEntry&
       CR_TRY(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
       cudaGraph_t body = cp.conditional.phGraph_out[0];
       CR_TRY(cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-      launch_nbr_build(ctx->side, ctx->p, ctx->grid, nbr_args(ctx, op.check_buf, ctx->cut_distance));
+      NbrArgs nb = nbr_args(ctx, op.check_buf, ctx->cut_distance);
+      nb.count_update = 1;  // DPM2D::checkDisplacement's updateCount (src/DPM2D.cu:1397-1405)
+      launch_nbr_build(ctx->side, ctx->p, ctx->grid, nb);
       cudaGraph_t body_out;
       CR_TRY(cudaStreamEndCapture(ctx->side, &body_out));
     }
@@ -469,6 +474,8 @@ int run_direct(cr_ctx* ctx, const std::vector<Op>& ops, size_t first, int kind) 
     if (ctx->status_h->abort) return CR_OK;  // caller inspects
     if (op.check_after && ctx->status_h->rebuild) {
       if ((rc = build_list(ctx, op.check_buf, ctx->cut_distance))) return rc;
+      ctx->status_h->update_count += 1;  // DPM2D::checkDisplacement's updateCount
+      if ((rc = upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus)))) return rc;
     }
   }
   return CR_OK;
@@ -553,6 +560,8 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
       if ((rc = build_list(ctx, plan[j][(size_t)k - 1].check_buf, ctx->cut_distance))) return rc;
       if ((rc = clear_flags(ctx))) return rc;
       if ((rc = run_direct(ctx, plan[j], (size_t)k, kind))) return rc;
+      if (ctx->status_h->nonfinite)
+        return ctx->fail(CR_ENONFINITE, "non-finite force after resuming from a neighbour-list overflow");
       if (ctx->status_h->abort) return ctx->fail(CR_ENBR_OVERFLOW, "neighbour list overflow during resume");
       c = j + 1;
       continue;
@@ -569,6 +578,19 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
 }
 
 int check_ctx(const cr_ctx* ctx) { return ctx ? CR_OK : CR_EINVAL; }
+
+// Tiles: consecutive whole rings up to the tile capacity of the lane count.
+void make_tiles(cr_ctx* ctx) {
+  const int tv = tile_vertices(ctx->lanes);
+  ctx->tiles_h.clear();
+  int r = 0;
+  while (r < ctx->np) {
+    int r1 = r, cnt = 0;
+    while (r1 < ctx->np && cnt + ctx->ring_nv_h[r1] <= tv) cnt += ctx->ring_nv_h[r1++];
+    ctx->tiles_h.push_back(make_int4(r, r1, ctx->ring_first_h[r], ctx->ring_first_h[r] + cnt));
+    r = r1;
+  }
+}
 
 int set_current_device(cr_ctx* ctx) {
   cudaError_t e = cudaSetDevice(ctx->device);
@@ -643,15 +665,7 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
       pp[f + k] = make_int2(prev, f + k2);
     }
   }
-  // tiles: consecutive whole rings up to the tile capacity
-  const int tv = tile_vertices(ctx->lanes);
-  int r = 0;
-  while (r < ctx->np) {
-    int r1 = r, cnt = 0;
-    while (r1 < ctx->np && cnt + ctx->ring_nv_h[r1] <= tv) cnt += ctx->ring_nv_h[r1++];
-    ctx->tiles_h.push_back(make_int4(r, r1, ctx->ring_first_h[r], ctx->ring_first_h[r] + cnt));
-    r = r1;
-  }
+  make_tiles(ctx);
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking)) != cudaSuccess) {
     delete ctx;
@@ -1374,6 +1388,35 @@ int cr_profile_step_kernel(cr_ctx* ctx, long reps, double* ms_per_launch) {
   cudaFreeAsync(frc_s, ctx->stream);
   cudaFreeAsync(st_s, ctx->stream);
   CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+int cr_set_lanes(cr_ctx* ctx, int lanes) {
+  if (!ctx) return CR_EINVAL;
+  if (lanes != 1 && lanes != 2 && lanes != 4 && lanes != 8) return ctx->fail(CR_EINVAL, "lanes must be 1, 2, 4 or 8");
+  int maxnv = 0;
+  for (int n : ctx->ring_nv_h) maxnv = std::max(maxnv, n);
+  if (maxnv > tile_vertices(lanes)) return ctx->fail(CR_EINVAL, "a ring does not fit the tile of this lane count");
+  ctx->lanes = lanes;
+  make_tiles(ctx);
+  int rc;
+  if ((rc = dalloc(ctx, &ctx->tiles, ctx->tiles_h.size()))) return rc;
+  if ((rc = upload(ctx, ctx->tiles, ctx->tiles_h.data(), ctx->tiles_h.size() * sizeof(int4)))) return rc;
+  if ((rc = ensure_partials(ctx))) return rc;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_get_lanes(const cr_ctx* ctx, int* lanes) {
+  if (!ctx || !lanes) return CR_EINVAL;
+  *lanes = ctx->lanes;
+  return CR_OK;
+}
+
+int cr_set_use_graphs(cr_ctx* ctx, int on) {
+  if (!ctx) return CR_EINVAL;
+  ctx->use_graphs = on != 0;
+  drop_graphs(ctx);
   return CR_OK;
 }
 

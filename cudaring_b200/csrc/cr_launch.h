@@ -64,6 +64,7 @@ struct NbrArgs {
   int* cell_ring;     // [nv]
   DevStatus* status;
   int count_op;       // 1: the build is one op of a step sequence (ops_done += 1)
+  int count_update;   // 1: a displacement-triggered rebuild (DPM2D::updateCount += 1)
 };
 void launch_nbr_build(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n);
 

@@ -114,7 +114,7 @@ __device__ __forceinline__ void publish_build(const NbrArgs& n, int my_max, int 
         st->abort = 1;
       } else {
         st->rebuild = 0;
-        st->update_count += 1;
+        if (n.count_update) st->update_count += 1;
         if (n.count_op) st->ops_done += 1;
       }
       st->done_ctr = 0;

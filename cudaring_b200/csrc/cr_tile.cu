@@ -4,8 +4,12 @@
 
 namespace cr {
 
+// Occupancy target in threads per SM: 512 leaves 128 registers per thread,
+// where the smooth-interaction body compiles without spills.
+constexpr int kTileThreadsPerSM = 512;
+
 template <int POT, int INTER, int MODE, int BLOCK, int L>
-__global__ void __launch_bounds__(BLOCK) k_tile(const __grid_constant__ SysParams p,
+__global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const __grid_constant__ SysParams p,
                                                 const __grid_constant__ SysArrays a,
                                                 const __grid_constant__ StepArgs s) {
   constexpr int TV = BLOCK / L;
@@ -151,19 +155,40 @@ __global__ void __launch_bounds__(BLOCK) k_tile(const __grid_constant__ SysParam
         const double2 xq = s_pos[lq], xqq = s_pos[lqq];
         const double2 seg_i = s_seg[lq];    // pbc(x_i - x_q)
         const double2 pseg_i = s_seg[lqq];  // pbc(x_q - x_qq)
+        const double len2_i = fma(seg_i.y, seg_i.y, seg_i.x * seg_i.x);
+        const double range = pot_range<POT>(p);
+        double2 dummy = make_double2(0.0, 0.0);
         for (int sl = lane; sl < cnt; sl += L) {
           const int j = __ldg(a.nbr + (size_t)sl * p.nv + i);
           const double2 xj = a.pos[j];
           const double rsum = ri + __ldg(a.rad + j);
           const int2 pq = __ldg(a.pp_of + j);
           const double2 xjq = a.pos[pq.x];
-          const double2 xjqq = a.pos[pq.y];
-          double2 dummy0 = make_double2(0.0, 0.0), dummy1 = make_double2(0.0, 0.0);
-          // role 1: i against segment prev(j) -> j
-          smooth_unit<POT, true>(p, xi, xj, xjq, xjqq, pbc2(p, xj, xjq), pbc2(p, xjq, xjqq), rsum, fi, dummy0,
-                                 dummy1, ei);
-          // role 2: neighbour j against this vertex's segment prev(i) -> i
-          smooth_unit<POT, false>(p, xj, xi, xq, xqq, seg_i, pseg_i, rsum, dummy0, fi, fq, ei);
+          const double R = range * rsum;
+          const double inv_rsum = 1.0 / rsum;
+          const double2 w1 = pbc2(p, xi, xj);  // role 1: t = i, o = j
+          const double w2 = fma(w1.y, w1.y, w1.x * w1.x);
+          {
+            // role 1: i against the segment prev(j) -> j of the other ring
+            const double2 tq = pbc2(p, xi, xjq);
+            const double tq2 = fma(tq.y, tq.y, tq.x * tq.x);
+            const double2 seg = pbc2(p, xj, xjq);
+            const double len2 = fma(seg.y, seg.y, seg.x * seg.x);
+            if (!smooth_out_of_range(R, tq2, w2, len2)) {
+              const double2 xjqq = a.pos[pq.y];
+              smooth_core<POT, true>(p, xi, xjq, xjqq, seg, len2, pbc2(p, xjq, xjqq), tq, tq2, w1, rsum, inv_rsum,
+                                     fi, dummy, dummy, ei);
+            }
+          }
+          {
+            // role 2: neighbour j against this vertex's segment prev(i) -> i
+            const double2 tq = pbc2(p, xj, xq);
+            const double tq2 = fma(tq.y, tq.y, tq.x * tq.x);
+            if (!smooth_out_of_range(R, tq2, w2, len2_i)) {
+              smooth_core<POT, false>(p, xj, xq, xqq, seg_i, len2_i, pseg_i, tq, tq2,
+                                      make_double2(-w1.x, -w1.y), rsum, inv_rsum, dummy, fi, fq, ei);
+            }
+          }
         }
       }
     }
@@ -359,7 +384,7 @@ __global__ void __launch_bounds__(BLOCK) k_tile(const __grid_constant__ SysParam
         if (st->sums[S_NONFINITE] != 0.0) { st->nonfinite = 1; st->abort = 1; }
         if (s.kind == KIND_FIRE) {
           st->fire_iters += 1;
-          if (st->sums[S_FMAX2] <= s.fire_tol * s.fire_tol) st->converged = 1;
+          if (s.fire_tol >= 0.0 && st->sums[S_FMAX2] <= s.fire_tol * s.fire_tol) st->converged = 1;
         }
         st->ops_done += 1;
         if (s.kind != KIND_FIRE) st->rng_step += 1;
@@ -375,7 +400,8 @@ __global__ void __launch_bounds__(BLOCK) k_tile(const __grid_constant__ SysParam
 template <int POT, int INTER, int MODE>
 static void launch_tile_t(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s) {
   if (c.lanes == 1) k_tile<POT, INTER, MODE, 128, 1><<<c.grid, 128, 0, c.stream>>>(p, a, s);
-  else if (c.lanes == 4) k_tile<POT, INTER, MODE, 128, 4><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+  else if (c.lanes == 4) k_tile<POT, INTER, MODE, 256, 4><<<c.grid, 256, 0, c.stream>>>(p, a, s);
+  else if (c.lanes == 8) k_tile<POT, INTER, MODE, 256, 8><<<c.grid, 256, 0, c.stream>>>(p, a, s);
   else k_tile<POT, INTER, MODE, 128, 2><<<c.grid, 128, 0, c.stream>>>(p, a, s);
 }
 
@@ -401,6 +427,8 @@ void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysPara
 #undef CR_TILE_CASE
 }
 
-int tile_vertices(int lanes) { return 128 / (lanes <= 0 ? 2 : lanes); }
+// Tile capacity (vertices of whole rings per CTA) for a lane count:
+// 1 -> 128 threads x 1, 2 -> 128 x 2, 4 -> 256 x 4, 8 -> 256 x 8.
+int tile_vertices(int lanes) { return lanes >= 4 ? 256 / lanes : 128 / (lanes <= 0 ? 2 : lanes); }
 
 }  // namespace cr

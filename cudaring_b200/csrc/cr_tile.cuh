@@ -88,24 +88,163 @@ __device__ __forceinline__ double2 philox_normal2(unsigned long long seed, unsig
   return make_double2(rr * c, rr * s);
 }
 
-// In-range test + gradMultiple of the own-side vertex-vertex term
-// (calcContactInteraction .. calcWCAInteraction, include/cudaKernel.cuh:531-668).
+// Interaction range in units of radSum: the distance beyond which every pair
+// term of the potential is exactly zero.
+template <int POT>
+__device__ __forceinline__ double pot_range(const SysParams& p) {
+  if constexpr (POT == POT_HARMONIC) return 1.0;
+  else if constexpr (POT == POT_LJ) return p.lj_cutoff;
+  else if constexpr (POT == POT_ADHESIVE) return 1.0 + p.l2;
+  else return kWCAcut;
+}
+
+// Pair term from the squared distance: returns whether the pair is in range
+// (the reference's own test), gradMultiple gm (force on "this" = gm * delta / d),
+// 1/d and the half-pair energy.  Same arithmetic as calcContactInteraction ..
+// calcWCAInteraction / calcGradMultipleAndEnergy (include/cudaKernel.cuh:531-668,
+// 806-858) with the divisions by d and radSum taken as products with one
+// reciprocal square root and one reciprocal (rounding-level differences).
+template <int POT>
+__device__ __forceinline__ bool pair_eval(const SysParams& p, double d2, double rsum, double inv_rsum, double& gm,
+                                          double& inv_d, double& ep) {
+  inv_d = rsqrt(d2);
+  const double d = d2 * inv_d;
+  if constexpr (POT == POT_HARMONIC) {
+    const double ov = 1.0 - d * inv_rsum;
+    if (!(ov > 0.0)) return false;
+    gm = p.ec * ov * inv_rsum;
+    ep = (0.5 * p.ec * ov * ov) * 0.5;
+    return true;
+  } else if constexpr (POT == POT_LJ) {
+    if (!(d <= p.lj_cutoff * rsum)) return false;
+    const double ratio = rsum * inv_d;
+    const double r2 = ratio * ratio;
+    const double r6 = r2 * r2 * r2;
+    const double r12 = r6 * r6;
+    const double fshift = p.lj_fshift * inv_rsum;
+    gm = 24.0 * p.ec * (2.0 * r12 - r6) * inv_d - fshift;
+    ep = 0.5 * (4.0 * p.ec * (r12 - r6) - p.lj_ecut - fabs(fshift) * (d - p.lj_cutoff * rsum));
+    return true;
+  } else if constexpr (POT == POT_ADHESIVE) {
+    if (!(d < (1.0 + p.l2) * rsum)) return false;
+    const double ov = 1.0 - d * inv_rsum;
+    if (d < (1.0 + p.l1) * rsum) {
+      gm = p.ec * ov * inv_rsum;
+      ep = 0.5 * p.ec * (ov * ov - p.l1 * p.l2) * 0.5;
+    } else {
+      const double k = p.ec * p.l1 / (p.l2 - p.l1);
+      gm = -k * (ov + p.l2) * inv_rsum;
+      ep = -(0.5 * k * (ov + p.l2) * (ov + p.l2)) * 0.5;
+    }
+    return true;
+  } else {
+    if (!(d <= kWCAcut * rsum)) return false;
+    const double ratio = rsum * inv_d;
+    const double r2 = ratio * ratio;
+    const double r6 = r2 * r2 * r2;
+    const double r12 = r6 * r6;
+    gm = 24.0 * p.ec * (2.0 * r12 - r6) * inv_d;
+    ep = 0.5 * p.ec * (4.0 * (r12 - r6) + 1.0);
+    return true;
+  }
+}
+
+// Own-side vertex-vertex term of kernelCalcVertexInteraction (:690-722).
 template <int POT>
 __device__ __forceinline__ void pair_own(const SysParams& p, double2 dl, double rsum, double2& f, double& e) {
-  double d = dist_of(dl);
-  bool in;
-  if constexpr (POT == POT_HARMONIC) in = (1.0 - d / rsum) > 0.0;
-  else if constexpr (POT == POT_LJ) in = d <= p.lj_cutoff * rsum;
-  else if constexpr (POT == POT_ADHESIVE) in = d < (1.0 + p.l2) * rsum;
-  else in = d <= kWCAcut * rsum;
-  if (in) {
-    double ep = 0.0;
-    double g = pair_gm<POT>(p, d, rsum, ep);
-    double s = g / d;
+  const double d2 = fma(dl.y, dl.y, dl.x * dl.x);
+  const double R = pot_range<POT>(p) * rsum * (1.0 + 1e-12);
+  if (d2 > R * R) return;  // exactly zero beyond the range
+  double gm, inv_d, ep = 0.0;
+  if (pair_eval<POT>(p, d2, rsum, 1.0 / rsum, gm, inv_d, ep)) {
+    const double s = gm * inv_d;
     f.x += s * dl.x;
     f.y += s * dl.y;
     e += ep;
   }
+}
+
+// sign = cross / |cross| of calcVertexSegmentInteraction (:882-884), NaN for
+// cross == 0 exactly as there.
+__device__ __forceinline__ double sign_of(double c) {
+  return c > 0.0 ? 1.0 : (c < 0.0 ? -1.0 : __longlong_as_double(0x7ff8000000000000LL));
+}
+
+// Smooth unit from precomputed geometry.  t: the vertex, o: segment end,
+// q = prev(o), qq = prev(q); seg = pbc(o - q), pseg = pbc(q - qq),
+// tq = pbc(t - q), w = pbc(t - o), tq2 = |tq|^2.  See smooth_unit.
+template <int POT, bool ROLE1>
+__device__ __forceinline__ void smooth_core(const SysParams& p, double2 t, double2 q, double2 qq, double2 seg,
+                                            double len2, double2 pseg, double2 tq, double tq2, double2 w,
+                                            double rsum, double inv_rsum, double2& ft, double2& fo, double2& fq,
+                                            double& e) {
+  const double inv_len = rsqrt(len2);
+  const double inv_lsq = inv_len * inv_len;
+  const double proj = (tq.x * seg.x + tq.y * seg.y) * inv_lsq;
+  const double2 tqq = pbc2(p, t, qq);
+  const double pinv = rsqrt(fma(pseg.y, pseg.y, pseg.x * pseg.x));
+  const double pproj = (tqq.x * pseg.x + tqq.y * pseg.y) * (pinv * pinv);
+  if (proj >= 0.0 && proj < 1.0) {
+    const double2 pj = make_double2(q.x + proj * seg.x, q.y + proj * seg.y);
+    const double2 dp = pbc2(p, t, pj);
+    double gm, inv_d, ep = 0.0;
+    if (pair_eval<POT>(p, fma(dp.y, dp.y, dp.x * dp.x), rsum, inv_rsum, gm, inv_d, ep) && gm != 0.0) {
+      const double cross = seg.x * w.y - w.x * seg.y;
+      const double sign = sign_of(cross);
+      const double g = gm * inv_len;
+      if constexpr (ROLE1) {
+        ft.x += g * sign * (-seg.y);
+        ft.y += g * sign * seg.x;
+      } else {
+        const double a = fabs(cross) * inv_lsq;
+        fo.x += g * (sign * tq.y - a * seg.x);
+        fo.y += g * (-sign * tq.x - a * seg.y);
+        fq.x += g * (-sign * w.y + a * seg.x);
+        fq.y += g * (sign * w.x + a * seg.y);
+      }
+      e += ep;
+    }
+    if (pproj >= 0.0 && pproj < 1.0) {
+      // calcVertexVertexInteraction(previousPos, thisPos, ...): delta = pbc(q - t)
+      double g2, id2, ep2 = 0.0;
+      if (pair_eval<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != 0.0) {
+        const double s2 = g2 * id2;
+        if constexpr (ROLE1) {
+          ft.x -= s2 * tq.x;
+          ft.y -= s2 * tq.y;
+        } else {
+          fq.x += s2 * tq.x;
+          fq.y += s2 * tq.y;
+        }
+        e -= ep2;
+      }
+    }
+  } else if (proj < 0.0 && pproj >= 1.0) {
+    // calcVertexVertexInteraction(thisPos, previousPos, ...): delta = pbc(t - q)
+    double g2, id2, ep2 = 0.0;
+    if (pair_eval<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != 0.0) {
+      const double s2 = g2 * id2;
+      if constexpr (ROLE1) {
+        ft.x += s2 * tq.x;
+        ft.y += s2 * tq.y;
+      } else {
+        fq.x -= s2 * tq.x;
+        fq.y -= s2 * tq.y;
+      }
+      e += ep2;
+    }
+  }
+}
+
+// True when no term of a smooth unit can be in range: every point of the
+// segment is at least max(|t-o|, |t-q|) - |o-q| from t, and both corrections
+// use |t-q|.  The relative margin covers rounding, so a skipped unit is one
+// that would have contributed exactly zero.
+__device__ __forceinline__ bool smooth_out_of_range(double R, double tq2, double w2, double len2) {
+  const double Rm = R * (1.0 + 1e-12);
+  if (!(tq2 > Rm * Rm)) return false;
+  const double lim = Rm + sqrt(len2);
+  return fmax(tq2, w2) > lim * lim;
 }
 
 // One unit U(t; o) of kernelCalcSmoothInteraction (include/cudaKernel.cuh:922-975):

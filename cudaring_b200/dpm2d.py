@@ -206,6 +206,20 @@ class DPM2D:
 
     def getFIREState(self): return self._get("cr_get_fire_state", 3)
 
+    def setLanes(self, lanes): self._call("cr_set_lanes", int(lanes))
+
+    def getLanes(self):
+        out = C.c_int()
+        self._call("cr_get_lanes", C.byref(out))
+        return out.value
+
+    def setUseGraphs(self, on): self._call("cr_set_use_graphs", int(bool(on)))
+
+    def profileStepKernel(self, reps=100):
+        out = C.c_double()
+        self._call("cr_profile_step_kernel", int(reps), C.byref(out))
+        return out.value
+
     def getLaunchCount(self):
         out = C.c_longlong()
         self._call("cr_get_launch_count", C.byref(out))

@@ -168,7 +168,10 @@ def workload_config(index: int, scale_rings: int | None = None) -> dict:
     """Ring counts and parameters of the five benchmark configurations.
 
     index 0: 32 rings, nv 16/22 bidisperse 1:1.4, harmonic, calA0 1.0, phi 0.70.
-    index 1: 1024 rings, nv 32/45 (1:1.4), smooth LJ rc 2.5, calA0 1.05, phi 0.85.
+    index 1: 1024 rings, nv 32/45 (1:1.4), smooth LJ rc 2.5, calA0 1.05, phi 0.85;
+             the shape constants are those of the reference's NVE driver
+             (ea 1e5, el 20, eb 10; runNVE.cpp:39), stiff enough that the LJ
+             well (epsilon 1) does not crumple the rings.
     index 2: 4096 rigid ellipses, 24 vertices, WCA, phi 0.65.
     index 3: batched FIRE compression (see the batch module).
     index 4: 256 rings, nv 32, harmonic, phi 0.88.
@@ -185,7 +188,7 @@ def workload_config(index: int, scale_rings: int | None = None) -> dict:
         nv = [32] * (n // 2) + [45] * (n - n // 2)
         a0 = [1.0] * (n // 2) + [1.4 ** 2] * (n - n // 2)
         return dict(nv=nv, a0=a0, calA0=1.05, phi=0.85, potential="lennardJones", interaction="vertexSmooth",
-                    LJcutoff=2.5, ea=1.0, el=1.0, eb=0.01, ec=1.0, dt=0.002, T=0.01)
+                    LJcutoff=2.5, ea=1e5, el=20.0, eb=10.0, ec=1.0, dt=0.002, T=0.01)
     if index == 4:
         n = scale_rings or 256
         return dict(nv=[32] * n, a0=[1.0] * n, calA0=1.0, phi=0.88, potential="harmonic",

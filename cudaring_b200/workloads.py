@@ -16,7 +16,7 @@ import math
 import numpy as np
 
 from . import synth
-from .dpm2d import DPM2D
+from .dpm2d import DPM2D, simControl
 
 
 def lattice_packing(nv_list, a0_list, calA0, seed: int, spacing_scale: float = 1.02) -> synth.Packing:
@@ -49,10 +49,16 @@ def lattice_packing(nv_list, a0_list, calA0, seed: int, spacing_scale: float = 1
 
 def compress(d: DPM2D, phi0: float, phi1: float, dphi: float = 0.05, fire_dt: float = 2e-3,
              tol_mid: float = 1e-2, tol_end: float = 1e-4, max_iter: int = 20000) -> dict:
-    """Grow rings from preferred packing fraction phi0 to phi1 with FIRE relaxation."""
+    """Grow rings from preferred packing fraction phi0 to phi1 with FIRE relaxation.
+
+    Uses the potential currently set on ``d``; large steps need a bounded
+    (harmonic) repulsion, as Lennard-Jones overlaps of a few percent of a ring
+    radius give forces that no FIRE step survives.
+    """
     phi = phi0
     iters = 0
     cutoff_ = 0.5
+    fmax = float("nan")
     while True:
         size = 2.0 * d.getMeanVertexRadius()
         cut = d.setDisplacementCutoff(cutoff_, size)
@@ -100,8 +106,21 @@ def prepared_deformable(index: int = 1, rings: int | None = None, seed: int = 20
     if "LJcutoff" in c:
         kw["LJcutoff"] = c["LJcutoff"]
     d = DPM2D.from_packing(pk, **kw)
+    # Compress with soft shape constants and harmonic repulsion (bounded
+    # forces, large stable FIRE steps), rescale to the nominal ring size, then
+    # switch to the configuration's potential and shape constants and relax
+    # with a FIRE step small enough for its stiffest mode.
+    d.setPotentialType(simControl.potentialEnum.harmonic)
+    d.setEnergyCosts(1.0, 1.0, 0.01, c["ec"])
     info = compress(d, phi_start, c["phi"])
     rescale_lengths(d, math.sqrt(phi_start / c["phi"]))
+    d.setPotentialType(getattr(simControl.potentialEnum, c["potential"]))
+    d.setEnergyCosts(c["ea"], c["el"], c["eb"], c["ec"])
+    if "LJcutoff" in c:
+        d.setLJcutoff(c["LJcutoff"])
+    final = compress(d, c["phi"], c["phi"], fire_dt=1e-4, tol_end=1e-4, max_iter=30000)
+    info["fire_iterations"] += final["fire_iterations"]
+    info["max_force"] = final["max_force"]
     size = 2.0 * d.getMeanVertexRadius()
     cut = d.setDisplacementCutoff(0.5, size)
     d.calcNeighborList(cut)

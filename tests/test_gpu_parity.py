@@ -164,17 +164,22 @@ def test_full_size_config_neighbor_sets_and_forces(cuda_device):
     assert rel_inf(d.getVertexForces(), out["force"]) < TOL
 
 
-def test_nve_energy_conservation(cuda_device):
+def test_nve_energy_error_is_second_order(cuda_device):
+    # velocity Verlet: the energy error over a fixed time scales as dt^2
     g = load_golden(golden_files("traj_nve_harmonic_vv")[0])
-    d = _prepared(g)
-    d.initNVE(0.0, readState=True)
-    e0 = d.getEnergy()
-    es = []
-    for _ in range(20):
-        d.NVELoop(100)
-        es.append(d.getEnergy())
-    drift = max(abs(e - e0) for e in es) / abs(e0)
-    assert drift < 2e-3
+    errs = []
+    for dt, n in ((0.004, 250), (0.002, 500)):
+        d = _prepared(g)
+        d.setTimeStep(dt)
+        d.initNVE(0.0, readState=True)
+        e0 = d.getEnergy()
+        es = []
+        for _ in range(10):
+            d.NVELoop(n // 10)
+            es.append(d.getEnergy())
+        errs.append(max(abs(e - e0) for e in es) / abs(e0))
+    assert errs[0] < 5e-3
+    assert 2.5 < errs[0] / errs[1] < 6.0
 
 
 def test_force_is_minus_gradient(cuda_device):
