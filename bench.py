@@ -81,6 +81,9 @@ def prepared_state(args, rank):
                      fire_iterations=info["fire_iterations"])
     if args.lanes:
         d.setLanes(args.lanes)
+    elif not args.profile_kernel:
+        d.autotune(30)  # untimed: picks lanes per vertex by timing the fused kernel
+    info["lanes"] = d.getLanes()
     return d, info
 
 
@@ -360,7 +363,8 @@ def main():
                        "l2": "flushed between bench steps (256 MB write)", "parallelism": f"replicas x{world}",
                        "neighbour_rebuilds_in_timed_region": updates,
                        "energy_drift_rel": abs(e1 - e0) / abs(e0) if e0 else None,
-                       "prep_seconds": t_prep, "fire_iterations_prep": info["fire_iterations"]},
+                       "prep_seconds": t_prep, "fire_iterations_prep": info["fire_iterations"],
+                       "lanes_per_vertex": info["lanes"]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks.summary(),
         }

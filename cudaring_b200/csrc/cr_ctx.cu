@@ -1413,6 +1413,30 @@ int cr_get_lanes(const cr_ctx* ctx, int* lanes) {
   return CR_OK;
 }
 
+int cr_autotune(cr_ctx* ctx, long reps, int* lanes_out) {
+  if (!ctx || reps <= 0) return CR_EINVAL;
+  int maxnv = 0;
+  for (int n : ctx->ring_nv_h) maxnv = std::max(maxnv, n);
+  int best = ctx->lanes;
+  double best_ms = 1e300;
+  const int cand[] = {1, 2, 4, 8};
+  for (int lanes : cand) {
+    if (maxnv > tile_vertices(lanes)) continue;
+    int rc = cr_set_lanes(ctx, lanes);
+    if (rc) return rc;
+    double ms = 0.0;
+    if ((rc = cr_profile_step_kernel(ctx, reps, &ms))) return rc;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = lanes;
+    }
+  }
+  int rc = cr_set_lanes(ctx, best);
+  if (rc) return rc;
+  if (lanes_out) *lanes_out = best;
+  return CR_OK;
+}
+
 int cr_set_use_graphs(cr_ctx* ctx, int on) {
   if (!ctx) return CR_EINVAL;
   ctx->use_graphs = on != 0;

@@ -215,6 +215,11 @@ class DPM2D:
 
     def setUseGraphs(self, on): self._call("cr_set_use_graphs", int(bool(on)))
 
+    def autotune(self, reps=50):
+        out = C.c_int()
+        self._call("cr_autotune", int(reps), C.byref(out))
+        return out.value
+
     def profileStepKernel(self, reps=100):
         out = C.c_double()
         self._call("cr_profile_step_kernel", int(reps), C.byref(out))

@@ -219,6 +219,10 @@ int cr_get_lanes(const cr_ctx* ctx, int* lanes);
 /* 1: step sequences run as captured CUDA graphs with conditional rebuild
  * nodes (default); 0: direct launches with a host check after each op. */
 int cr_set_use_graphs(cr_ctx* ctx, int on);
+/* Times the fused step kernel for every lane count whose tile holds the
+ * largest ring (cr_profile_step_kernel, `reps` launches each) and keeps the
+ * fastest; reports the choice.  Needs a neighbour list. */
+int cr_autotune(cr_ctx* ctx, long reps, int* lanes_out);
 
 #ifdef __cplusplus
 }
