@@ -224,6 +224,32 @@ int cr_set_use_graphs(cr_ctx* ctx, int on);
  * fastest; reports the choice.  Needs a neighbour list. */
 int cr_autotune(cr_ctx* ctx, long reps, int* lanes_out);
 
+/* ---- neighbour list without allocation -----------------------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory themselves (a host framework that hands out only fixed, pre-sized
+ * buffers; code that must not call cudaMalloc/cudaFree because they
+ * synchronise the device and are refused during stream capture): builds the
+ * same neighbour list as cr_calc_neighbor_list from caller-owned device
+ * arrays, keeping every temporary in one static device array of the library,
+ * so it calls no cudaMalloc, cudaFree or allocating library routine.
+ *   pos[2 Nv] (double, AoS), rad[Nv], ring_of[Nv] (int32 ring index): device
+ *   boxSize[2]: host; maxRad >= every radius; cutDistance as returned by
+ *   cr_set_displacement_cutoff; neighbors: device int32 [capacity][Nv]
+ *   (slot-major: neighbour s of vertex v at neighbors[s * Nv + v]); counts:
+ *   device int32 [Nv]; *maxCount: host, largest count; stream: cudaStream_t
+ *   (NULL = legacy default stream); the call synchronises that stream.
+ * Limits: Nv <= CR_NOALLOC_MAX_VERTICES and at most CR_NOALLOC_MAX_CELLS
+ * cells, else CR_EINVAL before any buffer is touched; CR_ENBR_OVERFLOW when a
+ * count exceeds capacity (counts are still complete).  The first call on a
+ * device looks up the scratch array's address (once per device): make it
+ * before any stream capture.  All calls share that array: calls that
+ * overlap on the GPU race and must be serialised. */
+#define CR_NOALLOC_MAX_VERTICES 65536
+#define CR_NOALLOC_MAX_CELLS 65536
+int cr_neighbor_list_noalloc(const double* pos, const double* rad, const int* ring_of, long numVertices,
+                             const double* boxSize, double maxRad, double cutDistance, long capacity,
+                             int* neighbors, int* counts, long* maxCount, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
