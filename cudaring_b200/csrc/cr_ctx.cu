@@ -22,7 +22,7 @@ using namespace cr;
 
 namespace {
 
-enum OpType { OP_DRIFT = 0, OP_TILE = 1, OP_FIRE_PRE = 2, OP_CHECK = 3 };
+enum OpType { OP_DRIFT = 0, OP_TILE = 1, OP_FIRE_PRE = 2, OP_CHECK = 3, OP_RIGID_DRIFT = 4 };
 
 struct Op {
   int type;
@@ -93,6 +93,9 @@ struct cr_ctx {
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
   double* fire_state = nullptr;   // [2][4]
+  // rigid rings
+  double2 *p_vel = nullptr, *p_force = nullptr;
+  double *p_angvel = nullptr, *p_torque = nullptr, *p_moi = nullptr, *v_torque = nullptr, *sp_angle = nullptr;
 
   // integrators
   int sim_kind = -1;  // Kind
@@ -190,6 +193,19 @@ StepArgs base_args(cr_ctx* ctx) {
   s.seed = ctx->seed;
   s.fire_tol = -1.0;
   return s;
+}
+
+RigidArgs rigid_args(cr_ctx* ctx) {
+  RigidArgs r;
+  r.p_vel = ctx->p_vel;
+  r.p_angle = ctx->p_angle;
+  r.p_angvel = ctx->p_angvel;
+  r.p_force = ctx->p_force;
+  r.p_torque = ctx->p_torque;
+  r.p_moi = ctx->p_moi;
+  r.v_torque = ctx->v_torque;
+  r.sp_angle = ctx->sp_angle;
+  return r;
 }
 
 int inter_kind(cr_ctx* ctx) {
@@ -364,7 +380,7 @@ std::vector<Op> make_ops(cr_ctx* ctx, int kind, long nsteps) {
       b ^= 1;
     }
   } else {
-    ops.push_back(Op{OP_DRIFT, b, b ^ 1, 0, 1, b ^ 1});
+    ops.push_back(Op{ctx->shape == CR_SHAPE_RIGID ? OP_RIGID_DRIFT : OP_DRIFT, b, b ^ 1, 0, 1, b ^ 1});
     b ^= 1;
     for (long i = 0; i < nsteps; i++) {
       const bool last = (i == nsteps - 1);
@@ -410,7 +426,14 @@ void enqueue_op(cr_ctx* ctx, cudaStream_t st, const Op& op, int kind, bool use_c
     case OP_TILE: {
       LaunchCfg c = tile_cfg(ctx);
       c.stream = st;
-      launch_tile(c, ctx->potential, inter_kind(ctx), MODE_STEP, ctx->p, a, s);
+      if (ctx->shape == CR_SHAPE_RIGID) launch_rigid(c, ctx->potential, MODE_STEP, ctx->p, a, s, rigid_args(ctx));
+      else launch_tile(c, ctx->potential, inter_kind(ctx), MODE_STEP, ctx->p, a, s);
+      break;
+    }
+    case OP_RIGID_DRIFT: {
+      LaunchCfg c = tile_cfg(ctx);
+      c.stream = st;
+      launch_rigid_drift(c, ctx->p, a, s, rigid_args(ctx));
       break;
     }
   }
@@ -687,7 +710,11 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
       (rc = dalloc(ctx, &ctx->cell_of, nv)) || (rc = dalloc(ctx, &ctx->slot, nv)) ||
       (rc = dalloc(ctx, &ctx->cell_vid, nv)) || (rc = dalloc(ctx, &ctx->cell_ring, nv)) ||
       (rc = dalloc(ctx, &ctx->cell_pos, nv)) || (rc = dalloc(ctx, &ctx->cell_rad, nv)) ||
-      (rc = dalloc(ctx, &ctx->status, 1)) || (rc = dalloc(ctx, &ctx->fire_state, 8))) {
+      (rc = dalloc(ctx, &ctx->status, 1)) || (rc = dalloc(ctx, &ctx->fire_state, 8)) ||
+      (rc = dalloc(ctx, &ctx->p_vel, np)) || (rc = dalloc(ctx, &ctx->p_force, np)) ||
+      (rc = dalloc(ctx, &ctx->p_angvel, np)) || (rc = dalloc(ctx, &ctx->p_torque, np)) ||
+      (rc = dalloc(ctx, &ctx->p_moi, np)) || (rc = dalloc(ctx, &ctx->v_torque, nv)) ||
+      (rc = dalloc(ctx, &ctx->sp_angle, np))) {
     cr_destroy(ctx);
     return rc;
   }
@@ -735,7 +762,8 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->perimeter, ctx->p_angle, ctx->vertex_area, ctx->ring_of, ctx->ring_first, ctx->ring_nv,
                   ctx->zero_cnt, ctx->pp_of, ctx->tiles, ctx->nbr, ctx->nbr_cnt, ctx->cell_of, ctx->slot,
                   ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
-                  ctx->partials, ctx->status, ctx->fire_state};
+                  ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
+                  ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
@@ -1336,6 +1364,126 @@ int cr_get_fire_state(cr_ctx* ctx, double* out3) {
   out3[0] = st[b * 4];
   out3[1] = st[b * 4 + 1];
   out3[2] = st[b * 4 + 2];
+  return CR_OK;
+}
+
+// ------------------------------------------------------------------ rigid rings
+
+int cr_calc_rigid_force_energy(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  if (ctx->interaction != CR_INTERACTION_VERTEX_VERTEX)
+    return ctx->fail(CR_ENOTSUP, "rigid rings run the vertex-vertex interaction");
+  StepArgs s = base_args(ctx);
+  s.kind = KIND_NONE;
+  launch_rigid(tile_cfg(ctx), ctx->potential, MODE_FORCE, ctx->p, arrays(ctx, ctx->cur), s, rigid_args(ctx));
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+static int rigid_init(cr_ctx* ctx, double T, int readState) {
+  // DPM2D::initRigidNVE / initRigidLangevin (src/DPM2D.cu:3793-3838): angles
+  // and angular velocities start at zero, lastPos = pos, centroids current
+  int rc;
+  if (ctx->interaction != CR_INTERACTION_VERTEX_VERTEX)
+    return ctx->fail(CR_ENOTSUP, "rigid rings run the vertex-vertex interaction");
+  ctx->shape = CR_SHAPE_RIGID;
+  if ((rc = cr_reset_last_positions(ctx))) return rc;
+  if ((rc = reset_rng_step(ctx))) return rc;
+  CR_TRY(cudaMemsetAsync(ctx->p_angle, 0, CR_NP1, ctx->stream));
+  CR_TRY(cudaMemsetAsync(ctx->p_angvel, 0, CR_NP1, ctx->stream));
+  if (!readState) {
+    launch_rigid_inject(ctx->stream, ctx->np, ctx->p_vel, std::sqrt(T), ctx->seed, (1ull << 60) + ctx->rng_calls++);
+    ctx->launches++;
+    CR_TRY(cudaGetLastError());
+  }
+  if (!ctx->nbr_built && (rc = build_list(ctx, ctx->cur, ctx->cut_distance))) return rc;
+  if ((rc = cr_calc_rigid_force_energy(ctx))) return rc;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_init_rigid_nve(cr_ctx* ctx, double T, int readState) {
+  if (!ctx) return CR_EINVAL;
+  int rc = rigid_init(ctx, T, readState);
+  if (rc) return rc;
+  ctx->sim_kind = KIND_NVE;
+  ctx->T = T;
+  return CR_OK;
+}
+
+int cr_rigid_nve_loop(cr_ctx* ctx, long nsteps) {
+  if (!ctx || nsteps < 0) return CR_EINVAL;
+  if (ctx->shape != CR_SHAPE_RIGID || ctx->sim_kind != KIND_NVE)
+    return ctx->fail(CR_ESTATE, "cr_rigid_nve_loop before cr_init_rigid_nve");
+  if (nsteps == 0) return CR_OK;
+  return run_ops(ctx, KIND_NVE, nsteps);
+}
+
+int cr_init_rigid_langevin(cr_ctx* ctx, double T, double gamma, int readState) {
+  if (!ctx) return CR_EINVAL;
+  int rc = rigid_init(ctx, T, readState);
+  if (rc) return rc;
+  ctx->sim_kind = KIND_LANGEVIN;
+  ctx->T = T;
+  ctx->gamma = gamma;
+  ctx->noise = std::sqrt(2.0 * T * gamma / ctx->dt);
+  return CR_OK;
+}
+
+int cr_rigid_langevin_loop(cr_ctx* ctx, long nsteps) {
+  if (!ctx || nsteps < 0) return CR_EINVAL;
+  if (ctx->shape != CR_SHAPE_RIGID || ctx->sim_kind != KIND_LANGEVIN)
+    return ctx->fail(CR_ESTATE, "cr_rigid_langevin_loop before cr_init_rigid_langevin");
+  if (nsteps == 0) return CR_OK;
+  return run_ops(ctx, KIND_LANGEVIN, nsteps);
+}
+
+int cr_get_particle_velocities(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->p_vel, (size_t)ctx->np * sizeof(double2));
+}
+int cr_set_particle_velocities(cr_ctx* ctx, const double* in) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->p_vel, in, (size_t)ctx->np * sizeof(double2));
+}
+int cr_get_particle_angles(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->p_angle, CR_NP1);
+}
+int cr_set_particle_angles(cr_ctx* ctx, const double* in) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->p_angle, in, CR_NP1);
+}
+int cr_get_particle_angular_velocities(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->p_angvel, CR_NP1);
+}
+int cr_set_particle_angular_velocities(cr_ctx* ctx, const double* in) {
+  if (!ctx) return CR_EINVAL;
+  return upload(ctx, ctx->p_angvel, in, CR_NP1);
+}
+int cr_get_particle_forces(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->p_force, (size_t)ctx->np * sizeof(double2));
+}
+int cr_get_particle_torques(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->p_torque, CR_NP1);
+}
+int cr_get_vertex_torques(const cr_ctx* ctx, double* out) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, out, ctx->v_torque, CR_NV1);
+}
+int cr_get_particle_kinetic_energy(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  std::vector<double> v(2 * (size_t)ctx->np);
+  int rc = download(ctx, v.data(), ctx->p_vel, v.size() * sizeof(double));
+  if (rc) return rc;
+  double s = 0.0;
+  for (double x : v) s += x * x;
+  *out = 0.5 * s;  // DPM2D::getParticleKineticEnergy (src/DPM2D.cu:1101-1106)
   return CR_OK;
 }
 

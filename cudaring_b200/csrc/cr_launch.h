@@ -39,6 +39,24 @@ void launch_advance_angles(cudaStream_t st, int np, double* angle, double amp, u
 void launch_vertex_area(cudaStream_t st, int np, const int* ring_first, const int* ring_nv, const double* rad,
                         double* out);
 
+// cr_rigid.cu
+struct RigidArgs {
+  double2* p_vel;      // ring velocity (half-step velocity between ops of a sequence)
+  double* p_angle;     // ring orientation angle
+  double* p_angvel;    // ring angular velocity
+  double2* p_force;    // ring force (sum over vertices, plus thermostat / propulsion terms)
+  double* p_torque;    // ring torque / moment of inertia (angular acceleration)
+  double* p_moi;       // ring moment of inertia (unit vertex mass)
+  double* v_torque;    // per-vertex torque about the centroid
+  double* sp_angle;    // self-propulsion angle of active rigid rings
+};
+void launch_rigid(const LaunchCfg& c, int pot, int mode, const SysParams& p, const SysArrays& a, const StepArgs& s,
+                  const RigidArgs& r);
+void launch_rigid_drift(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s,
+                        const RigidArgs& r);
+void launch_rigid_inject(cudaStream_t st, int np, double2* p_vel, double amp, unsigned long long seed,
+                         unsigned long long stream);
+
 // cr_nbr.cu
 struct CellGrid {
   int ncx, ncy;       // cells per dimension (>= 3 each), or 0 for brute force

@@ -268,24 +268,32 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
   } else {
     // ---- MODE_STEP: integrator tail (src/Simulator.cu, src/FIRE.cu) ----------
     double sums[NSUM] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    if (t < nvt) {
-      const int v = v0 + t;
-      const unsigned long long step = (unsigned long long)st->rng_step;
-      if (s.active) {
-        // addSelfPropulsion (src/DPM2D.cu:1995-2035): the ring's angle takes a
-        // N(0, sqrt(2 dt / taup)) increment and is wrapped to [-pi, pi).
+    const unsigned long long step = (unsigned long long)st->rng_step;
+    if (s.active) {
+      // addSelfPropulsion (src/DPM2D.cu:1995-2035): the ring's angle takes a
+      // N(0, sqrt(2 dt / taup)) increment and is wrapped to [-pi, pi); the
+      // ring's first vertex updates it once and shares it through its s_theta
+      // slot, which the step tail no longer reads
+      if (t < nvt && k == 0) {
         double psi = s.p_angle[ring];
         const double2 z = philox_normal2(s.seed, 2ull * step + 1ull, (unsigned long long)ring);
         psi += s.sp_amp * z.x;
         psi = psi + kPi;
         psi = psi - 2.0 * kPi * floor(psi / (2.0 * kPi));
         psi = psi - kPi;
+        s.p_angle[ring] = psi;
+        s_theta[t] = psi;
+      }
+      __syncthreads();
+      if (t < nvt) {
         double sn, cs;
-        sincos(psi, &sn, &cs);
+        sincos(s_theta[lf], &sn, &cs);
         F.x += s.driving * cs;
         F.y += s.driving * sn;
-        if (k == 0) s.p_angle[ring] = psi;  // every vertex computed the same value
       }
+    }
+    if (t < nvt) {
+      const int v = v0 + t;
       double2 vh = s.vel[v];
       const double2 x = s_pos[t];
       double2 vn;

@@ -206,6 +206,31 @@ class DPM2D:
 
     def getFIREState(self): return self._get("cr_get_fire_state", 3)
 
+    # ------------------------------------------------------------ rigid rings
+    def calcRigidForceEnergy(self): self._call("cr_calc_rigid_force_energy")
+    def initRigidNVE(self, T, readState=False): self._call("cr_init_rigid_nve", T, int(bool(readState)))
+    def rigidNVELoop(self, nsteps=1): self._call("cr_rigid_nve_loop", int(nsteps))
+
+    def initRigidLangevin(self, T, gamma, readState=False):
+        self._call("cr_init_rigid_langevin", T, gamma, int(bool(readState)))
+
+    def rigidLangevinLoop(self, nsteps=1): self._call("cr_rigid_langevin_loop", int(nsteps))
+    def getParticleVelocities(self): return self._get("cr_get_particle_velocities", 2 * self.numParticles)
+    def setParticleVelocities(self, a): self._call("cr_set_particle_velocities", _f64(a).ctypes.data)
+    def getParticleAngles(self): return self._get("cr_get_particle_angles", self.numParticles)
+    def setParticleAngles(self, a): self._call("cr_set_particle_angles", _f64(a).ctypes.data)
+
+    def getParticleAngularVelocities(self):
+        return self._get("cr_get_particle_angular_velocities", self.numParticles)
+
+    def setParticleAngularVelocities(self, a):
+        self._call("cr_set_particle_angular_velocities", _f64(a).ctypes.data)
+
+    def getParticleForces(self): return self._get("cr_get_particle_forces", 2 * self.numParticles)
+    def getParticleTorques(self): return self._get("cr_get_particle_torques", self.numParticles)
+    def getVertexTorques(self): return self._get("cr_get_vertex_torques", self.numVertices)
+    def getParticleKineticEnergy(self): return self._scalar("cr_get_particle_kinetic_energy")
+
     def setLanes(self, lanes): self._call("cr_set_lanes", int(lanes))
 
     def getLanes(self):

@@ -164,6 +164,58 @@ def make_packing(nv_list, a0_list, calA0, phi: float, seed: int, jitter: float =
                    meta={"seed": seed, "phi": phi, "jitter": jitter, "placement": placement})
 
 
+def ellipse_vertices(nv: int, a: float, b: float, orientation: float) -> np.ndarray:
+    """nv points at equal arc length on the ellipse x=a cos t, y=b sin t,
+    counter-clockwise, rotated by ``orientation`` (BumpyEllipse::initEllipse,
+    src/BumpyEllipse.cu:39-75, places vertices at equal arc length too; here
+    the arc length is integrated numerically on a fine grid)."""
+    t = np.linspace(0.0, 2.0 * np.pi, 20001)
+    ds = np.hypot(a * np.sin(t), b * np.cos(t))
+    s = np.concatenate([[0.0], np.cumsum(0.5 * (ds[1:] + ds[:-1]) * np.diff(t))])
+    targets = np.arange(nv) * s[-1] / nv
+    tk = np.interp(targets, s, t)
+    x, y = a * np.cos(tk), b * np.sin(tk)
+    c, sn = np.cos(orientation), np.sin(orientation)
+    return np.stack([c * x - sn * y, sn * x + c * y], axis=1)
+
+
+def make_ellipse_packing(n: int, nv: int, ratio_range: tuple[float, float], phi: float, seed: int,
+                         a0: float = 1.0, placement: str = "rsa") -> Packing:
+    """Rigid "bumpy ellipse" rings: aspect ratio a/b uniform in ratio_range,
+    area a0 (a = sqrt(ratio a0 / pi), b = a / ratio), nv vertices at equal arc
+    length, vertex radius half the arc spacing, random orientation.  The box
+    is sized with the rigid packing fraction sum(a0) / L^2 (DPM2D::getRigidPhi,
+    src/DPM2D.cu:1242-1252); ``placement`` "rsa" places circumscribing discs
+    without overlap, "uniform" anywhere."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    ratios = rng.uniform(ratio_range[0], ratio_range[1], n)
+    orient = rng.uniform(0.0, 2.0 * np.pi, n)
+    L = math.sqrt(n * a0 / phi)
+    pts, rads, l0s, th0s, rcirc = [], [], [], [], []
+    for q in range(n):
+        a = math.sqrt(ratios[q] * a0 / math.pi)
+        b = a / ratios[q]
+        v = ellipse_vertices(nv, a, b, orient[q])
+        seg = np.roll(v, -1, axis=0) - v
+        lens = np.hypot(seg[:, 0], seg[:, 1])
+        r = 0.5 * lens.mean()
+        pts.append(v)
+        rads.append(np.full(nv, r))
+        l0s.append(lens)
+        th0s.append(np.full(nv, 2.0 * np.pi / nv))
+        rcirc.append(a + r)
+    rcirc = np.array(rcirc)
+    if placement == "rsa":
+        centres = rsa_centres(rcirc, L, rng)
+    else:
+        centres = rng.uniform(0.0, L, size=(n, 2))
+    pos = np.concatenate([p + c for p, c in zip(pts, centres)]).reshape(-1)
+    nv_list = np.full(n, nv, dtype=np.int64)
+    return Packing(nv_list=nv_list, pos=pos, vel=np.zeros_like(pos), rad=np.concatenate(rads),
+                   l0=np.concatenate(l0s), theta0=np.concatenate(th0s), a0=np.full(n, a0), box=np.array([L, L]),
+                   centres=centres, meta={"seed": seed, "phi": phi, "ratios": ratios, "placement": placement})
+
+
 def workload_config(index: int, scale_rings: int | None = None) -> dict:
     """Ring counts and parameters of the five benchmark configurations.
 
@@ -189,6 +241,11 @@ def workload_config(index: int, scale_rings: int | None = None) -> dict:
         a0 = [1.0] * (n // 2) + [1.4 ** 2] * (n - n // 2)
         return dict(nv=nv, a0=a0, calA0=1.05, phi=0.85, potential="lennardJones", interaction="vertexSmooth",
                     LJcutoff=2.5, ea=1e5, el=20.0, eb=10.0, ec=1.0, dt=0.002, T=0.01)
+    if index == 2:
+        n = scale_rings or 4096
+        return dict(rigid=True, n=n, nv=24, ratio_range=(1.2, 2.0), phi=0.65, potential="wca",
+                    interaction="vertexVertex", ea=0.0, el=0.0, eb=0.0, ec=1.0, dt=0.001, T=0.1, gamma=1.0,
+                    driving=0.1, taup=100.0)
     if index == 4:
         n = scale_rings or 256
         return dict(nv=[32] * n, a0=[1.0] * n, calA0=1.0, phi=0.88, potential="harmonic",

@@ -200,6 +200,38 @@ int cr_fire_minimize(cr_ctx* ctx, double tol, long maxIter, long* iterations, do
 /* FIRE scalars {dt, a, numStep} after the last iteration. */
 int cr_get_fire_state(cr_ctx* ctx, double* out3);
 
+/* ---- rigid rings (src/DPM2D.cu:2128-2179, src/Simulator.cu:241-371) ----- */
+/* DPM2D::calcRigidForceEnergy (include/DPM2D.h:567): vertex-vertex forces,
+ * per-vertex torque about the ring centroid, ring force, torque / moment of
+ * inertia (the angular acceleration), moment of inertia and energy. */
+int cr_calc_rigid_force_energy(cr_ctx* ctx);
+/* DPM2D::initRigidNVE / rigidNVELoop (include/DPM2D.h:697-699): ring
+ * velocities N(0, sqrt(T)) with zero mean unless readState; angles and
+ * angular velocities start at zero. */
+int cr_init_rigid_nve(cr_ctx* ctx, double T, int readState);
+int cr_rigid_nve_loop(cr_ctx* ctx, long nsteps);
+/* DPM2D::initRigidLangevin / rigidLangevinLoop (include/DPM2D.h:693-695).
+ * Deliberate fix: the ring velocity takes noise*xi - gamma*v with noise =
+ * sqrt(2 T gamma / dt); the reference adds unscaled N(0,1) draws
+ * (src/Simulator.cu:272-289).  Active rigid rings (particle type active) are
+ * pushed along a self-propulsion angle that diffuses with 1/taup. */
+int cr_init_rigid_langevin(cr_ctx* ctx, double T, double gamma, int readState);
+int cr_rigid_langevin_loop(cr_ctx* ctx, long nsteps);
+/* Ring state (include/DPM2D.h:339-354): velocities [2 Np], angles [Np],
+ * angular velocities [Np], forces [2 Np], torques [Np] (angular
+ * accelerations), vertex torques [Nv]. */
+int cr_get_particle_velocities(const cr_ctx* ctx, double* out);
+int cr_set_particle_velocities(cr_ctx* ctx, const double* in);
+int cr_get_particle_angles(const cr_ctx* ctx, double* out);
+int cr_set_particle_angles(cr_ctx* ctx, const double* in);
+int cr_get_particle_angular_velocities(const cr_ctx* ctx, double* out);
+int cr_set_particle_angular_velocities(cr_ctx* ctx, const double* in);
+int cr_get_particle_forces(const cr_ctx* ctx, double* out);
+int cr_get_particle_torques(const cr_ctx* ctx, double* out);
+int cr_get_vertex_torques(const cr_ctx* ctx, double* out);
+/* DPM2D::getParticleKineticEnergy (include/DPM2D.h:415): 1/2 sum |v_ring|^2 */
+int cr_get_particle_kinetic_energy(cr_ctx* ctx, double* out);
+
 /* ---- run statistics and measurement ------------------------------------ */
 /* Kernels this context has run since creation (direct launches, graph-node
  * kernels per replay and the rebuild kernels of conditional nodes). */

@@ -68,11 +68,23 @@ class OracleState:
         self.forces()
         self.vel += 0.5 * dt * self.force
 
-    def langevin_step(self, dt, gamma, noise_amp, xi):
+    def self_propulsion(self, driving, dpsi):
+        """DPM2D::addSelfPropulsion (src/DPM2D.cu:1995-2035) with given increments."""
+        if not hasattr(self, "pangle"):
+            self.pangle = np.zeros(self.s.np)
+        a = self.pangle + dpsi + math.pi
+        a = a - 2.0 * math.pi * np.floor(a / (2.0 * math.pi))
+        self.pangle = a - math.pi
+        p = self.pangle[self.s.pid]
+        self.force = self.force + driving * np.stack([np.cos(p), np.sin(p)], axis=1).reshape(-1)
+
+    def langevin_step(self, dt, gamma, noise_amp, xi, driving=0.0, dpsi=None):
         self.vel += 0.5 * dt * self.force
         self.pos += dt * self.vel
         self.check()
         self.forces()
+        if dpsi is not None:
+            self.self_propulsion(driving, dpsi)
         r = xi[self.s.pid].reshape(-1)
         self.force = self.force + noise_amp * r - gamma * self.vel
         self.vel += 0.5 * dt * self.force
@@ -126,6 +138,56 @@ class OracleFIRE:
         st.check()
         st.forces()
         st.vel += 0.5 * self.dt * st.force
+
+
+class OracleRigid:
+    """Rigid rings: RigidNVE::integrate (src/Simulator.cu:316-371) with forces
+    from oc_rigid_force_energy and vertex moves from oc_translate_rotate."""
+
+    def __init__(self, sys_: System, pk, cutoff_: float = 0.5):
+        import ctypes as C
+
+        from . import lib
+
+        self.C, self.L = C, lib()
+        self.s = sys_
+        self.pos = pk.pos.copy()
+        self.rad = pk.rad.copy()
+        size = 2 * self.rad.mean()
+        self.cut_distance = sys_.cut_distance(cutoff_)
+        self.cutoff = cutoff_ * size
+        self.update_count = 0
+        self.s.neighbor_list(self.pos, self.rad, self.cut_distance)
+        self.last_pos = self.pos.copy()
+        self.forces()
+        self.pvel = np.zeros(2 * sys_.np)
+        self.pangvel = np.zeros(sys_.np)
+        self.pangle = np.zeros(sys_.np)
+
+    def forces(self):
+        self.out = self.s.rigid_force_energy(self.pos, self.rad)
+        self.ppos = self.out["ppos"]
+
+    def check(self):
+        d = (self.pos - self.last_pos).reshape(-1, 2)
+        box = np.array([self.s.s.lx, self.s.s.ly])
+        d -= box * np.round(d / box)
+        if np.any(3 * np.sqrt((d * d).sum(1)) > self.cutoff):
+            self.s.neighbor_list(self.pos, self.rad, self.cut_distance)
+            self.last_pos = self.pos.copy()
+            self.update_count += 1
+
+    def nve_step(self, dt):
+        plast, alast = self.ppos.copy(), self.pangle.copy()
+        self.pvel += 0.5 * dt * self.out["p_force"]
+        self.pangvel += 0.5 * dt * self.out["p_torque"]
+        pnew = self.ppos + dt * self.pvel
+        self.pangle = self.pangle + dt * self.pangvel
+        self.L.oc_translate_rotate(self.C.byref(self.s.s), pnew, plast, self.pangle, alast, self.pos)
+        self.check()
+        self.forces()
+        self.pvel += 0.5 * dt * self.out["p_force"]
+        self.pangvel += 0.5 * dt * self.out["p_torque"]
 
 
 def philox_noise(seed: int, stream: int, num_rings: int) -> np.ndarray:

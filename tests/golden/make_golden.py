@@ -192,8 +192,124 @@ def traj_cases():
     print("traj_langevin_harmonic_vv: done")
 
 
+RIGID_FIELDS = {"torque": 11, "p_force": 12, "p_torque": 13, "p_angle": 14, "moi": 15, "p_vel": 16,
+                "p_angvel": 17}
+
+
+def stochastic_cases():
+    # BAOAB, Brownian, driven Brownian and active Langevin with the library's
+    # Philox draws (seed, stream 2s for the thermostat of step s, 2s+1 for the
+    # self-propulsion angle) injected into the reference kernels.
+    seed = 4242
+    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 204)
+    rng = np.random.default_rng(5)
+    vel = np.repeat(rng.normal(0.0, 0.1, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
+    npart = pk.num_particles
+    dt, T, gamma, nsteps = 0.005, 0.01, 1.0, 60
+
+    def fresh():
+        pk.vel = vel.copy()
+        R, cut = setup_ref(pk, "harmonic", "vertexVertex")
+        R.ref_set_time_step(dt)
+        R.ref_calc_neighbor_list(cut)
+        R.ref_reset_last_positions()
+        R.ref_calc_force_energy()
+        return R, cut
+
+    xi = np.concatenate([philox_noise(seed, 2 * s, npart).reshape(-1) for s in range(nsteps)])
+    common = dict(potential=0, interaction=0, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, dt=dt, nsteps=nsteps,
+                  T=T, gamma=gamma, seed=seed)
+
+    R, cut = fresh()
+    gf = np.exp(-gamma * dt)
+    amp = np.sqrt(1 - np.exp(-2 * gamma * dt)) * np.sqrt(T)
+    R.ref_baoab_loop(nsteps, gf, amp, xi.ctypes.data)
+    d = inputs(pk, cut_distance=cut, **common)
+    d.update(grab(R, pk, ["pos", "vel", "force"]))
+    np.savez_compressed(os.path.join(OUT, "traj_baoab_harmonic_vv.npz"), **d)
+
+    R, cut = fresh()
+    amp = np.sqrt(2.0 * T * gamma / dt)
+    R.ref_brownian_loop(nsteps, gamma, amp, xi.ctypes.data, 0.0, None)
+    d = inputs(pk, cut_distance=cut, **common)
+    d.update(grab(R, pk, ["pos", "vel", "force"]))
+    np.savez_compressed(os.path.join(OUT, "traj_brownian_harmonic_vv.npz"), **d)
+
+    R, cut = fresh()
+    R.ref_brownian_loop(nsteps, gamma, amp, None, 0.0, None)
+    d = inputs(pk, cut_distance=cut, **common)
+    d.update(grab(R, pk, ["pos", "vel", "force"]))
+    np.savez_compressed(os.path.join(OUT, "traj_drivenbrownian_harmonic_vv.npz"), **d)
+
+    # active rings under Langevin: f0 = 0.05, taup = 10
+    driving, taup = 0.05, 10.0
+    R, cut = fresh()
+    R.ref_set_types(0, 0, 0, 1)
+    sp_amp = np.sqrt(2.0 * dt / taup)
+    dpsi = np.concatenate([sp_amp * philox_noise(seed, 2 * s + 1, npart)[:, 0] for s in range(nsteps)])
+    R.ref_langevin_loop(nsteps, gamma, amp, xi.ctypes.data, driving, dpsi.ctypes.data)
+    d = inputs(pk, cut_distance=cut, driving=driving, taup=taup, **common)
+    d.update(grab(R, pk, ["pos", "vel", "force"]))
+    ang = np.zeros(npart)
+    R.ref_get(14, ang)
+    d["out_p_angle"] = ang
+    np.savez_compressed(os.path.join(OUT, "traj_active_langevin_harmonic_vv.npz"), **d)
+    print("stochastic cases: done")
+
+
+def rigid_cases():
+    # Rigid bumpy ellipses, WCA vertex-vertex: an NVE run from a non-overlapping
+    # placement, then the force/torque sums at its final (colliding) state.
+    pk = synth.make_ellipse_packing(64, 24, (1.2, 2.0), 0.25, seed=20261203 + 300)
+    rng = np.random.default_rng(11)
+    pvel = rng.normal(0.0, 0.3, 2 * pk.num_particles)
+    pang = rng.normal(0.0, 0.5, pk.num_particles)
+    dt, nsteps = 0.002, 400
+    R, cut = setup_ref(pk, "wca", "vertexVertex")
+    R.ref_set_time_step(dt)
+    R.ref_calc_neighbor_list(cut)
+    R.ref_reset_last_positions()
+    R.ref_calc_rigid_force_energy()
+    R.ref_set_particle_state(None, pvel.ctypes.data, None, pang.ctypes.data)
+    R.ref_rigid_nve_loop(nsteps)
+    d = inputs(pk, potential=3, interaction=0, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, dt=dt,
+               nsteps=nsteps, cut_distance=cut)
+    d["p_vel"] = pvel
+    d["p_angvel"] = pang
+    d.update(grab(R, pk, ["pos", "ppos", "force"]))
+    for name, fid, n in (("p_vel", 16, 2 * pk.num_particles), ("p_angvel", 17, pk.num_particles),
+                         ("p_angle", 14, pk.num_particles), ("p_force", 12, 2 * pk.num_particles)):
+        a = np.zeros(n)
+        R.ref_get(fid, a)
+        d["out_" + name] = a
+    d["out_update_count"] = np.asarray(R.ref_update_count())
+    np.savez_compressed(os.path.join(OUT, "traj_rigid_nve_wca.npz"), **d)
+    print(f"traj_rigid_nve_wca: updates={int(d['out_update_count'])} maxF={np.abs(d['out_force']).max():.3e}")
+
+    pk.pos = d["out_pos"].copy()
+    R, cut = setup_ref(pk, "wca", "vertexVertex")
+    R.ref_calc_neighbor_list(cut)
+    R.ref_calc_rigid_force_energy()
+    d = inputs(pk, potential=3, interaction=0, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, cut_distance=cut)
+    d.update(grab(R, pk, ["force", "energy", "p_energy", "ppos"]))
+    for name, fid in (("torque", 11), ("p_force", 12), ("p_torque", 13), ("moi", 15)):
+        n = pk.num_vertices if name == "torque" else (2 if name == "p_force" else 1) * pk.num_particles
+        a = np.zeros(n)
+        R.ref_get(fid, a)
+        d["out_" + name] = a
+    np.savez_compressed(os.path.join(OUT, "rigid_force_wca.npz"), **d)
+    print(f"rigid_force_wca: nv={pk.num_vertices} maxF={np.abs(d['out_force']).max():.3e}")
+
+
 if __name__ == "__main__":
     if not oracle.ref_available():
         oracle.build()
-    force_cases()
-    traj_cases()
+    which = sys.argv[1:] or ["force", "traj", "stochastic", "rigid"]
+    if "force" in which:
+        force_cases()
+    if "traj" in which:
+        traj_cases()
+    if "stochastic" in which:
+        stochastic_cases()
+    if "rigid" in which:
+        rigid_cases()

@@ -127,6 +127,26 @@ def test_langevin_trajectory_philox(cuda_device):
     assert rel_inf(d.getVertexVelocities(), g["out_vel"]) < 1e-9
 
 
+@pytest.mark.parametrize("kind", ["baoab", "brownian", "drivenbrownian", "active_langevin"])
+def test_stochastic_integrators_match_reference(cuda_device, kind):
+    g = load_golden(golden_files(f"traj_{kind}_harmonic_vv")[0])
+    d = _prepared(g)
+    d.setSeed(int(g["param_seed"]))
+    noise = {"baoab": simControl.noiseEnum.baoab, "brownian": simControl.noiseEnum.brownian,
+             "drivenbrownian": simControl.noiseEnum.drivenBrownian,
+             "active_langevin": simControl.noiseEnum.langevin}[kind]
+    d.setNoiseType(noise)
+    if kind == "active_langevin":
+        d.setParticleType(simControl.particleEnum.active)
+        d.setSelfPropulsionParams(float(g["param_driving"]), float(g["param_taup"]))
+    d.initLangevin(float(g["param_T"]), float(g["param_gamma"]), readState=True)
+    d.langevinLoop(int(g["param_nsteps"]))
+    assert rel_inf(d.getVertexPositions(), g["out_pos"]) < 1e-12
+    assert rel_inf(d.getVertexVelocities(), g["out_vel"]) < 1e-9
+    if kind == "active_langevin":
+        assert np.allclose(d.getParticleAngles(), g["out_p_angle"], rtol=0, atol=1e-12)
+
+
 def _lj_smooth_packing(n, phi=0.40, seed=5, placement="rsa"):
     c = synth.workload_config(1, n)
     return c, synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=seed, placement=placement)

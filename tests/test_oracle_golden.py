@@ -104,6 +104,60 @@ def test_langevin_trajectory_with_philox_noise():
     assert rel_inf(st.vel, g["out_vel"]) < 1e-10
 
 
+def test_rigid_force_matches_reference():
+    g = load_golden(golden_files("rigid_force_wca")[0])
+    S = system_of(g)
+    S.neighbor_list(g["pos"], g["rad"], float(g["param_cut_distance"]))
+    out = S.rigid_force_energy(g["pos"], g["rad"])
+    assert rel_inf(out["force"], g["out_force"]) < TOL
+    assert rel_inf(out["p_force"], g["out_p_force"]) < TOL
+    assert rel_inf(out["torque"], g["out_torque"]) < TOL
+    assert rel_inf(out["p_torque"], g["out_p_torque"]) < 1e-11
+    assert np.allclose(out["moi"], g["out_moi"], rtol=1e-12, atol=0)
+    assert np.allclose(out["ppos"], g["out_ppos"], rtol=1e-13, atol=1e-13)
+    assert rel_inf(out["p_energy"], g["out_p_energy"]) < TOL
+
+
+def test_rigid_nve_trajectory():
+    from oracle.integrators import OracleRigid
+
+    g = load_golden(golden_files("traj_rigid_nve_wca")[0])
+    rig = OracleRigid(system_of(g), packing_of(g))
+    rig.pvel = g["p_vel"].copy()
+    rig.pangvel = g["p_angvel"].copy()
+    for _ in range(int(g["param_nsteps"])):
+        rig.nve_step(float(g["param_dt"]))
+    assert rig.update_count == int(g["out_update_count"])
+    assert rel_inf(rig.pos, g["out_pos"]) < 1e-11
+    assert rel_inf(rig.pvel, g["out_p_vel"]) < 1e-8
+    assert rel_inf(rig.pangvel, g["out_p_angvel"]) < 1e-8
+    assert rel_inf(rig.pangle, g["out_p_angle"]) < 1e-9
+
+
+@pytest.mark.parametrize("kind", ["baoab", "brownian", "drivenbrownian", "active_langevin"])
+def test_stochastic_integrators_with_philox_noise(kind):
+    g = load_golden(golden_files(f"traj_{kind}_harmonic_vv")[0])
+    st = _state(g)
+    dt, T, gamma, seed = (float(g["param_dt"]), float(g["param_T"]), float(g["param_gamma"]), int(g["param_seed"]))
+    npart = len(g["nv_list"])
+    for s in range(int(g["param_nsteps"])):
+        xi = philox_noise(seed, 2 * s, npart)
+        if kind == "baoab":
+            st.baoab_step(dt, np.exp(-gamma * dt), np.sqrt(1 - np.exp(-2 * gamma * dt)) * np.sqrt(T), xi)
+        elif kind == "brownian":
+            st.brownian_step(dt, gamma, np.sqrt(2 * T * gamma / dt), xi)
+        elif kind == "drivenbrownian":
+            st.brownian_step(dt, gamma, 0.0, None)
+        else:
+            sp = np.sqrt(2 * dt / float(g["param_taup"]))
+            st.langevin_step(dt, gamma, np.sqrt(2 * T * gamma / dt), xi, float(g["param_driving"]),
+                             sp * philox_noise(seed, 2 * s + 1, npart)[:, 0])
+    assert rel_inf(st.pos, g["out_pos"]) < 1e-12
+    assert rel_inf(st.vel, g["out_vel"]) < 1e-9
+    if kind == "active_langevin":
+        assert np.allclose(st.pangle, g["out_p_angle"], rtol=0, atol=1e-12)
+
+
 def test_philox_known_answer():
     # Known-answer vectors of Philox4x32-10 published with Random123 (kat_vectors):
     # counter 0, key 0 and counter/key of all ones.
