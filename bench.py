@@ -2,14 +2,19 @@
 
 Workload (default): 1024 rings, nv 32/45 bidisperse 1:1.4 (39,424 vertices),
 smooth vertex-segment Lennard-Jones (rc 2.5 sigma, epsilon 1), calA0 1.05,
-packing fraction 0.85, ka=kl=1, kb=0.01, NVE velocity Verlet at dt 0.002 with
-ring velocities drawn at T 0.01, FP64.  Inputs are synthetic and seeded: rings
-placed without overlap at phi 0.40, compressed to 0.85 with FIRE
-(cudaring_b200.workloads), then thermalised; none of that is timed.
+packing fraction 0.85, shape constants ea 1e5, el 20, eb 10, NVE velocity
+Verlet at dt 0.002 with ring velocities drawn at T 0.01.  Inputs are synthetic
+and seeded: rings placed without overlap at phi 0.40, compressed to 0.85 with
+FIRE (cudaring_b200.workloads), then given thermal velocities; none of that is
+timed.
 
 One bench step = ``--md-steps`` NVE steps (default 1000) through one
 ``DPM2D.NVELoop`` call, neighbour-list rebuilds included as they fall due.
-``value`` = vertices x MD steps x bench steps / device time (max over ranks);
+``value`` = vertices x MD steps x bench steps / device time (max over ranks)
+for ``--precision`` (default mixed: FP32 pair terms, everything else FP64);
+the other precision is timed the same way from the same start state and
+reported under ``precision_comparison`` with the force error of the mixed
+path against FP64 and both paths' NVE energy drift over ``--drift-steps``.
 ``e2e`` adds, every bench step, the upload of positions and velocities from
 pinned host memory and the download of positions, velocities and the
 potential energy through the public API.
@@ -52,6 +57,12 @@ def parse():
     ap.add_argument("--profile-kernel", action="store_true",
                     help="only time the fused step kernel (few launches; for ncu captures)")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per vertex of the fused kernel (0: library default)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="arithmetic of the timed run (the other one is timed for comparison)")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the other precision's run and the accuracy / energy-drift runs")
+    ap.add_argument("--drift-steps", type=int, default=100000,
+                    help="NVE steps of each precision's energy-drift run (untimed)")
     return ap.parse_args()
 
 
@@ -151,11 +162,12 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def committed_traffic() -> dict | None:
+def committed_traffic(precision: str) -> dict | None:
+    """DRAM bytes per launch of the step kernel from a committed ncu capture."""
     path = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
-            return json.load(f)
+            return json.load(f).get(precision)
     return None
 
 
@@ -185,7 +197,8 @@ def barrier(world: int):
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_reference_rate(d, threads: int, target_seconds: float = 12.0, rebuild_every: float | None = None) -> dict:
+def cpu_reference_rate(d, c: dict, threads: int, target_seconds: float = 12.0,
+                       rebuild_every: float | None = None) -> dict:
     """Reference kernels compiled as host code (oracle/_ref): one neighbour build
     plus NVE steps on the same prepared state; vertex-steps/s with the build
     amortised over the rebuild interval measured on the GPU run."""
@@ -206,9 +219,9 @@ def cpu_reference_rate(d, threads: int, target_seconds: float = 12.0, rebuild_ev
     R.ref_create(len(nvl), nvl)
     R.ref_set_box(float(box[0]), float(box[1]))
     R.ref_set_types(1, 1, 0, 0)
-    R.ref_set_energy_costs(1.0, 1.0, 0.01, 1.0)
-    R.ref_set_lj_cutoff(2.5)
-    R.ref_set_time_step(0.002)
+    R.ref_set_energy_costs(c["ea"], c["el"], c["eb"], c["ec"])
+    R.ref_set_lj_cutoff(c["LJcutoff"])
+    R.ref_set_time_step(c["dt"])
     R.ref_set_state(pos.ctypes.data, vel.ctypes.data, rad.ctypes.data, l0.ctypes.data, th0.ctypes.data,
                     a0.ctypes.data)
     cut = R.ref_set_displacement_cutoff(0.5, 2 * rad.mean())
@@ -239,6 +252,9 @@ def cpu_reference_rate(d, threads: int, target_seconds: float = 12.0, rebuild_ev
 
 
 # ------------------------------------------------------------------- main
+PREC_DTYPE = {"mixed": "f64 state + f32 pair terms", "fp64": "f64"}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -258,14 +274,19 @@ def main():
     d, info = prepared_state(args, rank)
     nv, npr = d.numVertices, d.numParticles
     if args.profile_kernel:
+        d.setPrecision(args.precision)
         ms = d.profileStepKernel(3)
-        print(json.dumps({"profile_kernel_ms": ms, "vertices": nv, "lanes": d.getLanes()}), flush=True)
+        print(json.dumps({"profile_kernel_ms": ms, "vertices": nv, "lanes": d.getLanes(),
+                          "precision": args.precision}), flush=True)
         d.close()
         return
     c = info["config"]
     d.setTimeStep(c["dt"])
     d.setSeed(1000 + rank)
     d.initNVE(c["T"], readState=False)
+    cut = d.setDisplacementCutoff(0.5, 2.0 * d.getMeanVertexRadius())
+    # the thermal start state that every run below begins from
+    x0, v0 = d.getVertexPositions(), d.getVertexVelocities()
     t_prep = time.perf_counter() - t_prep
 
     import ctypes
@@ -280,34 +301,53 @@ def main():
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
 
-    # warm-up (also compiles and caches the CUDA graphs)
-    for _ in range(args.warmup):
-        d.NVELoop(M)
-        l2_flush()
-    torch.cuda.synchronize()
-    upd0 = d.getUpdateCount()
-    launches0 = d.getLaunchCount()
-    e0 = d.getEnergy()
+    def restart(precision):
+        d.setPrecision(precision)
+        d.setVertexPositions(x0)
+        d.setVertexVelocities(v0)
+        d.calcNeighborList(cut)
+        d.calcForceEnergy()
+        d.initNVE(0.0, readState=True)
 
-    barrier(world)
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        for _ in range(args.steps):
+    def timed_run(precision):
+        restart(precision)
+        # warm-up (also captures and instantiates the CUDA graphs)
+        for _ in range(args.warmup):
             d.NVELoop(M)
             l2_flush()
-        ev1.record(stream)
         torch.cuda.synchronize()
-    barrier(world)
-    ms_total = max_over_ranks(ev0.elapsed_time(ev1), world)
-    launches = d.getLaunchCount() - launches0
-    updates = d.getUpdateCount() - upd0
-    e1 = d.getEnergy()
-    vertex_steps = nv * M * args.steps * world
-    value = vertex_steps / (ms_total / 1e3)
+        upd0, launches0, e0 = d.getUpdateCount(), d.getLaunchCount(), d.getEnergy()
+        barrier(world)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clocks:
+            ev0.record(stream)
+            for _ in range(args.steps):
+                d.NVELoop(M)
+                l2_flush()
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        barrier(world)
+        ms_total = max_over_ranks(ev0.elapsed_time(ev1), world)
+        return {"ms_total": ms_total, "value": nv * M * args.steps * world / (ms_total / 1e3),
+                "launches": d.getLaunchCount() - launches0, "updates": d.getUpdateCount() - upd0,
+                "energy_change_rel": abs(d.getEnergy() - e0) / abs(e0) if e0 else None,
+                "clocks": clocks.summary()}
 
-    # e2e through the public API with host buffers
+    def kernel_roofline(precision):
+        d.setPrecision(precision)
+        ms_launch = ctypes.c_double()
+        d._call("cr_profile_step_kernel", 200, ctypes.byref(ms_launch))
+        bytes_per_launch = 88 * nv + 8 * npr
+        achieved = bytes_per_launch / (ms_launch.value * 1e-3) / 1e9
+        return ms_launch.value, bytes_per_launch, achieved
+
+    prim = args.precision
+    run = timed_run(prim)
+    value = run["value"]
+    x_end = d.getVertexPositions()
+
+    # e2e through the public API with host buffers (same precision)
     e2e = None
     if not args.no_e2e:
         hpos = torch.empty(2 * nv, dtype=torch.float64, pin_memory=True).numpy()
@@ -317,7 +357,6 @@ def main():
         n_e2e = max(1, min(args.steps, 5))
         barrier(world)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
         ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ea.record(stream)
         for _ in range(n_e2e):
@@ -334,39 +373,50 @@ def main():
                "h2d_bytes_per_step": 2 * 16 * nv, "d2h_bytes_per_step": 2 * 16 * nv + 8}
 
     # roofline of the dominant kernel: the fused force + NVE step kernel
-    ms_launch = ctypes.c_double()
-    d._call("cr_profile_step_kernel", 200, ctypes.byref(ms_launch))
-    bytes_per_launch = 88 * nv + 8 * npr
-    achieved = bytes_per_launch / (ms_launch.value * 1e-3) / 1e9
+    ms_launch, bytes_per_launch, achieved = kernel_roofline(prim)
     peaks = measured_peaks()
-    traffic = committed_traffic()
+    traffic = committed_traffic(prim)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                 "traffic": traffic.get("bytes_per_launch") if traffic else None,
-                "kernel": "k_tile<LJ, smooth, step>", "ms_per_launch": ms_launch.value,
+                "kernel": f"k_tile<LJ, smooth, step, {prim}>", "ms_per_launch": ms_launch,
                 "algorithmic_bytes_per_launch": bytes_per_launch}
+
+    comparison = None
+    if not args.no_compare:
+        other = "fp64" if prim == "mixed" else "mixed"
+        orun = timed_run(other)
+        oms, _, oach = kernel_roofline(other)
+        comparison = {other: {"value": orun["value"], "ms_per_step": orun["ms_total"] / args.steps,
+                              "ms_per_launch": oms, "roofline_frac": oach / peaks["hbm_gbs"],
+                              "gpu_launches": orun["launches"], "clocks": orun["clocks"]}}
+        fp64_value = orun["value"] if prim == "mixed" else value
+        mixed_value = value if prim == "mixed" else orun["value"]
+        comparison["mixed_over_fp64"] = mixed_value / fp64_value
+        comparison["accuracy"] = precision_accuracy(d, cut, [x0, x_end], v0, args.drift_steps, restart)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        steps_per_rebuild = (M * args.steps / updates) if updates else None
-        cpu = cpu_reference_rate(d, os.cpu_count() or 1, rebuild_every=steps_per_rebuild)
+        steps_per_rebuild = (M * args.steps / run["updates"]) if run["updates"] else None
+        cpu = cpu_reference_rate(d, c, os.cpu_count() or 1, rebuild_every=steps_per_rebuild)
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "warmup": args.warmup, "ms_per_step": run["ms_total"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": PREC_DTYPE[prim],
             "data": "synthetic: seeded rings placed at phi 0.40, FIRE-compressed to 0.85, T=0.01 velocities",
             "config": {"workload": f"{npr} deformable rings nv 32/45 (1:1.4), {nv} vertices, smooth vertex-segment "
-                                   f"LJ rc 2.5, calA0 1.05, phi 0.85, NVE dt 0.002, FP64",
-                       "rings": npr, "vertices": nv, "md_steps_per_bench_step": M,
+                                   f"LJ rc 2.5, calA0 1.05, phi 0.85, ea {c['ea']:g} el {c['el']:g} "
+                                   f"eb {c['eb']:g}, NVE dt 0.002, precision {prim}",
+                       "precision": prim, "rings": npr, "vertices": nv, "md_steps_per_bench_step": M,
                        "l2": "flushed between bench steps (256 MB write)", "parallelism": f"replicas x{world}",
-                       "neighbour_rebuilds_in_timed_region": updates,
-                       "energy_drift_rel": abs(e1 - e0) / abs(e0) if e0 else None,
+                       "neighbour_rebuilds_in_timed_region": run["updates"],
+                       "energy_change_rel_timed_region": run["energy_change_rel"],
                        "prep_seconds": t_prep, "fire_iterations_prep": info["fire_iterations"],
                        "lanes_per_vertex": info["lanes"]},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks.summary(),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": run["launches"],
+            "clocks": run["clocks"], "precision_comparison": comparison,
         }
         print(json.dumps(line), flush=True)
     d.close()
@@ -374,6 +424,41 @@ def main():
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def precision_accuracy(d, cut, states, v0, drift_steps, restart) -> dict:
+    """Force / energy error of the mixed path against FP64 on thermal states,
+    and the NVE energy error of both precisions over ``drift_steps`` steps
+    from the same start state."""
+    errs, maxabs, eerr = [], [], []
+    for x in states:
+        d.setVertexPositions(x)
+        d.calcNeighborList(cut)
+        d.setPrecision("fp64")
+        d.calcForceEnergy()
+        f64, e64 = d.getVertexForces(), d.getPotentialEnergy()
+        d.setPrecision("mixed")
+        d.calcForceEnergy()
+        fmx, emx = d.getVertexForces(), d.getPotentialEnergy()
+        errs.append(float(np.linalg.norm(fmx - f64) / np.linalg.norm(f64)))
+        maxabs.append(float(np.abs(fmx - f64).max()))
+        eerr.append(abs(emx - e64) / abs(e64))
+    drift = {"steps": drift_steps}
+    chunk = 1000
+    for prec in ("fp64", "mixed"):
+        restart(prec)
+        e0 = d.getEnergy()
+        es = []
+        for _ in range(max(1, drift_steps // chunk)):
+            d.NVELoop(chunk)
+            es.append(d.getEnergy())
+        es = np.array(es)
+        t = np.arange(1, len(es) + 1) * chunk
+        slope = float(np.polyfit(t, (es - e0) / abs(e0), 1)[0]) if len(es) > 1 else None
+        drift[prec] = {"max_rel": float(np.abs(es - e0).max() / abs(e0)), "slope_rel_per_step": slope}
+    drift["mixed_over_fp64_max_rel"] = drift["mixed"]["max_rel"] / drift["fp64"]["max_rel"]
+    return {"force_err_l2_rel": errs, "force_err_max_abs": maxabs, "potential_energy_rel_err": eerr,
+            "states": "thermal start state and the end of the timed run", "energy_drift": drift}
 
 
 def run_reference_arm(args, world, rank):
@@ -402,8 +487,8 @@ def run_reference_arm(args, world, rank):
     R.ref_create(len(nvl), nvl)
     R.ref_set_box(float(box[0]), float(box[1]))
     R.ref_set_types(1, 1, 0, 0)
-    R.ref_set_energy_costs(1.0, 1.0, 0.01, 1.0)
-    R.ref_set_lj_cutoff(2.5)
+    R.ref_set_energy_costs(c["ea"], c["el"], c["eb"], c["ec"])
+    R.ref_set_lj_cutoff(c["LJcutoff"])
     R.ref_set_time_step(c["dt"])
     R.ref_set_state(pos.ctypes.data, vel.ctypes.data, rad.ctypes.data, l0.ctypes.data, th0.ctypes.data, a0.ctypes.data)
     cut = R.ref_set_displacement_cutoff(0.5, 2 * rad.mean())

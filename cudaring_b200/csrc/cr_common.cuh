@@ -5,8 +5,12 @@
 //   rad, l0, theta0 : double[Nv];  a0 : double[Np]
 //   ring_of         : int32[Nv];   ring_first, ring_nv : int32[Np]
 //   pp_of           : int2[Nv]     (previous, second-previous vertex of the ring)
+//   vtopo           : int2[Nv]     (ring, k | nv << 16)
 //   nbr             : int32[cap][Nv] column-major (slot-major) neighbour list,
 //                     nbr_cnt int32[Nv]; vertex ids in internal order
+//   nbr_pq          : int32[cap][Nv] packed ring-predecessor offsets of each
+//                     listed neighbour (lets a gather issue the neighbour's
+//                     own and its predecessors' loads together)
 //   tiles           : int4[T]      (first ring, end ring, first vertex, end vertex)
 // All arithmetic on the plain path is FP64, as in the reference.
 #pragma once
@@ -33,7 +37,20 @@ struct SysParams {
   double stiff, ext_sq;
   int monomer;   // 0 harmonic, 1 FENE
   int potential; // Pot
+  // FP32 copies of the pair constants for the mixed-precision pair terms,
+  // filled from the FP64 values when a mixed-precision kernel is launched
+  float f_ec, f_l1, f_l2, f_lj_cutoff, f_lj_ecut, f_lj_fshift;
 };
+
+inline SysParams with_f32_constants(SysParams p) {
+  p.f_ec = (float)p.ec;
+  p.f_l1 = (float)p.l1;
+  p.f_l2 = (float)p.l2;
+  p.f_lj_cutoff = (float)p.lj_cutoff;
+  p.f_lj_ecut = (float)p.lj_ecut;
+  p.f_lj_fshift = (float)p.lj_fshift;
+  return p;
+}
 
 // Device pointers of one system (internal order).
 struct SysArrays {
@@ -50,7 +67,17 @@ struct SysArrays {
   const int* nbr_cnt;
   const int4* tiles;
   int nbr_cap;
+  // per vertex: {ring, k | nv << 16}, k the vertex's index inside its ring
+  const int2* vtopo;
+  // per list entry (same [cap][nv] layout as nbr): the neighbour j's ring
+  // predecessors as offsets from j, (prev(j) - j) in the low 16 bits and
+  // (prev(prev(j)) - j) in the high 16 bits, both signed
+  const int* nbr_pq;
 };
+
+__host__ __device__ inline int pq_pack_of(int dq, int dqq) { return (dq & 0xffff) | (int)((unsigned)dqq << 16); }
+__device__ __forceinline__ int pq_first(int pk) { return (int)(short)(pk & 0xffff); }
+__device__ __forceinline__ int pq_second(int pk) { return pk >> 16; }
 
 // Minimum-image difference, reference pbcDistance (include/cudaKernel.cuh:70-74)
 // with delta/size replaced by delta*(1/size); the two agree except when

@@ -57,6 +57,7 @@ struct cr_ctx {
   std::vector<int> ring_first_h, ring_nv_h, ring_of_h;
   std::vector<int4> tiles_h;
   int lanes = 2;
+  int precision = CR_PRECISION_FP64;
 
   SysParams p{};
   int potential = 0, interaction = 0, monomer = 0, particle = 0, noise_type = 0, shape = 0, geometry = 0;
@@ -76,8 +77,11 @@ struct cr_ctx {
          *perimeter = nullptr, *p_angle = nullptr, *vertex_area = nullptr;
   int *ring_of = nullptr, *ring_first = nullptr, *ring_nv = nullptr, *zero_cnt = nullptr;
   int2* pp_of = nullptr;
+  int2* vtopo = nullptr;   // {ring, k | nv << 16}
+  int* pq_pack = nullptr;  // packed (prev - v, prev(prev) - v)
   int4* tiles = nullptr;
   int* nbr = nullptr;
+  int* nbr_pq = nullptr;   // companion of nbr: pq_pack of each listed neighbour
   int* nbr_cnt = nullptr;
   int cap = 0;
   bool nbr_built = false;
@@ -85,7 +89,7 @@ struct cr_ctx {
   CellGrid grid{0, 0, 0.0, 0.0};
   int ncells_alloc = 0;
   int *cell_of = nullptr, *slot = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_vid = nullptr,
-      *cell_ring = nullptr;
+      *cell_ring = nullptr, *cell_pq = nullptr;
   double2* cell_pos = nullptr;
   double* cell_rad = nullptr;
   double* partials = nullptr;
@@ -161,6 +165,8 @@ SysArrays arrays(cr_ctx* ctx, int buf, bool zero_list = false) {
   a.nbr_cnt = (zero_list || !ctx->nbr_built) ? ctx->zero_cnt : ctx->nbr_cnt;
   a.tiles = ctx->tiles;
   a.nbr_cap = ctx->cap;
+  a.vtopo = ctx->vtopo;
+  a.nbr_pq = ctx->nbr_pq;
   return a;
 }
 
@@ -213,7 +219,9 @@ int inter_kind(cr_ctx* ctx) {
                                                                                                       : INT_SMOOTH;
 }
 
-LaunchCfg tile_cfg(cr_ctx* ctx) { return LaunchCfg{ctx->stream, (int)ctx->tiles_h.size(), ctx->lanes}; }
+LaunchCfg tile_cfg(cr_ctx* ctx) {
+  return LaunchCfg{ctx->stream, (int)ctx->tiles_h.size(), ctx->lanes, ctx->precision};
+}
 
 int ensure_partials(cr_ctx* ctx) {
   int need = std::max<int>((int)ctx->tiles_h.size(), 2048) * NSUM;
@@ -263,6 +271,9 @@ NbrArgs nbr_args(cr_ctx* ctx, int buf, double cut) {
   n.cell_pos = ctx->cell_pos;
   n.cell_rad = ctx->cell_rad;
   n.cell_ring = ctx->cell_ring;
+  n.pq_pack = ctx->pq_pack;
+  n.nbr_pq = ctx->nbr_pq;
+  n.cell_pq = ctx->cell_pq;
   n.status = ctx->status;
   n.count_op = 0;
   n.count_update = 0;
@@ -292,6 +303,15 @@ int clear_flags(cr_ctx* ctx) {
   return CR_OK;
 }
 
+// Neighbour list and its companion at capacity `cap`.
+int alloc_lists(cr_ctx* ctx, int cap) {
+  int rc;
+  if ((rc = dalloc(ctx, &ctx->nbr, (size_t)cap * ctx->nv))) return rc;
+  if ((rc = dalloc(ctx, &ctx->nbr_pq, (size_t)cap * ctx->nv))) return rc;
+  ctx->cap = cap;
+  return CR_OK;
+}
+
 // Build the list from positions buffer `buf`; grows capacity like the
 // reference (two passes when the first overflowed).
 int build_list(cr_ctx* ctx, int buf, double cut) {
@@ -309,8 +329,7 @@ int build_list(cr_ctx* ctx, int buf, double cut) {
       if (mc * 2 > ctx->cap) {
         // keep headroom for rebuilds inside step sequences
         int newcap = (int)std::max<long long>(16, pow2ceil(2LL * mc));
-        if ((rc = dalloc(ctx, &ctx->nbr, (size_t)newcap * ctx->nv))) return rc;
-        ctx->cap = newcap;
+        if ((rc = alloc_lists(ctx, newcap))) return rc;
         drop_graphs(ctx);
         if ((rc = clear_flags(ctx))) return rc;
         continue;  // rebuild into the larger list
@@ -318,8 +337,7 @@ int build_list(cr_ctx* ctx, int buf, double cut) {
       return CR_OK;
     }
     int newcap = (int)std::max<long long>(16, pow2ceil(2LL * mc));
-    if ((rc = dalloc(ctx, &ctx->nbr, (size_t)newcap * ctx->nv))) return rc;
-    ctx->cap = newcap;
+    if ((rc = alloc_lists(ctx, newcap))) return rc;
     drop_graphs(ctx);
     if ((rc = clear_flags(ctx))) return rc;
   }
@@ -402,7 +420,9 @@ void enqueue_op(cr_ctx* ctx, cudaStream_t st, const Op& op, int kind, bool use_c
   s.cond = h;
   s.pos_out = ctx->pos[op.out_buf];
   s.advance = op.advance;
-  s.accumulate = 1;
+  // per-CTA sums feed FIRE's next iteration and the rigid tail; energies
+  // read by the caller are reduced afresh from the written arrays
+  s.accumulate = (kind == KIND_FIRE || ctx->shape == CR_SHAPE_RIGID) ? 1 : 0;
   s.write_out = (kind == KIND_FIRE || !op.advance) ? 1 : 0;
   s.fire_tol = ctx->fp.tol;
   const SysArrays a = arrays(ctx, op.in_buf);
@@ -678,7 +698,8 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
     return CR_ENOTSUP;
   }
   ctx->ring_of_h.resize(total);
-  std::vector<int2> pp(total);
+  std::vector<int2> pp(total), vtopo(total);
+  std::vector<int> pqp(total);
   for (int q = 0; q < ctx->np; q++) {
     const int f = ctx->ring_first_h[q], n = ctx->ring_nv_h[q];
     for (int k = 0; k < n; k++) {
@@ -686,6 +707,8 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
       const int prev = f + (k == 0 ? n - 1 : k - 1);
       const int k2 = (k - 2 + 2 * n) % n;
       pp[f + k] = make_int2(prev, f + k2);
+      vtopo[f + k] = make_int2(q, k | (n << 16));
+      pqp[f + k] = pq_pack_of(prev - (f + k), (f + k2) - (f + k));
     }
   }
   make_tiles(ctx);
@@ -709,6 +732,8 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
       (rc = dalloc(ctx, &ctx->tiles, ctx->tiles_h.size())) || (rc = dalloc(ctx, &ctx->nbr_cnt, nv)) ||
       (rc = dalloc(ctx, &ctx->cell_of, nv)) || (rc = dalloc(ctx, &ctx->slot, nv)) ||
       (rc = dalloc(ctx, &ctx->cell_vid, nv)) || (rc = dalloc(ctx, &ctx->cell_ring, nv)) ||
+      (rc = dalloc(ctx, &ctx->cell_pq, nv)) || (rc = dalloc(ctx, &ctx->vtopo, nv)) ||
+      (rc = dalloc(ctx, &ctx->pq_pack, nv)) ||
       (rc = dalloc(ctx, &ctx->cell_pos, nv)) || (rc = dalloc(ctx, &ctx->cell_rad, nv)) ||
       (rc = dalloc(ctx, &ctx->status, 1)) || (rc = dalloc(ctx, &ctx->fire_state, 8)) ||
       (rc = dalloc(ctx, &ctx->p_vel, np)) || (rc = dalloc(ctx, &ctx->p_force, np)) ||
@@ -718,8 +743,7 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
     cr_destroy(ctx);
     return rc;
   }
-  ctx->cap = 16;
-  if ((rc = dalloc(ctx, &ctx->nbr, (size_t)ctx->cap * nv))) {
+  if ((rc = alloc_lists(ctx, 16))) {
     cr_destroy(ctx);
     return rc;
   }
@@ -732,6 +756,8 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
       upload(ctx, ctx->ring_first, ctx->ring_first_h.data(), np * sizeof(int)) ||
       upload(ctx, ctx->ring_nv, ctx->ring_nv_h.data(), np * sizeof(int)) ||
       upload(ctx, ctx->pp_of, pp.data(), nv * sizeof(int2)) ||
+      upload(ctx, ctx->vtopo, vtopo.data(), nv * sizeof(int2)) ||
+      upload(ctx, ctx->pq_pack, pqp.data(), nv * sizeof(int)) ||
       upload(ctx, ctx->tiles, ctx->tiles_h.data(), ctx->tiles_h.size() * sizeof(int4))) {
     cr_destroy(ctx);
     return CR_ECUDA;
@@ -760,7 +786,8 @@ int cr_destroy(cr_ctx* ctx) {
   void* ptrs[] = {ctx->pos[0], ctx->pos[1], ctx->vel, ctx->force, ctx->last_pos, ctx->ppos, ctx->rad, ctx->l0,
                   ctx->theta0, ctx->a0, ctx->energy, ctx->p_energy, ctx->theta, ctx->length, ctx->area,
                   ctx->perimeter, ctx->p_angle, ctx->vertex_area, ctx->ring_of, ctx->ring_first, ctx->ring_nv,
-                  ctx->zero_cnt, ctx->pp_of, ctx->tiles, ctx->nbr, ctx->nbr_cnt, ctx->cell_of, ctx->slot,
+                  ctx->zero_cnt, ctx->pp_of, ctx->vtopo, ctx->pq_pack, ctx->nbr_pq, ctx->cell_pq,
+                  ctx->tiles, ctx->nbr, ctx->nbr_cnt, ctx->cell_of, ctx->slot,
                   ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
                   ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
                   ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle};
@@ -1510,7 +1537,7 @@ int cr_profile_step_kernel(cr_ctx* ctx, long reps, double* ms_per_launch) {
   StepArgs s = base_args(ctx);
   s.kind = ctx->sim_kind >= 0 && ctx->sim_kind != KIND_FIRE ? ctx->sim_kind : KIND_NVE;
   s.advance = 1;
-  s.accumulate = 1;
+  s.accumulate = 0;  // as in an NVE / Langevin step op
   s.active = 0;  // ring angles are state; the self-propulsion term is not timed here
   s.pos_out = pos_s;
   s.vel = vel_s;
@@ -1582,6 +1609,21 @@ int cr_autotune(cr_ctx* ctx, long reps, int* lanes_out) {
   int rc = cr_set_lanes(ctx, best);
   if (rc) return rc;
   if (lanes_out) *lanes_out = best;
+  return CR_OK;
+}
+
+int cr_set_precision(cr_ctx* ctx, int precision) {
+  if (!ctx) return CR_EINVAL;
+  if (precision != CR_PRECISION_FP64 && precision != CR_PRECISION_MIXED)
+    return ctx->fail(CR_EINVAL, "precision must be CR_PRECISION_FP64 or CR_PRECISION_MIXED");
+  ctx->precision = precision;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_get_precision(const cr_ctx* ctx, int* precision) {
+  if (!ctx || !precision) return CR_EINVAL;
+  *precision = ctx->precision;
   return CR_OK;
 }
 

@@ -11,13 +11,17 @@ struct StepArgs;
 struct LaunchCfg {
   cudaStream_t stream;
   int grid;    // number of tiles / CTAs
-  int lanes;   // lanes per vertex in the pair phase (1, 2, 4)
+  int lanes;   // lanes per vertex in the pair phase (1, 2, 4, 8)
+  int precision = CR_PRECISION_FP64;  // CR_PRECISION_* (deformable tile kernel)
 };
 
 // cr_tile.cu
 void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
                  const StepArgs& s);
 int tile_vertices(int lanes);
+// cr_tile_mixed.cu (expects p with its FP32 constants filled)
+void launch_tile_mixed(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
+                       const StepArgs& s);
 
 // cr_misc.cu
 struct FireParams {
@@ -80,6 +84,11 @@ struct NbrArgs {
   double2* cell_pos;  // [nv]
   double* cell_rad;   // [nv]
   int* cell_ring;     // [nv]
+  // optional companion list: per entry the packed ring-predecessor offsets
+  // of the neighbour (see SysArrays::nbr_pq); written when nbr_pq is set
+  const int* pq_pack = nullptr;  // [nv] per-vertex packed offsets
+  int* nbr_pq = nullptr;         // [cap][nv]
+  int* cell_pq = nullptr;        // [nv] cell-sorted copy of pq_pack
   DevStatus* status;
   int count_op;       // 1: the build is one op of a step sequence (ops_done += 1)
   int count_update;   // 1: a displacement-triggered rebuild (DPM2D::updateCount += 1)

@@ -14,7 +14,8 @@
 //   k_cell_scan    exclusive scan of the cell counts (one CTA), zeroes counts
 //   k_cell_fill    scatter vertex ids by cell
 //   k_cell_sort    sort each cell's ids ascending and copy pos/rad/ring (SoA)
-//   k_nbr_cells    stencil search -> slot-major list, counts, overflow flag,
+//   k_nbr_cells    stencil search -> slot-major list (and its companion of
+//                  packed ring-predecessor offsets), counts, overflow flag,
 //                  lastPos = pos; the last CTA publishes the build to status
 #include "cr_launch.h"
 #include "cr_tile.cuh"
@@ -72,7 +73,8 @@ __global__ void k_cell_fill(int nv, const int* cell_of, const int* slot, const i
 }
 
 __global__ void k_cell_sort(int ncells, const int* cell_start, int* cell_vid, const double2* pos, const double* rad,
-                            const int* ring_of, double2* cell_pos, double* cell_rad, int* cell_ring) {
+                            const int* ring_of, const int* pq_pack, double2* cell_pos, double* cell_rad,
+                            int* cell_ring, int* cell_pq) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c < ncells) {
     const int b = cell_start[c], e = cell_start[c + 1];
@@ -90,6 +92,7 @@ __global__ void k_cell_sort(int ncells, const int* cell_start, int* cell_vid, co
       cell_pos[i] = pos[v];
       cell_rad[i] = rad[v];
       cell_ring[i] = ring_of[v];
+      if (cell_pq) cell_pq[i] = pq_pack[v];
     }
   }
 }
@@ -145,7 +148,10 @@ __global__ void __launch_bounds__(256) k_nbr_cells(const __grid_constant__ SysPa
         for (int k = b; k < e; k++) {
           if (n.cell_ring[k] == ring) continue;
           if (is_neighbor(p, xi, n.cell_pos[k], ri + n.cell_rad[k], n.cut_distance)) {
-            if (cnt < n.cap) n.nbr[(size_t)cnt * p.nv + i] = n.cell_vid[k];
+            if (cnt < n.cap) {
+              n.nbr[(size_t)cnt * p.nv + i] = n.cell_vid[k];
+              if (n.nbr_pq) n.nbr_pq[(size_t)cnt * p.nv + i] = n.cell_pq[k];
+            }
             cnt++;
           }
         }
@@ -178,7 +184,10 @@ __global__ void __launch_bounds__(256) k_nbr_brute(const __grid_constant__ SysPa
     for (int j = 0; j < p.nv; j++) {
       if (n.ring_of[j] == ring) continue;
       if (is_neighbor(p, xi, n.pos[j], ri + n.rad[j], n.cut_distance)) {
-        if (cnt < n.cap) n.nbr[(size_t)cnt * p.nv + i] = j;
+        if (cnt < n.cap) {
+          n.nbr[(size_t)cnt * p.nv + i] = j;
+          if (n.nbr_pq) n.nbr_pq[(size_t)cnt * p.nv + i] = n.pq_pack[j];
+        }
         cnt++;
       }
     }
@@ -213,7 +222,8 @@ void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g
     k_cell_scan<<<1, 1024, 0, stream>>>(ncells, n.cell_cnt, n.cell_start);
     k_cell_fill<<<nb, 256, 0, stream>>>(p.nv, n.cell_of, n.slot, n.cell_start, n.cell_vid);
     k_cell_sort<<<(ncells + 255) / 256, 256, 0, stream>>>(ncells, n.cell_start, n.cell_vid, n.pos, n.rad, n.ring_of,
-                                                          n.cell_pos, n.cell_rad, n.cell_ring);
+                                                          n.nbr_pq ? n.pq_pack : nullptr, n.cell_pos, n.cell_rad,
+                                                          n.cell_ring, n.nbr_pq ? n.cell_pq : nullptr);
     k_nbr_cells<<<nb, 256, 0, stream>>>(p, g.ncx, g.ncy, n);
   } else {
     k_nbr_brute<<<nb, 256, 0, stream>>>(p, n);

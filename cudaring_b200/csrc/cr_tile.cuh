@@ -6,13 +6,15 @@
 //   2. shape force per vertex (area, segment length or FENE, bending);
 //   3. pair forces with L lanes per vertex striding over the slot-major
 //      neighbour list; the smooth vertex-segment interaction is evaluated in a
-//      gather form (smooth_unit, roles 1 and 2) so no global atomics are needed
+//      gather form (smooth_core, roles 1 and 2) so no global atomics are needed
 //      and the result does not depend on scheduling order;
 //   4. integrator tail: the second half kick of this step and, when the op
 //      advances, the first half kick + drift of the next step written to a
 //      second position buffer (ping-pong), plus the displacement check that
 //      arms a neighbour-list rebuild.
 #pragma once
+#include <type_traits>
+
 #include "cr_common.cuh"
 
 namespace cr {
@@ -170,45 +172,178 @@ __device__ __forceinline__ double sign_of(double c) {
   return c > 0.0 ? 1.0 : (c < 0.0 ? -1.0 : __longlong_as_double(0x7ff8000000000000LL));
 }
 
-// Smooth unit from precomputed geometry.  t: the vertex, o: segment end,
-// q = prev(o), qq = prev(q); seg = pbc(o - q), pseg = pbc(q - qq),
-// tq = pbc(t - q), w = pbc(t - o), tq2 = |tq|^2.  See smooth_unit.
-template <int POT, bool ROLE1>
-__device__ __forceinline__ void smooth_core(const SysParams& p, double2 t, double2 q, double2 qq, double2 seg,
-                                            double len2, double2 pseg, double2 tq, double tq2, double2 w,
-                                            double rsum, double inv_rsum, double2& ft, double2& fo, double2& fq,
+// ----------------------------------------------------------------------------
+// FP32 pair arithmetic of the mixed-precision path.  Offsets arrive as the
+// FP64 minimum-image differences rounded to float; every smooth unit is
+// written in coordinates relative to its vertex t (tq = t - q, tqq = t - qq,
+// w = t - o), so no absolute coordinate is ever held in float.
+// ----------------------------------------------------------------------------
+
+__device__ __forceinline__ float2 f2(double2 d) { return make_float2((float)d.x, (float)d.y); }
+
+template <int POT>
+__device__ __forceinline__ float pot_range_f(const SysParams& p) {
+  if constexpr (POT == POT_HARMONIC) return 1.0f;
+  else if constexpr (POT == POT_LJ) return p.f_lj_cutoff;
+  else if constexpr (POT == POT_ADHESIVE) return 1.0f + p.f_l2;
+  else return (float)kWCAcut;
+}
+
+template <int POT>
+__device__ __forceinline__ bool pair_eval_f(const SysParams& p, float d2, float rsum, float inv_rsum, float& gm,
+                                            float& inv_d, float& ep) {
+  inv_d = rsqrtf(d2);
+  const float d = d2 * inv_d;
+  const float ec = p.f_ec;
+  if constexpr (POT == POT_HARMONIC) {
+    const float ov = 1.0f - d * inv_rsum;
+    if (!(ov > 0.0f)) return false;
+    gm = ec * ov * inv_rsum;
+    ep = 0.25f * ec * ov * ov;
+    return true;
+  } else if constexpr (POT == POT_LJ) {
+    const float rc = p.f_lj_cutoff;
+    if (!(d <= rc * rsum)) return false;
+    const float ratio = rsum * inv_d;
+    const float r2 = ratio * ratio;
+    const float r6 = r2 * r2 * r2;
+    const float r12 = r6 * r6;
+    const float fshift = p.f_lj_fshift * inv_rsum;
+    gm = 24.0f * ec * (2.0f * r12 - r6) * inv_d - fshift;
+    ep = 0.5f * (4.0f * ec * (r12 - r6) - p.f_lj_ecut - fabsf(fshift) * (d - rc * rsum));
+    return true;
+  } else if constexpr (POT == POT_ADHESIVE) {
+    const float l1 = p.f_l1, l2 = p.f_l2;
+    if (!(d < (1.0f + l2) * rsum)) return false;
+    const float ov = 1.0f - d * inv_rsum;
+    if (d < (1.0f + l1) * rsum) {
+      gm = ec * ov * inv_rsum;
+      ep = 0.25f * ec * (ov * ov - l1 * l2);
+    } else {
+      const float k = ec * l1 / (l2 - l1);
+      gm = -k * (ov + l2) * inv_rsum;
+      ep = -0.25f * k * (ov + l2) * (ov + l2);
+    }
+    return true;
+  } else {
+    if (!(d <= (float)kWCAcut * rsum)) return false;
+    const float ratio = rsum * inv_d;
+    const float r2 = ratio * ratio;
+    const float r6 = r2 * r2 * r2;
+    const float r12 = r6 * r6;
+    gm = 24.0f * ec * (2.0f * r12 - r6) * inv_d;
+    ep = 0.5f * ec * (4.0f * (r12 - r6) + 1.0f);
+    return true;
+  }
+}
+
+template <int POT>
+__device__ __forceinline__ void pair_own_f(const SysParams& p, float2 dl, float rsum, float2& f, double& e) {
+  const float d2 = fmaf(dl.y, dl.y, dl.x * dl.x);
+  const float R = pot_range_f<POT>(p) * rsum * 1.00001f;
+  if (d2 > R * R) return;
+  float gm, inv_d, ep = 0.0f;
+  if (pair_eval_f<POT>(p, d2, rsum, 1.0f / rsum, gm, inv_d, ep)) {
+    const float s = gm * inv_d;
+    f.x = fmaf(s, dl.x, f.x);
+    f.y = fmaf(s, dl.y, f.y);
+    e += (double)ep;
+  }
+}
+
+__device__ __forceinline__ float sign_of_f(float c) {
+  return c > 0.0f ? 1.0f : (c < 0.0f ? -1.0f : __int_as_float(0x7fc00000));
+}
+
+// ----------------------------------------------------------------------------
+// Smooth vertex-segment unit, one form for FP64 (the plain path) and FP32
+// (the mixed path's pair terms).
+//
+// One unit U(t; o) of kernelCalcSmoothInteraction (include/cudaKernel.cuh:922-975):
+// vertex t against the segment q -> o (q = prev(o), qq = prev(q)) of another
+// ring, with the concave correction (t also projects onto qq -> q: subtract
+// the t-q vertex-vertex term) and the convex one (t before q on both
+// segments: add it).  ROLE1 (t is this vertex) returns the force on t; ROLE2
+// (o is this vertex, t a neighbour) returns the forces on o and on q.  Both
+// add the unit energy, which the reference books on the rings of t and of o.
+//
+// Inputs are offsets from t: tq = t - q (minimum image), w = t - o, and the
+// segment vectors seg = o - q, pseg = q - qq; tabs, qabs are t and q in box
+// coordinates.  The reference forms t - qq and the projection point
+// q + proj * seg explicitly.  Here
+//   * FP64 forms the projection point as the reference does, in box
+//     coordinates; FP32 takes the projection distance as |tq - proj * seg|
+//     (the same point, relative to t, with no box-sized coordinate in FP32),
+//   * pproj = (t - qq).pseg / |pseg|^2 = 1 + tq.pseg / |pseg|^2, so its tests
+//     pproj in [0, 1) and pproj >= 1 read -|pseg|^2 <= tq.pseg < 0 and
+//     tq.pseg >= 0, with neither t - qq nor a division (this moves the
+//     decision only for pproj within rounding of 0 or 1).
+// ----------------------------------------------------------------------------
+
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+__device__ __forceinline__ double rsq(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsq(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double sgn_nan0(double c) { return sign_of(c); }
+__device__ __forceinline__ float sgn_nan0(float c) { return sign_of_f(c); }
+template <int POT>
+__device__ __forceinline__ bool pair_eval_t(const SysParams& p, double d2, double rsum, double inv_rsum, double& gm,
+                                            double& inv_d, double& ep) {
+  return pair_eval<POT>(p, d2, rsum, inv_rsum, gm, inv_d, ep);
+}
+template <int POT>
+__device__ __forceinline__ bool pair_eval_t(const SysParams& p, float d2, float rsum, float inv_rsum, float& gm,
+                                            float& inv_d, float& ep) {
+  return pair_eval_f<POT>(p, d2, rsum, inv_rsum, gm, inv_d, ep);
+}
+
+template <int POT, bool ROLE1, typename T, typename T2 = typename Vec2<T>::type>
+__device__ __forceinline__ void smooth_core(const SysParams& p, T2 tq, T tq2, T2 w, T2 seg, T len2, T2 pseg, T rsum,
+                                            T inv_rsum, double2 tabs, double2 qabs, T2& ft, T2& fo, T2& fq,
                                             double& e) {
-  const double inv_len = rsqrt(len2);
-  const double inv_lsq = inv_len * inv_len;
-  const double proj = (tq.x * seg.x + tq.y * seg.y) * inv_lsq;
-  const double2 tqq = pbc2(p, t, qq);
-  const double pinv = rsqrt(fma(pseg.y, pseg.y, pseg.x * pseg.x));
-  const double pproj = (tqq.x * pseg.x + tqq.y * pseg.y) * (pinv * pinv);
-  if (proj >= 0.0 && proj < 1.0) {
-    const double2 pj = make_double2(q.x + proj * seg.x, q.y + proj * seg.y);
-    const double2 dp = pbc2(p, t, pj);
-    double gm, inv_d, ep = 0.0;
-    if (pair_eval<POT>(p, fma(dp.y, dp.y, dp.x * dp.x), rsum, inv_rsum, gm, inv_d, ep) && gm != 0.0) {
-      const double cross = seg.x * w.y - w.x * seg.y;
-      const double sign = sign_of(cross);
-      const double g = gm * inv_len;
+  const T inv_len = rsq(len2);
+  const T inv_lsq = inv_len * inv_len;
+  const T proj = (tq.x * seg.x + tq.y * seg.y) * inv_lsq;
+  const T pc = tq.x * pseg.x + tq.y * pseg.y;
+  const T pl2 = fma(pseg.y, pseg.y, pseg.x * pseg.x);
+  if (proj >= T(0) && proj < T(1)) {
+    T dpx, dpy;
+    if constexpr (std::is_same<T, double>::value) {
+      // FP64: the projection point in box coordinates, as the reference forms
+      // it (pbcDistance(thisPos, previousPos + proj * segment)), so that
+      // near-contact distances carry the same rounding as there
+      const double2 pj = make_double2(qabs.x + proj * seg.x, qabs.y + proj * seg.y);
+      const double2 dpv = pbc2(p, tabs, pj);
+      dpx = dpv.x;
+      dpy = dpv.y;
+    } else {
+      dpx = fma(-proj, seg.x, tq.x);
+      dpy = fma(-proj, seg.y, tq.y);
+    }
+    T gm, inv_d, ep = T(0);
+    if (pair_eval_t<POT>(p, fma(dpy, dpy, dpx * dpx), rsum, inv_rsum, gm, inv_d, ep) && gm != T(0)) {
+      const T cross = seg.x * w.y - w.x * seg.y;
+      const T sign = sgn_nan0(cross);
+      const T g = gm * inv_len;
       if constexpr (ROLE1) {
         ft.x += g * sign * (-seg.y);
         ft.y += g * sign * seg.x;
       } else {
-        const double a = fabs(cross) * inv_lsq;
+        const T a = fabs(cross) * inv_lsq;
         fo.x += g * (sign * tq.y - a * seg.x);
         fo.y += g * (-sign * tq.x - a * seg.y);
         fq.x += g * (-sign * w.y + a * seg.x);
         fq.y += g * (sign * w.x + a * seg.y);
       }
-      e += ep;
+      e += (double)ep;
     }
-    if (pproj >= 0.0 && pproj < 1.0) {
-      // calcVertexVertexInteraction(previousPos, thisPos, ...): delta = pbc(q - t)
-      double g2, id2, ep2 = 0.0;
-      if (pair_eval<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != 0.0) {
-        const double s2 = g2 * id2;
+    if (pc >= -pl2 && pc < T(0)) {
+      // calcVertexVertexInteraction(previousPos, thisPos, ...): delta = q - t
+      T g2, id2, ep2 = T(0);
+      if (pair_eval_t<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != T(0)) {
+        const T s2 = g2 * id2;
         if constexpr (ROLE1) {
           ft.x -= s2 * tq.x;
           ft.y -= s2 * tq.y;
@@ -216,14 +351,14 @@ __device__ __forceinline__ void smooth_core(const SysParams& p, double2 t, doubl
           fq.x += s2 * tq.x;
           fq.y += s2 * tq.y;
         }
-        e -= ep2;
+        e -= (double)ep2;
       }
     }
-  } else if (proj < 0.0 && pproj >= 1.0) {
-    // calcVertexVertexInteraction(thisPos, previousPos, ...): delta = pbc(t - q)
-    double g2, id2, ep2 = 0.0;
-    if (pair_eval<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != 0.0) {
-      const double s2 = g2 * id2;
+  } else if (proj < T(0) && pc >= T(0)) {
+    // calcVertexVertexInteraction(thisPos, previousPos, ...): delta = t - q
+    T g2, id2, ep2 = T(0);
+    if (pair_eval_t<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != T(0)) {
+      const T s2 = g2 * id2;
       if constexpr (ROLE1) {
         ft.x += s2 * tq.x;
         ft.y += s2 * tq.y;
@@ -231,96 +366,20 @@ __device__ __forceinline__ void smooth_core(const SysParams& p, double2 t, doubl
         fq.x -= s2 * tq.x;
         fq.y -= s2 * tq.y;
       }
-      e += ep2;
+      e += (double)ep2;
     }
   }
 }
 
-// True when no term of a smooth unit can be in range: every point of the
-// segment is at least max(|t-o|, |t-q|) - |o-q| from t, and both corrections
-// use |t-q|.  The relative margin covers rounding, so a skipped unit is one
-// that would have contributed exactly zero.
-__device__ __forceinline__ bool smooth_out_of_range(double R, double tq2, double w2, double len2) {
-  const double Rm = R * (1.0 + 1e-12);
+// Exact skip test for a smooth unit: every term vanishes beyond R = range *
+// radSum, the projection distance is at least max(|tq|, |w|) - |seg| and the
+// corner terms use |tq|.  Evaluated in FP32 with a relative margin far above
+// FP32 rounding, so a skipped unit is one that contributes exactly zero.
+__device__ __forceinline__ bool smooth_out_of_range(float R, float tq2, float w2, float len) {
+  const float Rm = R * 1.00001f;
   if (!(tq2 > Rm * Rm)) return false;
-  const double lim = Rm + sqrt(len2);
-  return fmax(tq2, w2) > lim * lim;
-}
-
-// One unit U(t; o) of kernelCalcSmoothInteraction (include/cudaKernel.cuh:922-975):
-// vertex t against the segment q -> o (q = prev(o)) of another ring, with the
-// concave correction (t also projects onto qq -> q: subtract the t-q
-// vertex-vertex term) and the convex one (t before q on both segments: add
-// it).  ROLE1 (t is this vertex) returns the force on t; ROLE2 (o is this
-// vertex, t a neighbour) returns the forces on o and on q.  Both add the unit
-// energy, which the reference books on the rings of t and of o.
-//   seg = pbc(o - q), pseg = pbc(q - qq).
-template <int POT, bool ROLE1>
-__device__ __forceinline__ void smooth_unit(const SysParams& p, double2 t, double2 o, double2 q, double2 qq,
-                                            double2 seg, double2 pseg, double rsum, double2& ft, double2& fo,
-                                            double2& fq, double& e) {
-  double len = dist_of(seg);
-  double lsq = len * len;
-  double2 tq = pbc2(p, t, q);
-  double proj = (tq.x * seg.x + tq.y * seg.y) / lsq;
-  double plen = dist_of(pseg);
-  double2 tqq = pbc2(p, t, qq);
-  double pproj = (tqq.x * pseg.x + tqq.y * pseg.y) / (plen * plen);
-  if (proj >= 0.0 && proj < 1.0) {
-    double2 pj = make_double2(q.x + proj * seg.x, q.y + proj * seg.y);
-    double dp = dist_of(pbc2(p, t, pj));
-    double ep = 0.0;
-    double gm = pair_gm<POT>(p, dp, rsum, ep);
-    if (gm != 0.0) {
-      double2 w = pbc2(p, t, o);
-      double cross = seg.x * w.y - w.x * seg.y;
-      double ac = fabs(cross);
-      double sign = cross / ac;
-      if constexpr (ROLE1) {
-        ft.x += gm * sign * (-seg.y) / len;
-        ft.y += gm * sign * seg.x / len;
-      } else {
-        fo.x += gm * (sign * tq.y - ac * seg.x / lsq) / len;
-        fo.y += gm * (-sign * tq.x - ac * seg.y / lsq) / len;
-        fq.x += gm * (-sign * w.y + ac * seg.x / lsq) / len;
-        fq.y += gm * (sign * w.x + ac * seg.y / lsq) / len;
-      }
-      e += ep;
-    }
-    if (pproj >= 0.0 && pproj < 1.0) {
-      // calcVertexVertexInteraction(previousPos, thisPos, ...): delta = pbc(q - t)
-      double d = dist_of(tq);
-      double ep2 = 0.0;
-      double g2 = pair_gm<POT>(p, d, rsum, ep2);
-      if (g2 != 0.0) {
-        if constexpr (ROLE1) {
-          ft.x += g2 * (-tq.x) / d;
-          ft.y += g2 * (-tq.y) / d;
-        } else {
-          fq.x += g2 * tq.x / d;
-          fq.y += g2 * tq.y / d;
-        }
-        e -= ep2;
-      }
-    }
-  } else if (proj < 0.0) {
-    if (pproj >= 1.0) {
-      // calcVertexVertexInteraction(thisPos, previousPos, ...): delta = pbc(t - q)
-      double d = dist_of(tq);
-      double ep2 = 0.0;
-      double g2 = pair_gm<POT>(p, d, rsum, ep2);
-      if (g2 != 0.0) {
-        if constexpr (ROLE1) {
-          ft.x += g2 * tq.x / d;
-          ft.y += g2 * tq.y / d;
-        } else {
-          fq.x -= g2 * tq.x / d;
-          fq.y -= g2 * tq.y / d;
-        }
-        e += ep2;
-      }
-    }
-  }
+  const float lim = Rm + len * 1.00001f;
+  return fmaxf(tq2, w2) > lim * lim;
 }
 
 // Last-CTA epilogue shared by all per-step kernels: sums the per-CTA partials

@@ -1,0 +1,492 @@
+// Tiled force + integrator kernel body (see cr_tile.cuh for the phase
+// structure), shared by the FP64 instantiations (cr_tile.cu) and the
+// mixed-precision ones (cr_tile_mixed.cu).
+//
+// Latency layout.  A step of this workload is one wave of CTAs with a few
+// warps per SM, so the time of a launch is the dependent-latency chain of one
+// thread, not a throughput limit.  The kernel therefore keeps that chain
+// short:
+//   * every per-vertex input is fetched in the prologue, in parallel: the ring
+//     topology from the packed vtopo word (no ring_of -> ring_first chain),
+//     rest lengths / angles into shared memory (neighbours read them there),
+//     and, for a step, velocity and last-build position by cp.async straight
+//     into shared memory (no registers held across the pair phase);
+//   * the neighbour gather reads each listed neighbour's ring predecessors
+//     from the companion list (nbr_pq), so the neighbour's position and both
+//     predecessor positions are loaded together, and the next slot's list
+//     entries are fetched before the current slot is evaluated;
+//   * per-CTA partial sums are formed only when an op needs them (FIRE); the
+//     non-finite check otherwise is one __syncthreads_or.
+#pragma once
+#include <type_traits>
+
+#include "cr_tile.cuh"
+
+namespace cr {
+
+// Occupancy target in threads per SM: 512 leaves 128 registers per thread,
+// where the smooth-interaction body compiles without spills.
+constexpr int kTileThreadsPerSM = 512;
+
+enum Prec : int { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+template <typename T2> __device__ __forceinline__ T2 cvt2(double2 d);
+template <> __device__ __forceinline__ double2 cvt2<double2>(double2 d) { return d; }
+template <> __device__ __forceinline__ float2 cvt2<float2>(double2 d) { return f2(d); }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC>
+__global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const __grid_constant__ SysParams p,
+                                                const __grid_constant__ SysArrays a,
+                                                const __grid_constant__ StepArgs s) {
+  constexpr int TV = BLOCK / L;
+  constexpr int TS = (MODE == MODE_STEP) ? TV : 1;
+  __shared__ double2 s_pos[TV];
+  __shared__ double2 s_seg[TV];     // pbc(pos[next] - pos[v])
+  __shared__ double s_theta[TV];
+  __shared__ double s_l0[TV];       // rest length of segment v -> next(v)
+  __shared__ double s_th0[TV];      // rest angle at v
+  __shared__ double s_r0[TV];       // shoelace terms -> ring area
+  __shared__ double s_r1[TV];       // segment lengths -> perimeter
+  __shared__ double2 s_r2[TV];      // offsets from the first vertex -> centroid
+  __shared__ double2 s_fpair[TV];   // pair force on v
+  __shared__ double2 s_fprev[TV];   // smooth: force on prev(v) gathered by v
+  __shared__ double s_epair[TV];
+  __shared__ int s_lp[TV];
+  __shared__ __align__(16) double2 s_vel[TS];
+  __shared__ __align__(16) double2 s_last[TS];
+  __shared__ double s_red[BLOCK / 32][NSUM];
+
+  DevStatus* st = s.status;
+  if (MODE == MODE_STEP && (st->abort | st->converged)) {
+    // keep the last-block protocol intact so later ops see a consistent counter
+    if (is_last_block(st)) {
+      if (threadIdx.x == 0) {
+        st->done_ctr = 0;
+        if (s.use_cond) cudaGraphSetConditional(s.cond, 0u);
+      }
+    }
+    return;
+  }
+
+  const int4 tile = a.tiles[blockIdx.x];
+  const int v0 = tile.z, nvt = tile.w - tile.z;
+  const int t = threadIdx.x;
+
+  // ---- prologue: every per-vertex input, in parallel ------------------------
+  int ring = -1, k = 0, lf = 0, lp = 0, ln = 0, nvr = 1;
+  double a0r = 1.0;
+  if (t < nvt) {
+    const int v = v0 + t;
+    if constexpr (MODE == MODE_STEP) {
+      cp_async16(&s_vel[t], s.vel + v);
+      cp_async16(&s_last[t], s.last_pos + v);
+      cp_async_commit();
+    }
+    const int2 tp = __ldg(a.vtopo + v);
+    s_pos[t] = __ldg(a.pos + v);
+    s_l0[t] = __ldg(a.l0 + v);
+    s_th0[t] = __ldg(a.theta0 + v);
+    ring = tp.x;
+    k = tp.y & 0xffff;
+    nvr = tp.y >> 16;
+    lf = t - k;
+    ln = lf + (k + 1 == nvr ? 0 : k + 1);
+    lp = lf + (k == 0 ? nvr - 1 : k - 1);
+    s_lp[t] = lp;
+    a0r = __ldg(a.a0 + ring);
+  }
+  __syncthreads();
+
+  // ---- phase 1: geometry --------------------------------------------------
+  if (t < nvt) {
+    const double2 x = s_pos[t];
+    const double2 xn = s_pos[ln];
+    const double2 seg = pbc2(p, xn, x);
+    s_seg[t] = seg;
+    const double2 x0 = s_pos[lf];
+    const double2 u = pbc2(p, x, x0);
+    const double2 un = pbc2(p, xn, x0);
+    s_r0[t] = u.x * un.y - un.x * u.y;
+    s_r1[t] = dist_of(seg);
+    s_r2[t] = u;
+  }
+  __syncthreads();
+  if (t < nvt) {
+    // calcAngle(nextSegment, previousSegment) (include/cudaKernel.cuh:423-427)
+    const double2 ns = s_seg[t];
+    const double2 ps = s_seg[lp];
+    s_theta[t] = atan2(ns.x * ps.y - ns.y * ps.x, ns.x * ps.x + ns.y * ps.y);
+  }
+  // deterministic per-ring tree over the ring's vertex range
+  for (int stride = 1; stride < TV; stride <<= 1) {
+    __syncthreads();
+    if (t < nvt && (k % (2 * stride)) == 0 && k + stride < nvr) {
+      s_r0[t] += s_r0[t + stride];
+      s_r1[t] += s_r1[t + stride];
+      s_r2[t].x += s_r2[t + stride].x;
+      s_r2[t].y += s_r2[t + stride].y;
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 2: shape force (kernelCalcShapeForceEnergy, include/cudaKernel.cuh:474-529)
+  double2 fsh = make_double2(0.0, 0.0);
+  double esh = 0.0;
+  if (t < nvt) {
+    const double area = fabs(s_r0[lf]) * 0.5;
+    const double dA = (area / a0r) - 1.0;
+    const double gmA = p.ea * dA / a0r;
+    const double2 ns = s_seg[t];
+    const double2 ps = s_seg[lp];
+    // nRel - pRel = pos[next] - pos[prev]
+    const double2 npd = make_double2(ns.x + ps.x, ns.y + ps.y);
+    fsh.x += 0.5 * gmA * (-npd.y);
+    fsh.y += 0.5 * gmA * (npd.x);
+    esh += (0.5 * p.ea * dA * dA) / nvr;
+    const double plen = dist_of(ps), nlen = dist_of(ns);
+    const double tl0 = s_l0[t], pl0 = s_l0[lp];
+    if (p.monomer == 0) {
+      const double pd = (plen / pl0) - 1.0;
+      const double nd = (nlen / tl0) - 1.0;
+      fsh.x += p.el * ((nd * ns.x / (tl0 * nlen)) - (pd * ps.x / (pl0 * plen)));
+      fsh.y += p.el * ((nd * ns.y / (tl0 * nlen)) - (pd * ps.y / (pl0 * plen)));
+      esh += 0.5 * p.el * pd * pd;
+    } else {
+      const double c = 2.0 * p.el * p.stiff * p.ext_sq;
+      const double an = nlen / (p.ext_sq * tl0 * tl0 - nlen * nlen);
+      const double ap = plen / (p.ext_sq * pl0 * pl0 - plen * plen);
+      fsh.x += c * (an * ns.x / nlen - ap * ps.x / plen);
+      fsh.y += c * (an * ns.y / nlen - ap * ps.y / plen);
+      esh += p.el * p.stiff * p.ext_sq * log(1.0 - plen * plen / (p.ext_sq * pl0 * pl0));
+    }
+    const double prevAD = s_theta[lp] - s_th0[lp];
+    const double thisAD = s_theta[t] - s_th0[t];
+    const double nextAD = s_theta[ln] - s_th0[ln];
+    const double pvar = (thisAD - prevAD) / (ps.x * ps.x + ps.y * ps.y);
+    const double nvar = (thisAD - nextAD) / (ns.x * ns.x + ns.y * ns.y);
+    fsh.x += p.eb * (pvar * ps.y + nvar * ns.y);
+    fsh.y += p.eb * (pvar * (-ps.x) + nvar * (-ns.x));
+    esh += 0.5 * p.eb * thisAD * thisAD;
+  }
+
+  // ---- phase 3: pair forces ------------------------------------------------
+  // L lanes per vertex stride over its list slots; each slot's list entries
+  // (neighbour id and packed predecessor offsets) are fetched one slot ahead,
+  // the neighbour's three positions together.
+  {
+    const int lv = t / L, lane = t % L;
+    using T = typename std::conditional<PREC == PREC_MIXED, float, double>::type;
+    typename Vec2<T>::type fi{0, 0}, fq{0, 0};
+    double ei = 0.0;
+    if (lv < nvt) {
+      const int i = v0 + lv;
+      const double2 xi = s_pos[lv];
+      const double ri = __ldg(a.rad + i);
+      const int cnt = min(__ldg(a.nbr_cnt + i), a.nbr_cap);  // an overflowed build stores counts above capacity
+      const size_t stride = (size_t)p.nv;
+      int sl = lane;
+      int jn = 0, pkn = 0;
+      if (sl < cnt) {
+        jn = __ldg(a.nbr + (size_t)sl * stride + i);
+        if constexpr (INTER == INT_SMOOTH) pkn = __ldg(a.nbr_pq + (size_t)sl * stride + i);
+      }
+      if constexpr (INTER == INT_VV) {
+        while (sl < cnt) {
+          const int j = jn;
+          const double2 xj = __ldg(a.pos + j);
+          const double rj = __ldg(a.rad + j);
+          sl += L;
+          if (sl < cnt) jn = __ldg(a.nbr + (size_t)sl * stride + i);
+          if constexpr (PREC == PREC_MIXED) pair_own_f<POT>(p, f2(pbc2(p, xi, xj)), (float)(ri + rj), fi, ei);
+          else pair_own<POT>(p, pbc2(p, xi, xj), ri + rj, fi, ei);
+        }
+      } else {
+        // Smooth units of vertex i: role 1 (i against the segment prev(j) -> j)
+        // and role 2 (j against i's own segment prev(i) -> i).  Offsets are
+        // formed in FP64 from the positions and, on the mixed path, rounded
+        // once to FP32 for the unit arithmetic.
+        using T2 = typename Vec2<T>::type;
+        const int lq = s_lp[lv];
+        const double2 xq = s_pos[lq];
+        const double2 seg_i64 = s_seg[lq];                // x_i - x_q
+        const T2 seg_i = cvt2<T2>(seg_i64);
+        const T2 pseg_i = cvt2<T2>(s_seg[s_lp[lq]]);      // x_q - x_qq
+        const T len2_i = fma(seg_i.y, seg_i.y, seg_i.x * seg_i.x);
+        const float len_i = sqrtf((float)len2_i);
+        const float range = pot_range_f<POT>(p);
+        T2 dummy{0, 0};
+        while (sl < cnt) {
+          const int j = jn, pk = pkn;
+          const double2 xj = __ldg(a.pos + j);
+          const double2 xjq = __ldg(a.pos + j + pq_first(pk));
+          const double2 xjqq = __ldg(a.pos + j + pq_second(pk));
+          const double rsum64 = ri + __ldg(a.rad + j);
+          sl += L;
+          if (sl < cnt) {
+            jn = __ldg(a.nbr + (size_t)sl * stride + i);
+            pkn = __ldg(a.nbr_pq + (size_t)sl * stride + i);
+          }
+          const T rsum = (T)rsum64;
+          const T inv_rsum = T(1) / rsum;
+          const float R = range * (float)rsum64;
+          const double2 w64 = pbc2(p, xi, xj);    // x_i - x_j
+          const double2 tq64 = pbc2(p, xi, xjq);  // x_i - x_jq
+          double2 seg1_64, tq2_64;
+          if constexpr (PREC == PREC_FP64) {
+            // the reference's own differences of box coordinates
+            seg1_64 = pbc2(p, xj, xjq);
+            tq2_64 = pbc2(p, xj, xq);
+          } else {
+            seg1_64 = make_double2(tq64.x - w64.x, tq64.y - w64.y);
+            tq2_64 = make_double2(seg_i64.x - w64.x, seg_i64.y - w64.y);
+          }
+          const T2 w1 = cvt2<T2>(w64);
+          const T2 tq1 = cvt2<T2>(tq64);
+          const T2 seg1 = cvt2<T2>(seg1_64);  // x_j - x_jq
+          const T2 tq2 = cvt2<T2>(tq2_64);    // x_j - x_q
+          const T w2 = fma(w1.y, w1.y, w1.x * w1.x);
+          const T tq1_2 = fma(tq1.y, tq1.y, tq1.x * tq1.x);
+          const T len1 = fma(seg1.y, seg1.y, seg1.x * seg1.x);
+          const T tq2_2 = fma(tq2.y, tq2.y, tq2.x * tq2.x);
+          if (!smooth_out_of_range(R, (float)tq1_2, (float)w2, sqrtf((float)len1))) {
+            const T2 pseg1 = cvt2<T2>(pbc2(p, xjq, xjqq));  // x_jq - x_jqq
+            smooth_core<POT, true, T>(p, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fi, dummy,
+                                      dummy, ei);
+          }
+          if (!smooth_out_of_range(R, (float)tq2_2, (float)w2, len_i)) {
+            const T2 mw1{-w1.x, -w1.y};  // x_j - x_i
+            smooth_core<POT, false, T>(p, tq2, tq2_2, mw1, seg_i, len2_i, pseg_i, rsum, inv_rsum, xj, xq, dummy, fi,
+                                       fq, ei);
+          }
+        }
+      }
+    }
+    // reduce over the L lanes of this vertex (lanes are contiguous in a warp)
+#pragma unroll
+    for (int o = L >> 1; o > 0; o >>= 1) {
+      fi.x += __shfl_xor_sync(0xffffffffu, fi.x, o);
+      fi.y += __shfl_xor_sync(0xffffffffu, fi.y, o);
+      ei += __shfl_xor_sync(0xffffffffu, ei, o);
+      if constexpr (INTER == INT_SMOOTH) {
+        fq.x += __shfl_xor_sync(0xffffffffu, fq.x, o);
+        fq.y += __shfl_xor_sync(0xffffffffu, fq.y, o);
+      }
+    }
+    if (lane == 0 && lv < nvt) {
+      s_fpair[lv] = make_double2(fi.x, fi.y);
+      s_epair[lv] = ei;
+      s_fprev[lv] = make_double2(fq.x, fq.y);
+    }
+  }
+  __syncthreads();
+
+  // ---- phase 4: totals and outputs ----------------------------------------
+  double2 F = make_double2(0.0, 0.0);
+  double evtx = 0.0;  // per-vertex energy as the reference stores it
+  double epair = 0.0;
+  if (t < nvt) {
+    const double2 fp = s_fpair[t];
+    F.x = fsh.x + fp.x;
+    F.y = fsh.y + fp.y;
+    if constexpr (INTER == INT_SMOOTH) {
+      const double2 fn = s_fprev[ln];
+      F.x += fn.x;
+      F.y += fn.y;
+      evtx = esh;
+    } else {
+      evtx = esh + s_epair[t];
+    }
+    epair = s_epair[t];
+  }
+
+  if constexpr (MODE == MODE_FORCE) {
+    if (t < nvt) {
+      const int v = v0 + t;
+      double2 Fo = F;
+      if (s.active) {
+        // DPM2D::addSelfPropulsion with the angle already advanced by the caller
+        const double psi = s.p_angle[ring];
+        double sn, cs;
+        sincos(psi, &sn, &cs);
+        Fo.x += s.driving * cs;
+        Fo.y += s.driving * sn;
+      }
+      s.force[v] = Fo;
+      s.energy[v] = evtx;
+      s.theta_out[v] = s_theta[t];
+      s.length_out[v] = dist_of(s_seg[t]);
+      if (k == 0) {
+        s.area_out[ring] = fabs(s_r0[t]) * 0.5;
+        s.perim_out[ring] = s_r1[t];
+        const double2 x0 = s_pos[t];
+        s.ppos_out[ring] = make_double2(x0.x + s_r2[t].x / nvr, x0.y + s_r2[t].y / nvr);
+      }
+    }
+    if constexpr (INTER == INT_SMOOTH) {
+      // ring energy = sum of the unit energies gathered by its vertices
+      __syncthreads();
+      if (t < nvt) s_r1[t] = epair;
+      for (int stride = 1; stride < TV; stride <<= 1) {
+        __syncthreads();
+        if (t < nvt && (k % (2 * stride)) == 0 && k + stride < nvr) s_r1[t] += s_r1[t + stride];
+      }
+      __syncthreads();
+      if (t < nvt && k == 0) s.p_energy[ring] = s_r1[t];
+    }
+    return;
+  } else {
+    // ---- MODE_STEP: integrator tail (src/Simulator.cu, src/FIRE.cu) ----------
+    double sums[NSUM] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    int nonfinite = 0;
+    const unsigned long long step = (unsigned long long)st->rng_step;
+    if (s.active) {
+      // addSelfPropulsion (src/DPM2D.cu:1995-2035): the ring's angle takes a
+      // N(0, sqrt(2 dt / taup)) increment and is wrapped to [-pi, pi); the
+      // ring's first vertex updates it once and shares it through its s_theta
+      // slot, which the step tail no longer reads
+      if (t < nvt && k == 0) {
+        double psi = s.p_angle[ring];
+        const double2 z = philox_normal2(s.seed, 2ull * step + 1ull, (unsigned long long)ring);
+        psi += s.sp_amp * z.x;
+        psi = psi + kPi;
+        psi = psi - 2.0 * kPi * floor(psi / (2.0 * kPi));
+        psi = psi - kPi;
+        s.p_angle[ring] = psi;
+        s_theta[t] = psi;
+      }
+      __syncthreads();
+      if (t < nvt) {
+        double sn, cs;
+        sincos(s_theta[lf], &sn, &cs);
+        F.x += s.driving * cs;
+        F.y += s.driving * sn;
+      }
+    }
+    if (t < nvt) {
+      const int v = v0 + t;
+      cp_async_wait_all();  // this thread's own copies of vel and last_pos
+      double2 vh = s_vel[t];
+      const double2 xl = s_last[t];
+      const double2 x = s_pos[t];
+      double2 vn;
+      double hdt = s.hdt;
+      if (s.kind == KIND_FIRE) hdt = 0.5 * s.fire_state[((st->fire_iters + 1) & 1) * 4];
+      if (s.kind == KIND_LANGEVIN) {
+        // langevinAddThermostatForces (src/Simulator.cu:68-73)
+        const double2 z = philox_normal2(s.seed, 2ull * step, (unsigned long long)ring);
+        F.x += s.noise * z.x - s.gamma * vh.x;
+        F.y += s.noise * z.y - s.gamma * vh.y;
+      }
+      if (s.kind == KIND_BROWNIAN || s.kind == KIND_DRIVEN_BROWNIAN) {
+        // updateBrownianVel / updateDrivenBrownianVel (src/Simulator.cu:168-200)
+        if (s.kind == KIND_BROWNIAN) {
+          const double2 z = philox_normal2(s.seed, 2ull * step, (unsigned long long)ring);
+          vn = make_double2((F.x + s.noise * z.x) / s.gamma, (F.y + s.noise * z.y) / s.gamma);
+        } else {
+          vn = make_double2(F.x / s.gamma, F.y / s.gamma);
+        }
+        const double2 xn = make_double2(x.x + s.dt * vn.x, x.y + s.dt * vn.y);
+        s.pos_out[v] = xn;
+        s.vel[v] = vn;
+        s.force[v] = F;
+        if (s.write_out) s.energy[v] = evtx;
+        if (3.0 * dist_of(pbc2(p, xn, xl)) > s.disp_cutoff) st->rebuild = 1;
+      } else {
+        // second half kick (kernelUpdateVertexVel, include/cudaKernel.cuh:1989-1996)
+        vn = make_double2(vh.x + hdt * F.x, vh.y + hdt * F.y);
+        if (s.advance) {
+          double2 vh2, xn;
+          if (s.kind == KIND_BAOAB) {
+            // BAOAB::integrate (src/Simulator.cu:112-144) for the next step
+            vh2 = make_double2(vn.x + s.hdt * F.x, vn.y + s.hdt * F.y);
+            xn = make_double2(x.x + s.hdt * vh2.x, x.y + s.hdt * vh2.y);
+            const double2 z = philox_normal2(s.seed, 2ull * (step + 1ull), (unsigned long long)ring);
+            vh2 = make_double2(s.gamma_factor * vh2.x + s.noise * z.x, s.gamma_factor * vh2.y + s.noise * z.y);
+            xn = make_double2(xn.x + s.hdt * vh2.x, xn.y + s.hdt * vh2.y);
+          } else {
+            vh2 = make_double2(vn.x + s.hdt * F.x, vn.y + s.hdt * F.y);
+            xn = make_double2(x.x + s.dt * vh2.x, x.y + s.dt * vh2.y);
+          }
+          s.pos_out[v] = xn;
+          s.vel[v] = vh2;
+          if (3.0 * dist_of(pbc2(p, xn, xl)) > s.disp_cutoff) st->rebuild = 1;
+        } else {
+          s.vel[v] = vn;
+          s.force[v] = F;
+          if (s.write_out) s.energy[v] = evtx;
+        }
+      }
+      if (s.accumulate) {
+        sums[S_PE] = evtx + ((INTER == INT_SMOOTH) ? epair : 0.0);
+        sums[S_VV] = vn.x * vn.x + vn.y * vn.y;
+        sums[S_VF] = vn.x * F.x + vn.y * F.y;
+        sums[S_FF] = F.x * F.x + F.y * F.y;
+        sums[S_FMAX2] = fmax(F.x * F.x, F.y * F.y);
+      }
+      if (!(isfinite(F.x) && isfinite(F.y))) {
+        sums[S_NONFINITE] = 1.0;
+        nonfinite = 1;
+      }
+    }
+    if (s.write_out && INTER == INT_SMOOTH) {
+      __syncthreads();
+      if (t < nvt) s_r1[t] = epair;
+      for (int stride = 1; stride < TV; stride <<= 1) {
+        __syncthreads();
+        if (t < nvt && (k % (2 * stride)) == 0 && k + stride < nvr) s_r1[t] += s_r1[t + stride];
+      }
+      __syncthreads();
+      if (t < nvt && k == 0) s.p_energy[ring] = s_r1[t];
+    }
+    if (s.accumulate) {
+      // per-CTA partials in a fixed order
+      const int warp = t / 32, wl = t % 32;
+#pragma unroll
+      for (int q = 0; q < NSUM; q++) {
+        double x = sums[q];
+        for (int o = 16; o > 0; o >>= 1) {
+          double y = __shfl_xor_sync(0xffffffffu, x, o);
+          x = (q == S_FMAX2) ? fmax(x, y) : x + y;
+        }
+        if (wl == 0) s_red[warp][q] = x;
+      }
+      __syncthreads();
+      if (t < NSUM) {
+        double x = 0.0;
+        for (int w = 0; w < BLOCK / 32; w++) x = (t == S_FMAX2) ? fmax(x, s_red[w][t]) : x + s_red[w][t];
+        s.partials[(size_t)blockIdx.x * NSUM + t] = x;
+      }
+    } else if (__syncthreads_or(nonfinite) && t == 0) {
+      st->nonfinite = 1;
+      st->abort = 1;
+    }
+    if (is_last_block(st)) {
+      if (s.accumulate) reduce_partials(s.partials, gridDim.x, st->sums);
+      __syncthreads();
+      if (t == 0) {
+        __threadfence();
+        if (s.accumulate && st->sums[S_NONFINITE] != 0.0) {
+          st->nonfinite = 1;
+          st->abort = 1;
+        }
+        if (s.kind == KIND_FIRE) {
+          st->fire_iters += 1;
+          if (s.fire_tol >= 0.0 && st->sums[S_FMAX2] <= s.fire_tol * s.fire_tol) st->converged = 1;
+        }
+        st->ops_done += 1;
+        if (s.kind != KIND_FIRE) st->rng_step += 1;
+        st->done_ctr = 0;
+        if (s.use_cond) cudaGraphSetConditional(s.cond, st->rebuild ? 1u : 0u);
+      }
+    }
+  }
+}
+
+}  // namespace cr

@@ -240,6 +240,17 @@ class DPM2D:
 
     def setUseGraphs(self, on): self._call("cr_set_use_graphs", int(bool(on)))
 
+    def setPrecision(self, precision):
+        """"fp64" (default, the reference's arithmetic) or "mixed" (FP32 pair
+        terms on FP64-formed offsets; everything else FP64)."""
+        code = {"fp64": 0, "mixed": 1}.get(precision, precision)
+        self._call("cr_set_precision", int(code))
+
+    def getPrecision(self):
+        out = C.c_int()
+        self._call("cr_get_precision", C.byref(out))
+        return {0: "fp64", 1: "mixed"}[out.value]
+
     def autotune(self, reps=50):
         out = C.c_int()
         self._call("cr_autotune", int(reps), C.byref(out))

@@ -49,6 +49,9 @@ enum { CR_PARTICLE_PASSIVE = 0, CR_PARTICLE_ACTIVE = 1, CR_PARTICLE_ACTIVE_SHAPE
 enum { CR_SHAPE_DEFORMABLE = 0, CR_SHAPE_RIGID = 1 };
 enum { CR_NOISE_LANGEVIN = 0, CR_NOISE_BAOAB = 1, CR_NOISE_BROWNIAN = 2, CR_NOISE_DRIVEN_BROWNIAN = 3 };
 enum { CR_GEOMETRY_NORMAL = 0, CR_GEOMETRY_FIXED_BOX = 1, CR_GEOMETRY_FIXED_SIDES = 2, CR_GEOMETRY_ROUND_BOX = 3 };
+/* Arithmetic of the deformable-ring force kernel (no reference counterpart;
+ * the reference is FP64 throughout). */
+enum { CR_PRECISION_FP64 = 0, CR_PRECISION_MIXED = 1 };
 
 /* ---- lifecycle -------------------------------------------------------- */
 
@@ -255,6 +258,14 @@ int cr_set_use_graphs(cr_ctx* ctx, int on);
  * largest ring (cr_profile_step_kernel, `reps` launches each) and keeps the
  * fastest; reports the choice.  Needs a neighbour list. */
 int cr_autotune(cr_ctx* ctx, long reps, int* lanes_out);
+/* CR_PRECISION_FP64 (default): every term in FP64, matching the reference.
+ * CR_PRECISION_MIXED: positions, velocities, integration, the shape terms
+ * and all reductions stay FP64; the vertex-vertex and vertex-segment pair
+ * terms run in FP32 on minimum-image offsets formed in FP64 and rounded
+ * once, with FP32 force accumulation per vertex.  Applies to the force
+ * evaluation, the fused step kernel and FIRE of deformable rings. */
+int cr_set_precision(cr_ctx* ctx, int precision);
+int cr_get_precision(const cr_ctx* ctx, int* precision);
 
 /* ---- neighbour list without allocation -----------------------------------
  * No counterpart in the reference.  For callers that cannot allocate device
