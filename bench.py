@@ -514,6 +514,7 @@ def run_reference_arm(args, world, rank):
     per = total_steps / max(1, args.steps)
     upd = R.ref_update_count()
     value = d.numVertices * total_steps / t
+    gpu_build = reference_cuda_build(d, c, vel)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -524,9 +525,42 @@ def run_reference_arm(args, world, rank):
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": f"{total_steps} NVE steps in {t:.1f} s, reference kernels as host code, "
                                        f"{threads} OpenMP threads"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_cuda_build": gpu_build}
     print(json.dumps(line), flush=True)
     d.close()
+
+
+def reference_cuda_build(d, c: dict, vel: np.ndarray, warmup: int = 100, steps: int = 2000) -> dict | None:
+    """The reference's own CUDA build (oracle/_ref/ref_gpu_nve, compiled from
+    its sources) on the same prepared state and thermal velocities, read from
+    the reference's on-disk packing format; timed with CUDA events inside it."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_gpu_nve")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_gpu_nve was not built (needs the reference checkout at build time)"}
+    import tempfile
+
+    from cudaring_b200 import packing_io, synth
+
+    nvl = d.numVertexInParticleList
+    pk = synth.Packing(nv_list=nvl, pos=d.getVertexPositions(), vel=vel, rad=d.getVertexRadii(), l0=d.getRestLengths(),
+                       theta0=d.getRestAngles(), a0=d.getRestAreas(), box=d.getBoxSize(),
+                       centres=np.zeros((len(nvl), 2)))
+    with tempfile.TemporaryDirectory() as tmp:
+        packing_io.save_packing_arrays(tmp, pk, digits=17)
+        try:
+            r = subprocess.run([exe, tmp, str(len(nvl)), str(warmup), str(steps), repr(c["dt"]), repr(c["ea"]),
+                                repr(c["el"]), repr(c["eb"]), "lj", "smooth", repr(c["LJcutoff"])],
+                               capture_output=True, text=True, timeout=600)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": "reference CUDA build did not finish within 600 s"}
+    if r.returncode != 0 or not r.stdout.strip():
+        return {"unavailable": f"reference CUDA build exited {r.returncode}: {r.stderr.strip()[-200:]}"}
+    info = json.loads(r.stdout.strip().splitlines()[-1])
+    return {"value": info["vertex_steps_per_s"], "unit": UNIT, "ms_per_step": info["ms_per_step"],
+            "steps": info["steps"], "warmup": info["warmup"], "rebuilds": info["updates"],
+            "sample": f"farceri/cudaRing DPM2D compiled for sm_100a, NVELoop() x {steps} after {warmup} warm-up "
+                      f"steps on the same {d.numVertices}-vertex state, CUDA-event timed"}
 
 
 if __name__ == "__main__":

@@ -391,6 +391,14 @@ std::vector<Op> make_ops(cr_ctx* ctx, int kind, long nsteps) {
       ops.push_back(Op{OP_FIRE_PRE, b, b, 0, 1, b});
       ops.push_back(Op{OP_TILE, b, b, 0, 0, b});
     }
+  } else if (kind == KIND_NVE_RESCALE) {
+    // NVERescale: rescale + first kick + drift, then force + second kick;
+    // the tile op's sum of v^2 feeds the next step's rescale
+    for (long i = 0; i < nsteps; i++) {
+      ops.push_back(Op{OP_DRIFT, b, b ^ 1, 0, 1, b ^ 1});
+      b ^= 1;
+      ops.push_back(Op{OP_TILE, b, b, 0, 0, b});
+    }
   } else if (kind == KIND_BROWNIAN || kind == KIND_DRIVEN_BROWNIAN) {
     ops.push_back(Op{OP_CHECK, b, b, 0, 1, b});
     for (long i = 0; i < nsteps; i++) {
@@ -422,7 +430,8 @@ void enqueue_op(cr_ctx* ctx, cudaStream_t st, const Op& op, int kind, bool use_c
   s.advance = op.advance;
   // per-CTA sums feed FIRE's next iteration and the rigid tail; energies
   // read by the caller are reduced afresh from the written arrays
-  s.accumulate = (kind == KIND_FIRE || ctx->shape == CR_SHAPE_RIGID) ? 1 : 0;
+  s.accumulate = (kind == KIND_FIRE || kind == KIND_NVE_RESCALE || ctx->shape == CR_SHAPE_RIGID) ? 1 : 0;
+  s.rescale_T = (kind == KIND_NVE_RESCALE && op.type == OP_DRIFT) ? ctx->T : 0.0;
   s.write_out = (kind == KIND_FIRE || !op.advance) ? 1 : 0;
   s.fire_tol = ctx->fp.tol;
   const SysArrays a = arrays(ctx, op.in_buf);
@@ -559,6 +568,14 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
     if ((rc = build_list(ctx, ctx->cur, ctx->cut_distance))) return rc;
   } else if ((rc = setup_grid(ctx, ctx->cut_distance))) {
     return rc;
+  }
+  if (kind == KIND_NVE_RESCALE) {
+    // the first rescale reads the sum of v^2 of the current velocities
+    launch_reduce(ctx->stream, ctx->nv, ctx->np, ctx->vel, ctx->force, ctx->energy, ctx->p_energy,
+                  inter_kind(ctx) == INT_SMOOTH, ctx->partials, ctx->status,
+                  std::min(2048, std::max(1, (ctx->nv + 255) / 256)));
+    ctx->launches++;
+    CR_TRY(cudaGetLastError());
   }
   if ((rc = clear_flags(ctx))) return rc;
   const long long upd0 = ctx->status_h->update_count;
@@ -996,6 +1013,10 @@ int cr_set_rest_angles(cr_ctx* ctx, const double* t0) {
   if (!ctx) return CR_EINVAL;
   return upload(ctx, ctx->theta0, t0, CR_NV1);
 }
+int cr_get_rest_angles(const cr_ctx* ctx, double* t0) {
+  if (!ctx) return CR_EINVAL;
+  return download(ctx, t0, ctx->theta0, CR_NV1);
+}
 int cr_get_areas(const cr_ctx* ctx, double* out) {
   if (!ctx) return CR_EINVAL;
   return download(ctx, out, ctx->area, CR_NP1);
@@ -1269,6 +1290,64 @@ int cr_init_nve(cr_ctx* ctx, double T, int readState) {
     CR_TRY(cudaStreamSynchronize(ctx->stream));
   }
   drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_init_nve_rescale(cr_ctx* ctx, double T) {
+  if (!ctx) return CR_EINVAL;
+  if (!(T > 0.0)) return ctx->fail(CR_EINVAL, "NVERescale needs a positive temperature");
+  // DPM2D::initNVERescale (src/DPM2D.cu:3778-3817): lastPos = pos, ring-rigid
+  // thermal velocities at amplitude sqrt(T), then scaled to T exactly
+  int rc = cr_reset_last_positions(ctx);
+  if (rc) return rc;
+  if ((rc = reset_rng_step(ctx))) return rc;
+  ctx->sim_kind = KIND_NVE_RESCALE;
+  ctx->T = T;
+  launch_inject_ke(ctx->stream, ctx->nv, ctx->ring_of, ctx->vel, std::sqrt(T), ctx->seed, (1ull << 61) + ctx->rng_calls++);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  if ((rc = reduce_now(ctx))) return rc;
+  const double Tcur = ctx->status_h->sums[S_VV] / (2.0 * ctx->nv);
+  if (!(Tcur > 0.0)) return ctx->fail(CR_ENONFINITE, "zero kinetic energy after the thermal draw");
+  launch_affine_vel(ctx->stream, ctx->nv, ctx->vel, std::sqrt(T / Tcur), make_double2(0.0, 0.0));
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_nve_rescale_loop(cr_ctx* ctx, long nsteps) {
+  if (!ctx || nsteps < 0) return CR_EINVAL;
+  if (ctx->sim_kind != KIND_NVE_RESCALE) return ctx->fail(CR_ESTATE, "cr_nve_rescale_loop before cr_init_nve_rescale");
+  if (nsteps == 0) return CR_OK;
+  return run_ops(ctx, KIND_NVE_RESCALE, nsteps);
+}
+
+int cr_conserve_momentum(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  int rc;
+  if (ctx->shape == CR_SHAPE_RIGID) {
+    // RigidLangevin / RigidNVE::conserveMomentum (src/Simulator.cu:309-312,
+    // 368-371): the mean ring velocity is removed (over every ring; the
+    // reference's single-CTA kernel covers only its first block of rings)
+    std::vector<double2> pv(ctx->np);
+    if ((rc = download(ctx, pv.data(), ctx->p_vel, ctx->np * sizeof(double2)))) return rc;
+    double mx = 0.0, my = 0.0;
+    for (const double2& u : pv) { mx += u.x; my += u.y; }
+    launch_affine_vel(ctx->stream, ctx->np, ctx->p_vel, 1.0, make_double2(-mx / ctx->np, -my / ctx->np));
+  } else {
+    // Langevin::conserveMomentum (src/Simulator.cu:91-108): the mean vertex
+    // velocity is removed
+    std::vector<double2> v(ctx->nv);
+    if ((rc = download(ctx, v.data(), ctx->vel, ctx->nv * sizeof(double2)))) return rc;
+    double mx = 0.0, my = 0.0;
+    for (const double2& u : v) { mx += u.x; my += u.y; }
+    launch_affine_vel(ctx->stream, ctx->nv, ctx->vel, 1.0, make_double2(-mx / ctx->nv, -my / ctx->nv));
+  }
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
   return CR_OK;
 }
 

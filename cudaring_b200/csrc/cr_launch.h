@@ -34,6 +34,7 @@ void launch_fire_pre(cudaStream_t st, const SysParams& p, const SysArrays& a, co
                      const FireParams& fp, double* fire_state, int nblocks);
 void launch_reduce(cudaStream_t st, int nv, int np, const double2* vel, const double2* force, const double* energy,
                    const double* p_energy, int use_p_energy, double* partials, DevStatus* status, int nblocks);
+void launch_affine_vel(cudaStream_t st, int n, double2* vel, double scale, double2 shift);
 void launch_inject_ke(cudaStream_t st, int nv, const int* ring_of, double2* vel, double amplitude,
                       unsigned long long seed, unsigned long long stream);
 void launch_scale_vertices(cudaStream_t st, int nv, int np, const int* ring_of, const double2* ppos, double2* pos,

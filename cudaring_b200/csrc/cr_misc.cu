@@ -32,7 +32,8 @@ __device__ __forceinline__ void op_finish(const StepArgs& s) {
 
 // First half kick + drift that opens an NVE / Langevin / BAOAB sequence:
 // kernelUpdateVertexVel(dt/2) then kernelUpdateVertexPos(dt)
-// (include/cudaKernel.cuh:1980-1996, src/Simulator.cu:23-30, 112-119).
+// (include/cudaKernel.cuh:1980-1996, src/Simulator.cu:23-30, 112-119); with
+// rescale_T set it opens every NVERescale step.
 __global__ void __launch_bounds__(256) k_drift(const __grid_constant__ SysParams p,
                                                const __grid_constant__ SysArrays a,
                                                const __grid_constant__ StepArgs s) {
@@ -43,6 +44,12 @@ __global__ void __launch_bounds__(256) k_drift(const __grid_constant__ SysParams
     const double2 x = a.pos[v];
     const double2 f = s.force[v];
     double2 vh = s.vel[v];
+    if (s.rescale_T > 0.0) {
+      // NVERescale::injectKineticEnergy (src/Simulator.cu:224-238): T from the
+      // sum of v^2 that the previous op reduced, T = sum v^2 / (2 Nv)
+      const double scale = sqrt(s.rescale_T / (st->sums[S_VV] / (2.0 * p.nv)));
+      vh = make_double2(vh.x * scale, vh.y * scale);
+    }
     vh = make_double2(vh.x + s.hdt * f.x, vh.y + s.hdt * f.y);
     double2 xn;
     if (s.kind == KIND_BAOAB) {
@@ -163,6 +170,16 @@ __global__ void __launch_bounds__(256) k_reduce(int nv, int np, const double2* v
   }
 }
 
+// v <- scale * v + shift for n double2 velocities (exact temperature after a
+// thermal draw; momentum removal).
+__global__ void k_affine_vel(int n, double2* vel, double scale, double2 shift) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < n) {
+    const double2 u = vel[v];
+    vel[v] = make_double2(scale * u.x + shift.x, scale * u.y + shift.y);
+  }
+}
+
 // Langevin::injectKineticEnergy (src/Simulator.cu:32-52): every vertex takes
 // its ring's N(0, amplitude) velocity.
 __global__ void k_inject_ke(int nv, const int* ring_of, double2* vel, double amplitude, unsigned long long seed,
@@ -229,6 +246,9 @@ void launch_fire_pre(cudaStream_t st, const SysParams& p, const SysArrays& a, co
 void launch_reduce(cudaStream_t st, int nv, int np, const double2* vel, const double2* force, const double* energy,
                    const double* p_energy, int use_p_energy, double* partials, DevStatus* status, int nblocks) {
   k_reduce<<<nblocks, 256, 0, st>>>(nv, np, vel, force, energy, p_energy, use_p_energy, partials, status);
+}
+void launch_affine_vel(cudaStream_t st, int n, double2* vel, double scale, double2 shift) {
+  k_affine_vel<<<(n + 255) / 256, 256, 0, st>>>(n, vel, scale, shift);
 }
 void launch_inject_ke(cudaStream_t st, int nv, const int* ring_of, double2* vel, double amplitude,
                       unsigned long long seed, unsigned long long stream) {

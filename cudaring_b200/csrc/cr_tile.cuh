@@ -22,7 +22,7 @@ namespace cr {
 enum Mode : int { MODE_FORCE = 0, MODE_STEP = 1 };
 enum Kind : int {
   KIND_NVE = 0, KIND_LANGEVIN = 1, KIND_BAOAB = 2, KIND_BROWNIAN = 3, KIND_DRIVEN_BROWNIAN = 4,
-  KIND_FIRE = 5, KIND_NONE = 6
+  KIND_FIRE = 5, KIND_NONE = 6, KIND_NVE_RESCALE = 7
 };
 
 constexpr int NSUM = 6;  // per-CTA partial sums: PE, sum v^2, v.F, sum v^2 (again), sum F^2, max F_d^2
@@ -55,6 +55,7 @@ struct StepArgs {
   double driving, sp_amp;
   double disp_cutoff;
   double fire_tol;
+  double rescale_T;        // > 0: scale velocities to this temperature before the kick (NVERescale)
   unsigned long long seed;
 };
 

@@ -137,6 +137,7 @@ class DPM2D:
     def setRestLengths(self, a): self._call("cr_set_rest_lengths", _f64(a).ctypes.data)
     def getRestLengths(self): return self._get("cr_get_rest_lengths", self.numVertices)
     def setRestAngles(self, a): self._call("cr_set_rest_angles", _f64(a).ctypes.data)
+    def getRestAngles(self): return self._get("cr_get_rest_angles", self.numVertices)
     def getAreas(self): return self._get("cr_get_areas", self.numParticles)
     def getPerimeters(self): return self._get("cr_get_perimeters", self.numParticles)
     def getSegmentLengths(self): return self._get("cr_get_segment_lengths", self.numVertices)
@@ -191,6 +192,9 @@ class DPM2D:
     # ------------------------------------------------------------ integrators
     def initNVE(self, T, readState=False): self._call("cr_init_nve", T, int(bool(readState)))
     def NVELoop(self, nsteps=1): self._call("cr_nve_loop", int(nsteps))
+    def initNVERescale(self, T): self._call("cr_init_nve_rescale", T)
+    def NVERescaleLoop(self, nsteps=1): self._call("cr_nve_rescale_loop", int(nsteps))
+    def conserveMomentum(self): self._call("cr_conserve_momentum")
     def initLangevin(self, T, gamma, readState=False): self._call("cr_init_langevin", T, gamma, int(bool(readState)))
     def langevinLoop(self, nsteps=1): self._call("cr_langevin_loop", int(nsteps))
 

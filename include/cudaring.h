@@ -119,6 +119,7 @@ int cr_get_rest_areas(const cr_ctx* ctx, double* a0);
 int cr_set_rest_lengths(cr_ctx* ctx, const double* l0);
 int cr_get_rest_lengths(const cr_ctx* ctx, double* l0);
 int cr_set_rest_angles(cr_ctx* ctx, const double* theta0);
+int cr_get_rest_angles(const cr_ctx* ctx, double* theta0);
 /* DPM2D::getAreas / getPerimeters / getSegmentLengths / getSegmentAngles
  * (include/DPM2D.h:295-302), as of the last force evaluation. */
 int cr_get_areas(const cr_ctx* ctx, double* area);
@@ -185,6 +186,15 @@ int cr_scale_vertices(cr_ctx* ctx, double scale);
 int cr_init_nve(cr_ctx* ctx, double T, int readState);
 /* DPM2D::NVELoop (include/DPM2D.h:686), nsteps times. */
 int cr_nve_loop(cr_ctx* ctx, long nsteps);
+/* DPM2D::initNVERescale (include/DPM2D.h:688): ring-rigid thermal
+ * velocities scaled to exactly T; each NVERescaleLoop step (:690) first
+ * scales all velocities back to T (NVERescale, src/Simulator.cu:215-238). */
+int cr_init_nve_rescale(cr_ctx* ctx, double T);
+int cr_nve_rescale_loop(cr_ctx* ctx, long nsteps);
+/* SimInterface::conserveMomentum (include/Simulator.h:51): removes the mean
+ * vertex velocity (deformable rings, src/Simulator.cu:91-108) or the mean
+ * ring velocity over all rings (rigid rings, src/Simulator.cu:309-312). */
+int cr_conserve_momentum(cr_ctx* ctx);
 /* DPM2D::initLangevin (include/DPM2D.h:680): the noise type selects
  * Langevin, BAOAB, Brownian or driven Brownian (src/DPM2D.cu:3713-3753). */
 int cr_init_langevin(cr_ctx* ctx, double T, double gamma, int readState);

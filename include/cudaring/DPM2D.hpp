@@ -120,6 +120,9 @@ class DPM2D {
   // integrators (one step per call by default, as in the reference)
   void initNVE(double T, bool readState) { ok(cr_init_nve(ctx_, T, readState ? 1 : 0), "initNVE"); }
   void NVELoop(long nsteps = 1) { ok(cr_nve_loop(ctx_, nsteps), "NVELoop"); }
+  void initNVERescale(double T) { ok(cr_init_nve_rescale(ctx_, T), "initNVERescale"); }
+  void NVERescaleLoop(long nsteps = 1) { ok(cr_nve_rescale_loop(ctx_, nsteps), "NVERescaleLoop"); }
+  void conserveMomentum() { ok(cr_conserve_momentum(ctx_), "conserveMomentum"); }
   void initLangevin(double T, double gamma, bool readState) {
     ok(cr_init_langevin(ctx_, T, gamma, readState ? 1 : 0), "initLangevin");
   }

@@ -113,6 +113,7 @@ def ref():
                    "ref_total_force_magnitude", "ref_phi"):
             getattr(R, fn).restype = C.c_double
         R.ref_nve_loop.argtypes = [C.c_long]
+        R.ref_nve_rescale_loop.argtypes = [C.c_long, C.c_double]
         R.ref_langevin_loop.argtypes = [C.c_long, C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_void_p]
         R.ref_brownian_loop.argtypes = [C.c_long, C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_void_p]
         R.ref_baoab_loop.argtypes = [C.c_long, C.c_double, C.c_double, C.c_void_p]

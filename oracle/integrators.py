@@ -4,6 +4,7 @@ TEST INFRASTRUCTURE ONLY.  Forces come from the C restatement (oracle.c);
 the updates restate:
 
 * ``NVE::integrate`` (src/Simulator.cu:206-212),
+* ``NVERescale::integrate`` (src/Simulator.cu:215-238),
 * ``Langevin::integrate`` / ``updateThermalVel`` (src/Simulator.cu:23-30, 54-77),
 * ``BAOAB::integrate`` (src/Simulator.cu:112-144),
 * ``Brownian::integrate`` / ``DrivenBrownian`` (src/Simulator.cu:147-203),
@@ -77,6 +78,12 @@ class OracleState:
         self.pangle = a - math.pi
         p = self.pangle[self.s.pid]
         self.force = self.force + driving * np.stack([np.cos(p), np.sin(p)], axis=1).reshape(-1)
+
+    def nve_rescale_step(self, dt, T_inject):
+        """NVERescale::integrate / injectKineticEnergy (src/Simulator.cu:215-238)."""
+        T = float(np.dot(self.vel, self.vel)) / len(self.vel)
+        self.vel *= math.sqrt(T_inject / T)
+        self.nve_step(dt)
 
     def langevin_step(self, dt, gamma, noise_amp, xi, driving=0.0, dpsi=None):
         self.vel += 0.5 * dt * self.force

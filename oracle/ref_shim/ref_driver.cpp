@@ -345,6 +345,24 @@ void ref_nve_loop(long nsteps) {
   }
 }
 
+// NVERescale::integrate / injectKineticEnergy (Simulator.cu:215-238): scale
+// every velocity by sqrt(Tinject / T), T = 2K / (2 Nv) (DPM2D.cu getTemperature),
+// then one NVE step.
+void ref_nve_rescale_loop(long nsteps, double Tinject) {
+  for (long s = 0; s < nsteps; s++) {
+    double vv = 0.0;
+    for (long i = 0; i < 2 * M.nv; i++) vv += M.vel[i] * M.vel[i];
+    const double T = vv / (2.0 * M.nv);
+    const double scale = sqrt(Tinject / T);
+    for (long i = 0; i < 2 * M.nv; i++) M.vel[i] *= scale;
+    update_vertex_vel(0.5 * M.dt);
+    update_vertex_pos(M.dt);
+    check_neighbors();
+    calc_force_energy();
+    update_vertex_vel(0.5 * M.dt);
+  }
+}
+
 // Langevin::integrate (Simulator.cu:23-30).  `xi` holds nsteps * np * 2
 // standard-normal draws (the reference draws them from Thrust); step s uses
 // xi[s*np*2 .. (s+1)*np*2).  noise = sqrt(2 T gamma / dt) (DPM2D.cu:3718).

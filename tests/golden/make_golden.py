@@ -301,10 +301,30 @@ def rigid_cases():
     print(f"rigid_force_wca: nv={pk.num_vertices} maxF={np.abs(d['out_force']).max():.3e}")
 
 
+def rescale_cases():
+    # NVE with velocity rescaling to Tinject before every step (NVERescale).
+    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 205)
+    rng = np.random.default_rng(9)
+    pk.vel = np.repeat(rng.normal(0.0, 0.1, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
+    dt, nsteps, Tinject = 0.005, 120, 0.02
+    R, cut = setup_ref(pk, "harmonic", "vertexVertex")
+    R.ref_set_time_step(dt)
+    R.ref_calc_neighbor_list(cut)
+    R.ref_reset_last_positions()
+    R.ref_calc_force_energy()
+    R.ref_nve_rescale_loop(nsteps, Tinject)
+    d = inputs(pk, potential=0, interaction=0, ea=1.0, el=1.0, eb=0.01, ec=1.0, lj_cutoff=2.5, dt=dt,
+               nsteps=nsteps, T=Tinject, cut_distance=cut)
+    d.update(grab(R, pk, ["pos", "vel", "force"]))
+    d["out_update_count"] = np.asarray(R.ref_update_count())
+    np.savez_compressed(os.path.join(OUT, "traj_nverescale_harmonic_vv.npz"), **d)
+    print(f"traj_nverescale_harmonic_vv: updates={int(d['out_update_count'])}")
+
+
 if __name__ == "__main__":
     if not oracle.ref_available():
         oracle.build()
-    which = sys.argv[1:] or ["force", "traj", "stochastic", "rigid"]
+    which = sys.argv[1:] or ["force", "traj", "stochastic", "rigid", "rescale"]
     if "force" in which:
         force_cases()
     if "traj" in which:
@@ -313,3 +333,5 @@ if __name__ == "__main__":
         stochastic_cases()
     if "rigid" in which:
         rigid_cases()
+    if "rescale" in which:
+        rescale_cases()

@@ -127,6 +127,30 @@ def test_langevin_trajectory_philox(cuda_device):
     assert rel_inf(d.getVertexVelocities(), g["out_vel"]) < 1e-9
 
 
+def test_nve_rescale_trajectory(cuda_device):
+    g = load_golden(golden_files("traj_nverescale_harmonic_vv")[0])
+    d = _prepared(g)
+    T = float(g["param_T"])
+    d.initNVERescale(T)
+    assert d.getTemperature() == pytest.approx(T, rel=1e-12)
+    d.setVertexVelocities(g["vel"])
+    d.NVERescaleLoop(int(g["param_nsteps"]))
+    assert d.getUpdateCount() == int(g["out_update_count"])
+    assert rel_inf(d.getVertexPositions(), g["out_pos"]) < 1e-12
+    assert rel_inf(d.getVertexVelocities(), g["out_vel"]) < 1e-9
+
+
+def test_conserve_momentum(cuda_device):
+    g = load_golden(golden_files("traj_nve_harmonic_vv")[0])
+    d = _prepared(g)
+    d.setVertexVelocities(g["vel"] + 0.25)
+    d.conserveMomentum()
+    v = d.getVertexVelocities().reshape(-1, 2)
+    assert np.abs(v.mean(axis=0)).max() < 1e-14
+    assert np.allclose(v, (g["vel"] + 0.25).reshape(-1, 2) - (g["vel"] + 0.25).reshape(-1, 2).mean(axis=0),
+                       rtol=0, atol=1e-14)
+
+
 @pytest.mark.parametrize("kind", ["baoab", "brownian", "drivenbrownian", "active_langevin"])
 def test_stochastic_integrators_match_reference(cuda_device, kind):
     g = load_golden(golden_files(f"traj_{kind}_harmonic_vv")[0])

@@ -80,6 +80,16 @@ def test_nve_trajectory_lj_smooth():
     assert rel_inf(st.force, g["out_force"]) < 1e-9
 
 
+def test_nve_rescale_trajectory():
+    g = load_golden(golden_files("traj_nverescale_harmonic_vv")[0])
+    st = _state(g)
+    for _ in range(int(g["param_nsteps"])):
+        st.nve_rescale_step(float(g["param_dt"]), float(g["param_T"]))
+    assert st.update_count == int(g["out_update_count"])
+    assert rel_inf(st.pos, g["out_pos"]) < 1e-12
+    assert rel_inf(st.vel, g["out_vel"]) < 1e-10
+
+
 def test_fire_trajectory():
     g = load_golden(golden_files("traj_fire_harmonic_vv")[0])
     st = _state(g)
