@@ -86,9 +86,17 @@ __device__ __forceinline__ int pq_second(int pk) { return pk >> 16; }
 __device__ __forceinline__ double pbc1(double d, double size, double inv) {
   return d - size * round(d * inv);
 }
-__device__ __forceinline__ double2 pbc2(const SysParams& p, double2 a, double2 b) {
+// B: anything with lx, ly, inv_lx, inv_ly (SysParams, or Box for one system
+// of a batch)
+template <class B>
+__device__ __forceinline__ double2 pbc2(const B& p, double2 a, double2 b) {
   return make_double2(pbc1(a.x - b.x, p.lx, p.inv_lx), pbc1(a.y - b.y, p.ly, p.inv_ly));
 }
+
+// Periodic box of one system of a batch.
+struct Box {
+  double lx, ly, inv_lx, inv_ly;
+};
 
 // Pair magnitude for the vertex-vertex path: returns gradMultiple g (force on
 // "this" is g * delta / d) and sets the half-pair energy.  Restates

@@ -19,6 +19,10 @@ struct LaunchCfg {
 void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
                  const StepArgs& s);
 int tile_vertices(int lanes);
+// cr_tile_batch.cu: the same kernel over the tiles of many systems (tile.x =
+// system, s.bsys the per-system table); lanes 1, 2 or 4
+void launch_tile_batch(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
+                       const StepArgs& s);
 // cr_tile_mixed.cu (expects p with its FP32 constants filled)
 void launch_tile_mixed(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
                        const StepArgs& s);
@@ -95,5 +99,8 @@ struct NbrArgs {
   int count_update;   // 1: a displacement-triggered rebuild (DPM2D::updateCount += 1)
 };
 void launch_nbr_build(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n);
+// building blocks shared with the batched build (cr_batch.cu)
+void launch_cell_scan(cudaStream_t st, int ncells, int* cell_cnt, int* cell_start);
+void launch_cell_sort(cudaStream_t st, int ncells, const NbrArgs& n);
 
 }  // namespace cr

@@ -213,6 +213,16 @@ __global__ void k_nbr_guard_reset(DevStatus* st) {
   }
 }
 
+void launch_cell_scan(cudaStream_t st, int ncells, int* cell_cnt, int* cell_start) {
+  k_cell_scan<<<1, 1024, 0, st>>>(ncells, cell_cnt, cell_start);
+}
+
+void launch_cell_sort(cudaStream_t st, int ncells, const NbrArgs& n) {
+  k_cell_sort<<<(ncells + 255) / 256, 256, 0, st>>>(ncells, n.cell_start, n.cell_vid, n.pos, n.rad, n.ring_of,
+                                                    n.nbr_pq ? n.pq_pack : nullptr, n.cell_pos, n.cell_rad,
+                                                    n.cell_ring, n.nbr_pq ? n.cell_pq : nullptr);
+}
+
 void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g, const NbrArgs& n) {
   const int nb = (p.nv + 255) / 256;
   k_nbr_guard_reset<<<1, 32, 0, stream>>>(n.status);

@@ -28,6 +28,21 @@ enum Kind : int {
 constexpr int NSUM = 6;  // per-CTA partial sums: PE, sum v^2, v.F, sum v^2 (again), sum F^2, max F_d^2
 enum SumIdx : int { S_PE = 0, S_VV = 1, S_VF = 2, S_FF = 3, S_FMAX2 = 4, S_NONFINITE = 5 };
 
+// One system of a batch: its box, rebuild/convergence flags, FIRE counters
+// and the sums its last tile reduces from its tiles' partials.
+struct BatchSys {
+  Box box;
+  double disp_cutoff;      // DPM2D::cutoff of this system
+  double fire_tol;         // FIRE stops when max_i,d |F_i,d| <= fire_tol (< 0: never)
+  double sums[NSUM];
+  long long fire_iters;
+  int tile_begin, tile_end;
+  int rebuild;             // this system's displacement check fired
+  int converged;           // FIRE reached fire_tol: the system is frozen
+  int active;              // 0: the system takes no part in step ops
+  unsigned int done_ctr;   // tiles of this system finished in the current op
+};
+
 struct StepArgs {
   double2* pos_out;        // next positions (MODE_STEP with advance)
   double2* vel;
@@ -56,6 +71,8 @@ struct StepArgs {
   double disp_cutoff;
   double fire_tol;
   double rescale_T;        // > 0: scale velocities to this temperature before the kick (NVERescale)
+  BatchSys* bsys;          // batch mode: per-system table (tile.x is the system)
+  const double* bfire_state;  // batch mode: [S][2][4] FIRE scalars per system
   unsigned long long seed;
 };
 
@@ -300,10 +317,10 @@ __device__ __forceinline__ bool pair_eval_t(const SysParams& p, float d2, float 
   return pair_eval_f<POT>(p, d2, rsum, inv_rsum, gm, inv_d, ep);
 }
 
-template <int POT, bool ROLE1, typename T, typename T2 = typename Vec2<T>::type>
-__device__ __forceinline__ void smooth_core(const SysParams& p, T2 tq, T tq2, T2 w, T2 seg, T len2, T2 pseg, T rsum,
-                                            T inv_rsum, double2 tabs, double2 qabs, T2& ft, T2& fo, T2& fq,
-                                            double& e) {
+template <int POT, bool ROLE1, typename T, class B, typename T2 = typename Vec2<T>::type>
+__device__ __forceinline__ void smooth_core(const SysParams& p, const B& bx, T2 tq, T tq2, T2 w, T2 seg, T len2,
+                                            T2 pseg, T rsum, T inv_rsum, double2 tabs, double2 qabs, T2& ft,
+                                            T2& fo, T2& fq, double& e) {
   const T inv_len = rsq(len2);
   const T inv_lsq = inv_len * inv_len;
   const T proj = (tq.x * seg.x + tq.y * seg.y) * inv_lsq;
@@ -316,7 +333,7 @@ __device__ __forceinline__ void smooth_core(const SysParams& p, T2 tq, T tq2, T2
       // it (pbcDistance(thisPos, previousPos + proj * segment)), so that
       // near-contact distances carry the same rounding as there
       const double2 pj = make_double2(qabs.x + proj * seg.x, qabs.y + proj * seg.y);
-      const double2 dpv = pbc2(p, tabs, pj);
+      const double2 dpv = pbc2(bx, tabs, pj);
       dpx = dpv.x;
       dpy = dpv.y;
     } else {

@@ -1,0 +1,45 @@
+// Batch-mode instantiations of the tiled force + integrator kernel (many
+// independent systems in one grid; see BatchSys), FP64 and mixed precision.
+#include "cr_launch.h"
+#include "cr_tile_kernel.cuh"
+
+namespace cr {
+
+template <int POT, int INTER, int MODE, int PREC>
+static void launch_batch_t(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s) {
+  if (c.lanes == 1) k_tile<POT, INTER, MODE, 128, 1, PREC, true><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+  else if (c.lanes == 4) k_tile<POT, INTER, MODE, 256, 4, PREC, true><<<c.grid, 256, 0, c.stream>>>(p, a, s);
+  else k_tile<POT, INTER, MODE, 128, 2, PREC, true><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+}
+
+template <int PREC>
+static void launch_batch_p(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
+                           const StepArgs& s) {
+#define CR_BATCH_CASE(P)                                                                   \
+  case P:                                                                                  \
+    if (inter == INT_VV) {                                                                 \
+      if (mode == MODE_FORCE) launch_batch_t<P, INT_VV, MODE_FORCE, PREC>(c, p, a, s);     \
+      else launch_batch_t<P, INT_VV, MODE_STEP, PREC>(c, p, a, s);                         \
+    } else {                                                                               \
+      if (mode == MODE_FORCE) launch_batch_t<P, INT_SMOOTH, MODE_FORCE, PREC>(c, p, a, s); \
+      else launch_batch_t<P, INT_SMOOTH, MODE_STEP, PREC>(c, p, a, s);                     \
+    }                                                                                      \
+    break;
+  switch (pot) {
+    CR_BATCH_CASE(POT_HARMONIC)
+    CR_BATCH_CASE(POT_LJ)
+    CR_BATCH_CASE(POT_ADHESIVE)
+    CR_BATCH_CASE(POT_WCA)
+    default: break;
+  }
+#undef CR_BATCH_CASE
+}
+
+void launch_tile_batch(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p_in, const SysArrays& a,
+                       const StepArgs& s) {
+  const SysParams p = with_f32_constants(p_in);
+  if (c.precision == CR_PRECISION_MIXED) launch_batch_p<PREC_MIXED>(c, pot, inter, mode, p, a, s);
+  else launch_batch_p<PREC_FP64>(c, pot, inter, mode, p, a, s);
+}
+
+}  // namespace cr

@@ -41,7 +41,30 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC>
+// Box of the current tile: the system's parameters, or one system of a batch.
+template <bool BATCH> struct BoxSel;
+template <> struct BoxSel<false> {
+  __device__ static const SysParams& get(const SysParams& p, const Box&) { return p; }
+};
+template <> struct BoxSel<true> {
+  __device__ static const Box& get(const SysParams&, const Box& b) { return b; }
+};
+
+// Every CTA ends in the last-block protocol so that the op counter and the
+// conditional rebuild node see each op exactly once.
+__device__ __forceinline__ void tile_skip(const StepArgs& s, DevStatus* st) {
+  if (is_last_block(st)) {
+    if (threadIdx.x == 0) {
+      st->done_ctr = 0;
+      if (s.use_cond) cudaGraphSetConditional(s.cond, st->rebuild ? 1u : 0u);
+    }
+  }
+}
+
+// BATCH: the grid covers the tiles of many independent systems; tile.x is
+// the system, whose box, displacement cutoff, FIRE scalars and flags come
+// from s.bsys, and whose last tile reduces the system's partial sums.
+template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH = false>
 __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const __grid_constant__ SysParams p,
                                                 const __grid_constant__ SysArrays a,
                                                 const __grid_constant__ StepArgs s) {
@@ -62,6 +85,8 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
   __shared__ __align__(16) double2 s_vel[TS];
   __shared__ __align__(16) double2 s_last[TS];
   __shared__ double s_red[BLOCK / 32][NSUM];
+  __shared__ Box s_box;
+  __shared__ bool s_syslast;
 
   DevStatus* st = s.status;
   if (MODE == MODE_STEP && (st->abort | st->converged)) {
@@ -78,6 +103,16 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
   const int4 tile = a.tiles[blockIdx.x];
   const int v0 = tile.z, nvt = tile.w - tile.z;
   const int t = threadIdx.x;
+  const int sysid = BATCH ? tile.x : 0;
+  if constexpr (BATCH) {
+    const BatchSys& bs = s.bsys[sysid];
+    if (!bs.active || (MODE == MODE_STEP && bs.converged)) {
+      if constexpr (MODE == MODE_STEP) tile_skip(s, st);
+      return;
+    }
+    if (t == 0) s_box = bs.box;
+  }
+  const auto& bx = BoxSel<BATCH>::get(p, s_box);
 
   // ---- prologue: every per-vertex input, in parallel ------------------------
   int ring = -1, k = 0, lf = 0, lp = 0, ln = 0, nvr = 1;
@@ -108,11 +143,11 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
   if (t < nvt) {
     const double2 x = s_pos[t];
     const double2 xn = s_pos[ln];
-    const double2 seg = pbc2(p, xn, x);
+    const double2 seg = pbc2(bx, xn, x);
     s_seg[t] = seg;
     const double2 x0 = s_pos[lf];
-    const double2 u = pbc2(p, x, x0);
-    const double2 un = pbc2(p, xn, x0);
+    const double2 u = pbc2(bx, x, x0);
+    const double2 un = pbc2(bx, xn, x0);
     s_r0[t] = u.x * un.y - un.x * u.y;
     s_r1[t] = dist_of(seg);
     s_r2[t] = u;
@@ -204,8 +239,8 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
           const double rj = __ldg(a.rad + j);
           sl += L;
           if (sl < cnt) jn = __ldg(a.nbr + (size_t)sl * stride + i);
-          if constexpr (PREC == PREC_MIXED) pair_own_f<POT>(p, f2(pbc2(p, xi, xj)), (float)(ri + rj), fi, ei);
-          else pair_own<POT>(p, pbc2(p, xi, xj), ri + rj, fi, ei);
+          if constexpr (PREC == PREC_MIXED) pair_own_f<POT>(p, f2(pbc2(bx, xi, xj)), (float)(ri + rj), fi, ei);
+          else pair_own<POT>(p, pbc2(bx, xi, xj), ri + rj, fi, ei);
         }
       } else {
         // Smooth units of vertex i: role 1 (i against the segment prev(j) -> j)
@@ -236,13 +271,13 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
           const T rsum = (T)rsum64;
           const T inv_rsum = T(1) / rsum;
           const float R = range * (float)rsum64;
-          const double2 w64 = pbc2(p, xi, xj);    // x_i - x_j
-          const double2 tq64 = pbc2(p, xi, xjq);  // x_i - x_jq
+          const double2 w64 = pbc2(bx, xi, xj);    // x_i - x_j
+          const double2 tq64 = pbc2(bx, xi, xjq);  // x_i - x_jq
           double2 seg1_64, tq2_64;
           if constexpr (PREC == PREC_FP64) {
             // the reference's own differences of box coordinates
-            seg1_64 = pbc2(p, xj, xjq);
-            tq2_64 = pbc2(p, xj, xq);
+            seg1_64 = pbc2(bx, xj, xjq);
+            tq2_64 = pbc2(bx, xj, xq);
           } else {
             seg1_64 = make_double2(tq64.x - w64.x, tq64.y - w64.y);
             tq2_64 = make_double2(seg_i64.x - w64.x, seg_i64.y - w64.y);
@@ -256,13 +291,13 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
           const T len1 = fma(seg1.y, seg1.y, seg1.x * seg1.x);
           const T tq2_2 = fma(tq2.y, tq2.y, tq2.x * tq2.x);
           if (!smooth_out_of_range(R, (float)tq1_2, (float)w2, sqrtf((float)len1))) {
-            const T2 pseg1 = cvt2<T2>(pbc2(p, xjq, xjqq));  // x_jq - x_jqq
-            smooth_core<POT, true, T>(p, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fi, dummy,
+            const T2 pseg1 = cvt2<T2>(pbc2(bx, xjq, xjqq));  // x_jq - x_jqq
+            smooth_core<POT, true, T>(p, bx, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fi, dummy,
                                       dummy, ei);
           }
           if (!smooth_out_of_range(R, (float)tq2_2, (float)w2, len_i)) {
             const T2 mw1{-w1.x, -w1.y};  // x_j - x_i
-            smooth_core<POT, false, T>(p, tq2, tq2_2, mw1, seg_i, len2_i, pseg_i, rsum, inv_rsum, xj, xq, dummy, fi,
+            smooth_core<POT, false, T>(p, bx, tq2, tq2_2, mw1, seg_i, len2_i, pseg_i, rsum, inv_rsum, xj, xq, dummy, fi,
                                        fq, ei);
           }
         }
@@ -377,7 +412,11 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
       const double2 x = s_pos[t];
       double2 vn;
       double hdt = s.hdt;
-      if (s.kind == KIND_FIRE) hdt = 0.5 * s.fire_state[((st->fire_iters + 1) & 1) * 4];
+      if (s.kind == KIND_FIRE) {
+        if constexpr (BATCH) hdt = 0.5 * s.bfire_state[(sysid * 2 + ((s.bsys[sysid].fire_iters + 1) & 1)) * 4];
+        else hdt = 0.5 * s.fire_state[((st->fire_iters + 1) & 1) * 4];
+      }
+      const double dcut = BATCH ? s.bsys[sysid].disp_cutoff : s.disp_cutoff;
       if (s.kind == KIND_LANGEVIN) {
         // langevinAddThermostatForces (src/Simulator.cu:68-73)
         const double2 z = philox_normal2(s.seed, 2ull * step, (unsigned long long)ring);
@@ -397,7 +436,10 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
         s.vel[v] = vn;
         s.force[v] = F;
         if (s.write_out) s.energy[v] = evtx;
-        if (3.0 * dist_of(pbc2(p, xn, xl)) > s.disp_cutoff) st->rebuild = 1;
+        if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
+          st->rebuild = 1;
+          if constexpr (BATCH) s.bsys[sysid].rebuild = 1;
+        }
       } else {
         // second half kick (kernelUpdateVertexVel, include/cudaKernel.cuh:1989-1996)
         vn = make_double2(vh.x + hdt * F.x, vh.y + hdt * F.y);
@@ -416,7 +458,10 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
           }
           s.pos_out[v] = xn;
           s.vel[v] = vh2;
-          if (3.0 * dist_of(pbc2(p, xn, xl)) > s.disp_cutoff) st->rebuild = 1;
+          if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
+            st->rebuild = 1;
+            if constexpr (BATCH) s.bsys[sysid].rebuild = 1;
+          }
         } else {
           s.vel[v] = vn;
           s.force[v] = F;
@@ -467,16 +512,45 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
       st->nonfinite = 1;
       st->abort = 1;
     }
+    if constexpr (BATCH) {
+      if (s.accumulate) {
+        // the system's last tile reduces the system's partials
+        BatchSys& bs = s.bsys[sysid];
+        __syncthreads();
+        if (t == 0) {
+          __threadfence();
+          const unsigned int prev = atomicAdd(&bs.done_ctr, 1u);
+          s_syslast = (prev == (unsigned int)(bs.tile_end - bs.tile_begin - 1));
+        }
+        __syncthreads();
+        if (s_syslast) {
+          reduce_partials(s.partials + (size_t)bs.tile_begin * NSUM, bs.tile_end - bs.tile_begin, bs.sums);
+          __syncthreads();
+          if (t == 0) {
+            __threadfence();
+            if (bs.sums[S_NONFINITE] != 0.0) {
+              st->nonfinite = 1;
+              st->abort = 1;
+            }
+            if (s.kind == KIND_FIRE) {
+              bs.fire_iters += 1;
+              if (bs.fire_tol >= 0.0 && bs.sums[S_FMAX2] <= bs.fire_tol * bs.fire_tol) bs.converged = 1;
+            }
+            bs.done_ctr = 0;
+          }
+        }
+      }
+    }
     if (is_last_block(st)) {
-      if (s.accumulate) reduce_partials(s.partials, gridDim.x, st->sums);
+      if (!BATCH && s.accumulate) reduce_partials(s.partials, gridDim.x, st->sums);
       __syncthreads();
       if (t == 0) {
         __threadfence();
-        if (s.accumulate && st->sums[S_NONFINITE] != 0.0) {
+        if (!BATCH && s.accumulate && st->sums[S_NONFINITE] != 0.0) {
           st->nonfinite = 1;
           st->abort = 1;
         }
-        if (s.kind == KIND_FIRE) {
+        if (!BATCH && s.kind == KIND_FIRE) {
           st->fire_iters += 1;
           if (s.fire_tol >= 0.0 && st->sums[S_FMAX2] <= s.fire_tol * s.fire_tol) st->converged = 1;
         }
