@@ -303,6 +303,87 @@ int cr_neighbor_list_noalloc(const double* pos, const double* rad, const int* ri
                              const double* boxSize, double maxRad, double cutDistance, long capacity,
                              int* neighbors, int* counts, long* maxCount, void* stream);
 
+/* ---- batches of independent systems -------------------------------------
+ * No single reference counterpart: the reference holds one system per process
+ * (its parameters live in __constant__ symbols, include/cudaKernel.cuh:17-67)
+ * and its drivers loop over packings one at a time (compressFIRE.cpp).  A
+ * batch holds S systems of deformable rings with their own boxes, ring counts
+ * and packing fractions in concatenated arrays (system s's rings and
+ * vertices follow system s-1's, in the order of numParticles[] and
+ * numVertexInParticleList[]), and runs every op as one launch over all of
+ * them; each system keeps its own neighbour list, FIRE scalars, convergence
+ * and rebuild flags.  Energy costs, potential and interaction are shared.
+ * Arrays are in the single-system layout, concatenated over systems. */
+typedef struct cr_batch cr_batch;
+int cr_batch_create(long numSystems, const long* numParticles, const long* numVertexInParticleList, cr_batch** out);
+int cr_batch_destroy(cr_batch* b);
+const char* cr_batch_last_error(const cr_batch* b);
+int cr_batch_get_sizes(const cr_batch* b, long* numSystems, long* numParticles, long* numVertices);
+int cr_batch_set_potential_type(cr_batch* b, int potential);
+int cr_batch_set_interaction_type(cr_batch* b, int interaction);
+int cr_batch_set_energy_costs(cr_batch* b, double ea, double el, double eb, double ec);
+int cr_batch_set_lj_cutoff(cr_batch* b, double LJcutoff);
+int cr_batch_set_attraction_constants(cr_batch* b, double l1, double l2);
+int cr_batch_set_precision(cr_batch* b, int precision);
+/* lanes per vertex of the batched tile kernel: 1, 2 or 4 */
+int cr_batch_set_lanes(cr_batch* b, int lanes);
+int cr_batch_get_lanes(const cr_batch* b, int* lanes);
+/* times the batched FIRE force kernel for each admissible lane count and keeps the fastest */
+int cr_batch_autotune(cr_batch* b, long reps, int* lanes_out);
+int cr_batch_profile_fire_tile(cr_batch* b, long reps, double* ms_per_launch);
+/* boxSizes[2 S] = {Lx_0, Ly_0, Lx_1, ...} */
+int cr_batch_set_box_sizes(cr_batch* b, const double* boxSizes);
+int cr_batch_get_box_sizes(const cr_batch* b, double* boxSizes);
+int cr_batch_set_vertex_positions(cr_batch* b, const double* pos);
+int cr_batch_get_vertex_positions(cr_batch* b, double* pos);
+int cr_batch_set_vertex_velocities(cr_batch* b, const double* vel);
+int cr_batch_get_vertex_velocities(cr_batch* b, double* vel);
+int cr_batch_get_vertex_forces(cr_batch* b, double* force);
+int cr_batch_get_vertex_energies(cr_batch* b, double* energy);
+int cr_batch_set_vertex_radii(cr_batch* b, const double* rad);
+int cr_batch_get_vertex_radii(cr_batch* b, double* rad);
+int cr_batch_set_rest_areas(cr_batch* b, const double* a0);
+int cr_batch_get_rest_areas(cr_batch* b, double* a0);
+int cr_batch_set_rest_lengths(cr_batch* b, const double* l0);
+int cr_batch_get_rest_lengths(cr_batch* b, double* l0);
+int cr_batch_set_rest_angles(cr_batch* b, const double* theta0);
+/* DPM2D::setDisplacementCutoff per system with size_ = 2 <r> of that system;
+ * returns the shared cutDistance */
+int cr_batch_set_displacement_cutoff(cr_batch* b, double cutoff_, double* cutDistance);
+int cr_batch_calc_neighbor_lists(cr_batch* b);
+int cr_batch_calc_force_energy(cr_batch* b);
+/* per-system results, arrays of S */
+int cr_batch_get_potential_energies(cr_batch* b, double* U);
+int cr_batch_get_max_unbalanced_forces(cr_batch* b, double* maxF);
+int cr_batch_get_phis(cr_batch* b, double* phi);
+int cr_batch_get_preferred_phis(cr_batch* b, double* phi);
+int cr_batch_get_mean_particle_sizes(cr_batch* b, double* sigma);
+/* 1: the system takes part in the batch's ops, 0: it is frozen */
+int cr_batch_set_active(cr_batch* b, const int* active);
+/* DPM2D::initFIRE for every system; dt (nullable) gives per-system time
+ * steps, dt_max scaled with them */
+int cr_batch_init_fire(cr_batch* b, const double* FIREparams7, const double* dt, long minStep);
+/* FIRE iterations until max |F_i,d| <= tol[s] in every system or maxIter */
+int cr_batch_fire_minimize(cr_batch* b, const double* tol, long maxIter, long* iterations, double* maxForce);
+/* DPM2D::scaleVertices with one factor per system */
+int cr_batch_scale_vertices(cr_batch* b, const double* scale);
+/* Quasi-static compression to jamming (compressFIRE.cpp:101-205) of every
+ * system.  state[s]: 1 jammed, 2 step limit, 3 compression step halved below
+ * min_dphi (phi within min_dphi of jamming). */
+typedef struct cr_compress_params {
+  double dphi;          /* starting packing-fraction step */
+  double min_dphi;      /* stop a system once its halved step falls below this */
+  double fire_dt;       /* FIRE time step in units of the mean particle size */
+  double tol0;          /* force tolerance times the mean particle size */
+  double energy_tol;    /* criterion 1: potential energy per ring threshold */
+  long max_fire_iters;  /* FIRE iterations per compression step */
+  long max_steps;       /* compression steps */
+  int criterion;        /* 0: maximum force (the reference's), 1: energy */
+} cr_compress_params;
+int cr_batch_compress(cr_batch* b, const cr_compress_params* params, double* phi, long* steps, int* state,
+                      long* fireIterations);
+int cr_batch_get_launch_count(const cr_batch* b, long long* out);
+
 #ifdef __cplusplus
 }
 #endif

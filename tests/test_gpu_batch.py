@@ -1,0 +1,147 @@
+"""Batches of independent systems (cr_batch_*) against the single-system
+path of the same library, system by system.
+
+Forces: every system of a batch evaluates the same tiles with the same
+arithmetic as its own context, so forces and energies agree to FP64 rounding
+(1e-12 of the largest component).  FIRE: the per-system iteration matches
+the single-system one; the runs start from sums reduced in a different
+order, so trajectories agree to the minimiser's tolerance.  Compression:
+the batched protocol reaches the same packing fractions as the per-system
+loop (cudaring_b200.compress.compress_system).
+"""
+import numpy as np
+import pytest
+
+from cudaring_b200 import DPM2D, synth
+from cudaring_b200.batch import Batch
+from cudaring_b200.compress import batch_packings, compress_system
+
+from conftest import rel_inf
+
+pytestmark = pytest.mark.gpu
+
+
+def _systems(cfg, sizes, phi, seed, placement="rsa", rad_scale=1.0):
+    out = []
+    for k, n in enumerate(sizes):
+        c = synth.workload_config(cfg, n)
+        pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=seed + k, placement=placement)
+        pk.rad = pk.rad * rad_scale
+        out.append(pk)
+    return out
+
+
+def _single(pk, **kw):
+    d = DPM2D.from_packing(pk, **kw)
+    d.calcNeighborList(d.setDisplacementCutoff(0.5, 2.0 * d.getMeanVertexRadius()))
+    d.resetLastPositions()
+    d.calcForceEnergy()
+    return d
+
+
+@pytest.mark.parametrize("potential,interaction,cfg,rad_scale", [
+    ("harmonic", "vertexVertex", 0, 1.5), ("lennardJones", "vertexSmooth", 1, 1.0), ("wca", "vertexSmooth", 1, 1.3)])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_forces_match_single(cuda_device, potential, interaction, cfg, rad_scale, precision):
+    pks = _systems(cfg, [8, 24, 40, 16, 64], 0.40, seed=101, rad_scale=rad_scale)
+    kw = dict(potential=potential, interaction=interaction, ea=1.0, el=1.0, eb=0.01, ec=1.0, LJcutoff=2.5)
+    b = Batch.from_packings(pks, **kw)
+    b.setPrecision(precision)
+    b.setLanes(2)  # the single-system default here; FP32 sums follow the lane split
+    b.setDisplacementCutoff(0.5)
+    b.calcNeighborLists()
+    b.calcForceEnergy()
+    f = b.getVertexForces()
+    u = b.getPotentialEnergies()
+    assert np.all(np.isfinite(f))
+    for s, pk in enumerate(pks):
+        d = _single(pk, **kw)
+        d.setLanes(2)
+        d.setPrecision(precision)
+        d.calcForceEnergy()
+        fs = d.getVertexForces()
+        assert np.abs(fs).max() > 0
+        assert rel_inf(f[b.system_slice(s)], fs) < 1e-12
+        assert u[s] == pytest.approx(d.getPotentialEnergy(), rel=1e-12)
+        d.close()
+    phi = b.getPhis()
+    for s, pk in enumerate(pks):
+        d = _single(pk, **kw)
+        assert phi[s] == pytest.approx(d.getPhi(), rel=1e-13)
+        d.close()
+
+
+def test_batch_fire_matches_single(cuda_device):
+    pks = _systems(0, [16, 32, 20], 0.70, seed=7, placement="uniform")
+    kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
+    b = Batch.from_packings(pks, **kw)
+    b.setDisplacementCutoff(0.5)
+    sig = b.getMeanParticleSizes()
+    dt = 1e-2 * sig
+    b.initFIRE([0.2, 0.5, 1.1, 0.99, 1e-2, 1e-1, 0.2], 20, dt=dt)
+    tol = 1e-10 / sig
+    its, fmax = b.fireMinimize(tol, 20000)
+    pos = b.getVertexPositions()
+    for s, pk in enumerate(pks):
+        assert fmax[s] <= tol[s]
+        d = _single(pk, **kw)
+        d.initFIRE([0.2, 0.5, 1.1, 0.99, dt[s], 10 * dt[s], 0.2], 20, 0, d.numVertices)
+        it1, f1 = d.minimizeFIRE(tol[s], 20000)
+        assert f1 <= tol[s]
+        assert abs(its[s] - it1) <= max(20, 0.05 * it1)
+        assert rel_inf(pos[b.system_slice(s)], d.getVertexPositions()) < 1e-6
+        d.close()
+
+
+def test_batch_scale_matches_single(cuda_device):
+    pks = _systems(0, [16, 24], 0.40, seed=3)
+    kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
+    b = Batch.from_packings(pks, **kw)
+    b.setDisplacementCutoff(0.5)
+    b.calcNeighborLists()
+    b.scaleVertices(np.array([1.01, 0.99]))
+    b.calcForceEnergy()
+    pos, phi = b.getVertexPositions(), b.getPhis()
+    for s, (pk, f) in enumerate(zip(pks, (1.01, 0.99))):
+        d = _single(pk, **kw)
+        d.scaleVertices(f)
+        d.calcForceEnergy()
+        assert rel_inf(pos[b.system_slice(s)], d.getVertexPositions()) < 1e-14
+        assert phi[s] == pytest.approx(d.getPhi(), rel=1e-13)
+        d.close()
+
+
+def test_batch_compress_matches_per_system_loop(cuda_device):
+    pks = batch_packings(3, seed=5, rings=(16, 40))
+    kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
+    prm = dict(dphi=2e-2, min_dphi=1e-3, fire_dt=1e-2, tol0=1e-6, max_fire_iters=50000, max_steps=5)
+    b = Batch.from_packings(pks, **kw)
+    b.setDisplacementCutoff(0.5)
+    res = b.compress(**prm)
+    assert np.all(res["steps"] >= 1)
+    for s, pk in enumerate(pks):
+        d = DPM2D.from_packing(pk, **kw)
+        d.calcNeighborList(d.setDisplacementCutoff(0.5, 2.0 * d.getMeanVertexRadius()))
+        one = compress_system(d, **prm)
+        assert one["steps"] == res["steps"][s]
+        assert one["state"] == res["state"][s]
+        # FIRE stops at max |F| <= tol0 / sigma: the two runs' end points (and
+        # so the areas behind phi) agree to the residual force, not to rounding
+        assert one["phi"] == pytest.approx(res["phi"][s], rel=1e-6)
+        d.close()
+
+
+def test_batch_autotune_and_lanes(cuda_device):
+    pks = _systems(1, [16, 32], 0.40, seed=9)
+    kw = dict(potential="lennardJones", interaction="vertexSmooth", ea=1.0, el=1.0, eb=0.01, ec=1.0, LJcutoff=2.5)
+    b = Batch.from_packings(pks, **kw)
+    b.setDisplacementCutoff(0.5)
+    b.calcNeighborLists()
+    b.calcForceEnergy()
+    f1 = b.getVertexForces()
+    lanes = b.autotune(5)
+    assert lanes in (1, 2, 4)
+    for L in (1, 2, 4):
+        b.setLanes(L)
+        b.calcForceEnergy()
+        assert rel_inf(b.getVertexForces(), f1) < 1e-12
