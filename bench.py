@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--md-steps", type=int, default=1000)
     ap.add_argument("--rings", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched-systems FIRE / compression measurement")
+    ap.add_argument("--batch-systems", type=int, default=256)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--save-state", default=None, help="write the prepared state (npz) after preparation")
     ap.add_argument("--load-state", default=None, help="start from a state written by --save-state")
@@ -316,6 +319,7 @@ def main():
             d.NVELoop(M)
             l2_flush()
         torch.cuda.synchronize()
+        x_warm = d.getVertexPositions()
         upd0, launches0, e0 = d.getUpdateCount(), d.getLaunchCount(), d.getEnergy()
         barrier(world)
         torch.cuda.synchronize()
@@ -332,7 +336,7 @@ def main():
         return {"ms_total": ms_total, "value": nv * M * args.steps * world / (ms_total / 1e3),
                 "launches": d.getLaunchCount() - launches0, "updates": d.getUpdateCount() - upd0,
                 "energy_change_rel": abs(d.getEnergy() - e0) / abs(e0) if e0 else None,
-                "clocks": clocks.summary()}
+                "clocks": clocks.summary(), "x_warm": x_warm}
 
     def kernel_roofline(precision):
         d.setPrecision(precision)
@@ -393,7 +397,11 @@ def main():
         fp64_value = orun["value"] if prim == "mixed" else value
         mixed_value = value if prim == "mixed" else orun["value"]
         comparison["mixed_over_fp64"] = mixed_value / fp64_value
-        comparison["accuracy"] = precision_accuracy(d, cut, [x0, x_end], v0, args.drift_steps, restart)
+        comparison["accuracy"] = precision_accuracy(d, cut, [run["x_warm"], x_end], v0, args.drift_steps, restart)
+
+    batch = None
+    if rank == 0 and not args.no_batch:
+        batch = batched_fire_measurement(args.batch_systems)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -416,7 +424,7 @@ def main():
                        "prep_seconds": t_prep, "fire_iterations_prep": info["fire_iterations"],
                        "lanes_per_vertex": info["lanes"]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": run["launches"],
-            "clocks": run["clocks"], "precision_comparison": comparison,
+            "clocks": run["clocks"], "precision_comparison": comparison, "batched_systems": batch,
         }
         print(json.dumps(line), flush=True)
     d.close()
@@ -424,6 +432,87 @@ def main():
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def batched_fire_measurement(num_systems: int, fire_iters: int = 2000, loop_systems: int = 8) -> dict:
+    """Many independent systems in one launch per op (cr_batch_*): the FIRE
+    throughput of the batch against the per-system single-context loop on the
+    same states, plus a bounded sample of the compression protocol.
+
+    Workload: ``num_systems`` deformable-ring packings, ring counts uniform in
+    [16, 512], bidisperse 1:1.4 with nv 16/22, calA0 uniform in [1.0, 1.2],
+    harmonic repulsion, brought to packing fraction 0.60 (untimed).  Timed:
+    FIRE to max |F| <= 1e-10 / sigma (at most ``fire_iters`` iterations) on
+    every system, as vertex-iterations per second; the per-system loop runs
+    the same minimisation on ``loop_systems`` of them one at a time."""
+    import torch
+
+    from cudaring_b200 import DPM2D
+    from cudaring_b200.batch import Batch
+    from cudaring_b200.compress import batch_packings, prepare_batch
+
+    t0 = time.perf_counter()
+    pks = batch_packings(num_systems, seed=20261207)
+    kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
+    b = Batch.from_packings(pks, **kw)
+    prepare_batch(b, 0.60, step=0.03, tol0=1e-6, max_fire_iters=5000)
+    lanes = b.autotune(10)
+    t_prep = time.perf_counter() - t0
+    nvs = np.array([p.num_vertices for p in pks])
+    pos, rad, l0, a0 = b.getVertexPositions(), b.getVertexRadii(), b.getRestLengths(), b.getRestAreas()
+    out = {"workload": f"{num_systems} systems, {int(nvs.sum())} vertices, rings U[16,512] nv 16/22, harmonic, "
+                       f"phi 0.60, FIRE to 1e-10/sigma (<= {fire_iters} iterations)",
+           "unit": "vertex-iterations/s", "lanes_per_vertex": lanes, "prep_seconds": t_prep}
+    for prec in ("fp64", "mixed"):
+        b.setVertexPositions(pos)
+        b.setVertexVelocities(np.zeros_like(pos))
+        b.setPrecision(prec)
+        sig = b.getMeanParticleSizes()
+        b.initFIRE([0.2, 0.5, 1.1, 0.99, 1e-2, 1e-1, 0.2], 20, dt=1e-2 * sig)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        its, fmax = b.fireMinimize(1e-10 / sig, fire_iters)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[prec] = {"value": float((its * nvs).sum()) / dt, "seconds": dt, "iterations_mean": float(its.mean()),
+                     "converged_systems": int((fmax <= 1e-10 / sig).sum())}
+    # the per-system loop: the same minimisation through single contexts
+    vi, tt = 0.0, 0.0
+    for s in range(min(loop_systems, num_systems)):
+        pk = pks[s]
+        pk.pos = pos[b.system_slice(s)].copy()
+        pk.rad = rad[b.system_slice(s, dim=1)].copy()
+        pk.l0 = l0[b.system_slice(s, dim=1)].copy()
+        pk.a0 = a0[b.system_slice(s, per="ring", dim=1)].copy()
+        pk.vel = np.zeros_like(pk.pos)
+        d = DPM2D.from_packing(pk, **kw)
+        d.calcNeighborList(d.setDisplacementCutoff(0.5, 2 * d.getMeanVertexRadius()))
+        d.calcForceEnergy()
+        sg = d.getMeanParticleSize()
+        d.initFIRE([0.2, 0.5, 1.1, 0.99, 1e-2 * sg, 1e-1 * sg, 0.2], 20, 0, d.numVertices)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        it, _ = d.minimizeFIRE(1e-10 / sg, fire_iters)
+        torch.cuda.synchronize()
+        tt += time.perf_counter() - t0
+        vi += it * d.numVertices
+        d.close()
+    out["per_system_loop_fp64"] = {"value": vi / tt, "systems": min(loop_systems, num_systems),
+                                   "sample": "the first systems of the batch, one single-system context each"}
+    out["batch_over_loop_fp64"] = out["fp64"]["value"] / out["per_system_loop_fp64"]["value"]
+    # compression protocol sample (compressFIRE.cpp:101-205) from phi 0.60
+    b.setVertexPositions(pos)
+    b.setVertexVelocities(np.zeros_like(pos))
+    b.setPrecision("fp64")
+    t0 = time.perf_counter()
+    res = b.compress(dphi=1e-3, min_dphi=1e-6, fire_dt=1e-2, tol0=1e-10, max_fire_iters=20000, max_steps=3)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    out["compression_sample"] = {"steps": 3, "dphi": 1e-3, "seconds": dt,
+                                 "value": float((res["fire_iterations"] * nvs).sum()) / dt,
+                                 "phi_mean": float(res["phi"].mean())}
+    b.close()
+    return out
 
 
 def precision_accuracy(d, cut, states, v0, drift_steps, restart) -> dict:
@@ -458,7 +547,7 @@ def precision_accuracy(d, cut, states, v0, drift_steps, restart) -> dict:
         drift[prec] = {"max_rel": float(np.abs(es - e0).max() / abs(e0)), "slope_rel_per_step": slope}
     drift["mixed_over_fp64_max_rel"] = drift["mixed"]["max_rel"] / drift["fp64"]["max_rel"]
     return {"force_err_l2_rel": errs, "force_err_max_abs": maxabs, "potential_energy_rel_err": eerr,
-            "states": "thermal start state and the end of the timed run", "energy_drift": drift}
+            "states": "thermal states: the start and the end of the timed run", "energy_drift": drift}
 
 
 def run_reference_arm(args, world, rank):

@@ -93,6 +93,11 @@ struct cr_ctx {
   double2* cell_pos = nullptr;
   double* cell_rad = nullptr;
   double* partials = nullptr;
+  // derivative evaluations (cr_hvp, cr_calc_pressure, cr_param_derivatives)
+  double* diff_f = nullptr;   // [nv][8]
+  double* diff_e = nullptr;   // [nv][4]
+  double* diff_dot = nullptr; // [256] dot-product partials
+  double* diff_vec = nullptr; // [5][2 nv] CG vectors
   int partials_n = 0;
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
@@ -807,6 +812,7 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->tiles, ctx->nbr, ctx->nbr_cnt, ctx->cell_of, ctx->slot,
                   ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
                   ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
+                  ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec,
                   ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle};
   for (void* p : ptrs)
     if (p) cudaFree(p);
@@ -1711,6 +1717,201 @@ int cr_set_use_graphs(cr_ctx* ctx, int on) {
   ctx->use_graphs = on != 0;
   drop_graphs(ctx);
   return CR_OK;
+}
+
+// ---------------------------------------------------------------- derivatives
+
+static int diff_ready(cr_ctx* ctx) {
+  if (ctx->shape == CR_SHAPE_RIGID) return ctx->fail(CR_ENOTSUP, "derivatives are for deformable rings");
+  if (inter_kind(ctx) != INT_VV) return ctx->fail(CR_ENOTSUP, "derivatives cover the vertex-vertex interaction");
+  if (ctx->monomer != CR_MONOMER_HARMONIC) return ctx->fail(CR_ENOTSUP, "derivatives cover harmonic monomers");
+  int rc;
+  if (!ctx->nbr_built && (rc = build_list(ctx, ctx->cur, ctx->cut_distance))) return rc;
+  if (!ctx->diff_f) {
+    if ((rc = dalloc(ctx, &ctx->diff_f, (size_t)8 * ctx->nv)) || (rc = dalloc(ctx, &ctx->diff_e, (size_t)4 * ctx->nv)) ||
+        (rc = dalloc(ctx, &ctx->diff_dot, 256)) || (rc = dalloc(ctx, &ctx->diff_vec, (size_t)10 * ctx->nv)))
+      return rc;
+  }
+  return CR_OK;
+}
+
+static DiffArgs diff_args(cr_ctx* ctx) {
+  DiffArgs g;
+  memset(&g, 0, sizeof(g));
+  g.p = ctx->p;
+  g.pos = ctx->pos[ctx->cur];
+  g.rad = ctx->rad;
+  g.l0 = ctx->l0;
+  g.theta0 = ctx->theta0;
+  g.a0 = ctx->a0;
+  g.vtopo = ctx->vtopo;
+  g.nbr = ctx->nbr;
+  g.nbr_cnt = ctx->nbr_cnt;
+  g.nbr_cap = ctx->cap;
+  g.force_out = ctx->diff_f;
+  g.energy_out = ctx->diff_e;
+  return g;
+}
+
+static int diff_launch(cr_ctx* ctx, const DiffArgs& g) {
+  launch_diff(ctx->stream, ctx->potential, g);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  return CR_OK;
+}
+
+// host sums of the hyper-dual energy parts, in vertex order
+static int diff_energy(cr_ctx* ctx, double out[4]) {
+  std::vector<double> e((size_t)4 * ctx->nv);
+  int rc = download(ctx, e.data(), ctx->diff_e, e.size() * sizeof(double));
+  if (rc) return rc;
+  for (int q = 0; q < 4; q++) out[q] = 0.0;
+  for (int v = 0; v < ctx->nv; v++)
+    for (int q = 0; q < 4; q++) out[q] += e[(size_t)4 * v + q];
+  return CR_OK;
+}
+
+static int dev_dot(cr_ctx* ctx, const double* a, const double* b, int n, double* out) {
+  const int nb = std::min(256, std::max(1, (n + 255) / 256));
+  launch_dot_partials(ctx->stream, n, a, b, ctx->diff_dot, nb);
+  ctx->launches++;
+  double part[256];
+  int rc = download(ctx, part, ctx->diff_dot, nb * sizeof(double));
+  if (rc) return rc;
+  double s = 0.0;
+  for (int i = 0; i < nb; i++) s += part[i];
+  *out = s;
+  return CR_OK;
+}
+
+static int dev_project(cr_ctx* ctx, double* x) {
+  std::vector<double> h((size_t)2 * ctx->nv);
+  int rc = download(ctx, h.data(), x, h.size() * sizeof(double));
+  if (rc) return rc;
+  double mx = 0.0, my = 0.0;
+  for (int v = 0; v < ctx->nv; v++) {
+    mx += h[2 * v];
+    my += h[2 * v + 1];
+  }
+  launch_sub_mean(ctx->stream, ctx->nv, x, mx / ctx->nv, my / ctx->nv);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  return CR_OK;
+}
+
+extern "C" int cr_hvp_device(cr_ctx* ctx, const double* v_dev, double* hv_dev) {
+  if (!ctx || !v_dev || !hv_dev) return CR_EINVAL;
+  int rc;
+  if ((rc = diff_ready(ctx))) return rc;
+  DiffArgs g = diff_args(ctx);
+  g.t1 = reinterpret_cast<const double2*>(v_dev);
+  if ((rc = diff_launch(ctx, g))) return rc;
+  launch_extract_hv(ctx->stream, ctx->nv, ctx->diff_f, hv_dev);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+extern "C" int cr_hvp(cr_ctx* ctx, const double* v, double* hv) {
+  if (!ctx || !v || !hv) return CR_EINVAL;
+  int rc;
+  if ((rc = diff_ready(ctx))) return rc;
+  double* vd = ctx->diff_vec;
+  double* hd_ = ctx->diff_vec + (size_t)2 * ctx->nv;
+  if ((rc = upload(ctx, vd, v, (size_t)2 * ctx->nv * sizeof(double)))) return rc;
+  if ((rc = cr_hvp_device(ctx, vd, hd_))) return rc;
+  return download(ctx, hv, hd_, (size_t)2 * ctx->nv * sizeof(double));
+}
+
+extern "C" int cr_calc_pressure(cr_ctx* ctx, double* P) {
+  if (!ctx || !P) return CR_EINVAL;
+  int rc;
+  if ((rc = diff_ready(ctx))) return rc;
+  DiffArgs g = diff_args(ctx);
+  g.t1 = ctx->pos[ctx->cur];  // affine dilation: x -> (1 + e) x, L -> (1 + e) L
+  g.s1 = 1.0;
+  if ((rc = diff_launch(ctx, g))) return rc;
+  double e[4];
+  if ((rc = diff_energy(ctx, e))) return rc;
+  *P = -e[1] / (2.0 * ctx->p.lx * ctx->p.ly);
+  return CR_OK;
+}
+
+extern "C" int cr_param_derivatives(cr_ctx* ctx, int param, double* dU, double* dP, double* dF, double* dPdx) {
+  if (!ctx || param < 0 || param > 3) return CR_EINVAL;
+  int rc;
+  if ((rc = diff_ready(ctx))) return rc;
+  DiffArgs g = diff_args(ctx);
+  g.t1 = ctx->pos[ctx->cur];
+  g.s1 = 1.0;
+  if (param < 3) g.pe2[param] = 1.0;
+  else g.c2 = 1.0;
+  if ((rc = diff_launch(ctx, g))) return rc;
+  double e[4];
+  if ((rc = diff_energy(ctx, e))) return rc;
+  const double A2 = 2.0 * ctx->p.lx * ctx->p.ly;
+  if (dU) *dU = e[2];
+  if (dP) *dP = -e[3] / A2;
+  if (dF || dPdx) {
+    std::vector<double> f((size_t)8 * ctx->nv);
+    if ((rc = download(ctx, f.data(), ctx->diff_f, f.size() * sizeof(double)))) return rc;
+    for (int v = 0; v < ctx->nv; v++) {
+      const double* q = &f[(size_t)8 * v];
+      if (dF) {
+        dF[2 * v] = q[2];
+        dF[2 * v + 1] = q[6];
+      }
+      if (dPdx) {
+        dPdx[2 * v] = (q[0] + q[1]) / A2;
+        dPdx[2 * v + 1] = (q[4] + q[5]) / A2;
+      }
+    }
+  }
+  return CR_OK;
+}
+
+extern "C" int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double tol, long maxIter, long* iters,
+                                double* relres) {
+  if (!ctx || !b || !x || maxIter < 0) return CR_EINVAL;
+  int rc;
+  if ((rc = diff_ready(ctx))) return rc;
+  const int n = 2 * ctx->nv;
+  double* xd = ctx->diff_vec;
+  double* r = xd + n;
+  double* pv = r + n;
+  double* hp = pv + n;
+  // conjugate gradients on the Hessian restricted to vectors without a
+  // uniform translation (its null space in a periodic box): b and every
+  // iterate are projected
+  if ((rc = upload(ctx, r, b, (size_t)n * sizeof(double)))) return rc;
+  if ((rc = dev_project(ctx, r))) return rc;
+  CR_TRY(cudaMemsetAsync(xd, 0, (size_t)n * sizeof(double), ctx->stream));
+  CR_TRY(cudaMemcpyAsync(pv, r, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  double rr, bb;
+  if ((rc = dev_dot(ctx, r, r, n, &rr))) return rc;
+  bb = rr;
+  long it = 0;
+  while (it < maxIter && bb > 0.0 && std::sqrt(rr / bb) > tol) {
+    if ((rc = cr_hvp_device(ctx, pv, hp))) return rc;
+    if ((rc = dev_project(ctx, hp))) return rc;
+    double pHp;
+    if ((rc = dev_dot(ctx, pv, hp, n, &pHp))) return rc;
+    if (!(pHp > 0.0)) return ctx->fail(CR_ENONFINITE, "Hessian not positive along a CG direction");
+    const double alpha = rr / pHp;
+    launch_axpby(ctx->stream, n, alpha, pv, 1.0, xd);
+    launch_axpby(ctx->stream, n, -alpha, hp, 1.0, r);
+    double rr2;
+    if ((rc = dev_dot(ctx, r, r, n, &rr2))) return rc;
+    launch_axpby(ctx->stream, n, 1.0, r, rr2 / rr, pv);
+    ctx->launches += 3;
+    rr = rr2;
+    it++;
+  }
+  CR_TRY(cudaGetLastError());
+  if (iters) *iters = it;
+  if (relres) *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+  return download(ctx, x, xd, (size_t)n * sizeof(double));
 }
 
 int cr_get_launch_count(const cr_ctx* ctx, long long* out) {

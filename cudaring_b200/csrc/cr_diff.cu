@@ -1,0 +1,246 @@
+// Forces and energies in hyper-dual arithmetic: the derivative kernel behind
+// the Hessian-vector product, the virial pressure and the parameter
+// derivatives (cr_hvp, cr_calc_pressure, cr_param_derivatives).
+//
+// One thread per vertex evaluates the same per-vertex force and energy as the
+// fused kernel (shape terms of kernelCalcShapeForceEnergy,
+// include/cudaKernel.cuh:474-529, harmonic monomers, and the vertex-vertex
+// pair terms of kernelCalcVertexInteraction, :690-722) with every input a
+// hyper-dual number: positions x + t1 e1 + t2 e2, box L (1 + s1 e1 + s2 e2),
+// and the shape constants and rest lengths / radii along parameter tangents.
+// The e1 part of the force is then D_t1 F = -H t1 (the Hessian-vector
+// product), the e1 part of the energy along the affine dilation t1 = x,
+// s1 = 1 is dU/dlambda = -2 A P, and the e1 e2 parts give the mixed
+// derivatives that the adjoint gradients need.  The ring's area is summed by
+// each of its threads (O(nv) per vertex): this kernel serves small systems
+// and iterative solves, not the time-stepping hot path.
+#include "cr_hd.cuh"
+#include "cr_launch.h"
+#include "cr_tile.cuh"
+
+namespace cr {
+namespace {
+
+struct HBox {
+  HD lx, ly;
+};
+
+__device__ __forceinline__ HD pbc_hd(HD d, const HD& L) {
+  const double k = round(d.a / L.a);
+  return d - k * L;
+}
+
+__device__ __forceinline__ HD2 pbc2_hd(const HD2& a, const HD2& b, const HBox& bx) {
+  return HD2{pbc_hd(a.x - b.x, bx.lx), pbc_hd(a.y - b.y, bx.ly)};
+}
+
+__device__ __forceinline__ HD2 load_x(const DiffArgs& g, int i) {
+  const double2 x = g.pos[i];
+  double2 u1 = make_double2(0.0, 0.0), u2 = make_double2(0.0, 0.0);
+  if (g.t1) u1 = g.t1[i];
+  if (g.t2) u2 = g.t2[i];
+  return HD2{HD{x.x, u1.x, u2.x, 0.0}, HD{x.y, u1.y, u2.y, 0.0}};
+}
+
+// l0 and rad scale as sqrt(calA0) (the reference's conventions: l0 from the
+// preferred perimeter, rad = l0 / 2); along ln(calA0) a length w takes
+// w (1 + c1/2 e1 + c2/2 e2 - c1 c2 / 4 e1 e2).
+__device__ __forceinline__ HD scaled_length(const DiffArgs& g, double w) {
+  return HD{w, 0.5 * g.c1 * w, 0.5 * g.c2 * w, -0.25 * g.c1 * g.c2 * w};
+}
+
+template <int POT>
+__device__ __forceinline__ bool pair_hd(const DiffArgs& g, HD d, HD rsum, HD& gm, HD& ep) {
+  const SysParams& p = g.p;
+  const double ec = p.ec;
+  if constexpr (POT == POT_HARMONIC) {
+    const HD ov = 1.0 - d / rsum;
+    if (!(ov.a > 0.0)) return false;
+    gm = ec * ov / rsum;
+    ep = (0.25 * ec) * ov * ov;
+    return true;
+  } else if constexpr (POT == POT_LJ) {
+    if (!(d.a <= p.lj_cutoff * rsum.a)) return false;
+    const HD ratio = rsum / d;
+    const HD r2 = ratio * ratio;
+    const HD r6 = r2 * r2 * r2;
+    const HD r12 = r6 * r6;
+    const HD fshift = p.lj_fshift / rsum;
+    gm = (24.0 * ec) * (2.0 * r12 - r6) / d - fshift;
+    ep = 0.5 * ((4.0 * ec) * (r12 - r6) - p.lj_ecut - habs(fshift) * (d - p.lj_cutoff * rsum));
+    return true;
+  } else if constexpr (POT == POT_ADHESIVE) {
+    if (!(d.a < (1.0 + p.l2) * rsum.a)) return false;
+    const HD ov = 1.0 - d / rsum;
+    if (d.a < (1.0 + p.l1) * rsum.a) {
+      gm = ec * ov / rsum;
+      ep = (0.25 * ec) * (ov * ov - p.l1 * p.l2);
+    } else {
+      const double k = ec * p.l1 / (p.l2 - p.l1);
+      gm = -k * (ov + p.l2) / rsum;
+      ep = (-0.25 * k) * (ov + p.l2) * (ov + p.l2);
+    }
+    return true;
+  } else {
+    if (!(d.a <= kWCAcut * rsum.a)) return false;
+    const HD ratio = rsum / d;
+    const HD r2 = ratio * ratio;
+    const HD r6 = r2 * r2 * r2;
+    const HD r12 = r6 * r6;
+    gm = (24.0 * ec) * (2.0 * r12 - r6) / d;
+    ep = (0.5 * ec) * (4.0 * (r12 - r6) + 1.0);
+    return true;
+  }
+}
+
+__device__ __forceinline__ HD cross(const HD2& a, const HD2& b) { return a.x * b.y - b.x * a.y; }
+__device__ __forceinline__ HD dot(const HD2& a, const HD2& b) { return a.x * b.x + a.y * b.y; }
+__device__ __forceinline__ HD norm(const HD2& a) { return hsqrt(dot(a, a)); }
+// calcAngle(nextSegment, previousSegment) (include/cudaKernel.cuh:423-427)
+__device__ __forceinline__ HD angle(const HD2& ns, const HD2& ps) { return hatan2(cross(ns, ps), dot(ns, ps)); }
+
+template <int POT>
+__global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= g.p.nv) return;
+  const SysParams& p = g.p;
+  const HBox bx{HD{p.lx, p.lx * g.s1, p.lx * g.s2, 0.0}, HD{p.ly, p.ly * g.s1, p.ly * g.s2, 0.0}};
+  const HD ea{p.ea, g.pe1[0], g.pe2[0], 0.0}, el{p.el, g.pe1[1], g.pe2[1], 0.0}, eb{p.eb, g.pe1[2], g.pe2[2], 0.0};
+  const int2 tp = g.vtopo[v];
+  const int ring = tp.x, k = tp.y & 0xffff, nvr = tp.y >> 16;
+  const int f = v - k;
+  auto at = [&](int kk) { return f + ((kk % nvr) + nvr) % nvr; };
+  const int vp = at(k - 1), vn = at(k + 1), vpp = at(k - 2), vnn = at(k + 2);
+
+  // ring area by the shoelace sum of offsets from the first vertex
+  const HD2 x0 = load_x(g, f);
+  HD sum = hd(0.0);
+  {
+    HD2 u = HD2{hd(0.0), hd(0.0)};
+    for (int q = 0; q < nvr; q++) {
+      const HD2 un = pbc2_hd(load_x(g, at(q + 1)), x0, bx);
+      sum += cross(u, un);
+      u = un;
+    }
+  }
+  const HD area = 0.5 * habs(sum);
+  const HD2 x = load_x(g, v), xn = load_x(g, vn), xp = load_x(g, vp);
+  const HD2 ns = pbc2_hd(xn, x, bx), ps = pbc2_hd(x, xp, bx);
+  const HD2 pps = pbc2_hd(xp, load_x(g, vpp), bx), nns = pbc2_hd(load_x(g, vnn), xn, bx);
+  const HD th = angle(ns, ps), thp = angle(ps, pps), thn = angle(nns, ns);
+
+  HD2 F{hd(0.0), hd(0.0)};
+  HD E = hd(0.0);
+  // area
+  const double a0 = g.a0[ring];
+  const HD dA = area / a0 - 1.0;
+  const HD gmA = ea * dA / a0;
+  const HD2 npd{ns.x + ps.x, ns.y + ps.y};
+  F.x += 0.5 * gmA * (-npd.y);
+  F.y += 0.5 * gmA * npd.x;
+  E += (0.5 * ea * dA * dA) / (double)nvr;
+  // segment lengths (harmonic monomers)
+  const HD plen = norm(ps), nlen = norm(ns);
+  const HD tl0 = scaled_length(g, g.l0[v]), pl0 = scaled_length(g, g.l0[vp]);
+  const HD pd = plen / pl0 - 1.0, nd = nlen / tl0 - 1.0;
+  F.x += el * (nd * ns.x / (tl0 * nlen) - pd * ps.x / (pl0 * plen));
+  F.y += el * (nd * ns.y / (tl0 * nlen) - pd * ps.y / (pl0 * plen));
+  E += 0.5 * el * pd * pd;
+  // bending
+  const HD prevAD = thp - g.theta0[vp], thisAD = th - g.theta0[v], nextAD = thn - g.theta0[vn];
+  const HD pvar = (thisAD - prevAD) / dot(ps, ps);
+  const HD nvar = (thisAD - nextAD) / dot(ns, ns);
+  F.x += eb * (pvar * ps.y + nvar * ns.y);
+  F.y += eb * (pvar * (-ps.x) + nvar * (-ns.x));
+  E += 0.5 * eb * thisAD * thisAD;
+
+  // vertex-vertex pairs
+  const HD ri = scaled_length(g, g.rad[v]);
+  const int cnt = min(g.nbr_cnt[v], g.nbr_cap);
+  for (int s = 0; s < cnt; s++) {
+    const int j = g.nbr[(size_t)s * p.nv + v];
+    const HD2 dl = pbc2_hd(x, load_x(g, j), bx);
+    const HD d = norm(dl);
+    const HD rsum = ri + scaled_length(g, g.rad[j]);
+    HD gm, ep;
+    if (pair_hd<POT>(g, d, rsum, gm, ep)) {
+      const HD s2 = gm / d;
+      F.x += s2 * dl.x;
+      F.y += s2 * dl.y;
+      E += ep;
+    }
+  }
+  double* fo = g.force_out + (size_t)v * 8;
+  fo[0] = F.x.a; fo[1] = F.x.b; fo[2] = F.x.c; fo[3] = F.x.d;
+  fo[4] = F.y.a; fo[5] = F.y.b; fo[6] = F.y.c; fo[7] = F.y.d;
+  double* eo = g.energy_out + (size_t)v * 4;
+  eo[0] = E.a; eo[1] = E.b; eo[2] = E.c; eo[3] = E.d;
+}
+
+}  // namespace
+
+void launch_diff(cudaStream_t st, int pot, const DiffArgs& g) {
+  const int nb = (g.p.nv + 127) / 128;
+  switch (pot) {
+    case POT_HARMONIC: k_diff<POT_HARMONIC><<<nb, 128, 0, st>>>(g); break;
+    case POT_LJ: k_diff<POT_LJ><<<nb, 128, 0, st>>>(g); break;
+    case POT_ADHESIVE: k_diff<POT_ADHESIVE><<<nb, 128, 0, st>>>(g); break;
+    default: k_diff<POT_WCA><<<nb, 128, 0, st>>>(g); break;
+  }
+}
+
+// Fixed-order dot products for the Hessian solves: one partial per CTA, the
+// host sums them in CTA order.
+__global__ void __launch_bounds__(256) k_dot_partials(int n, const double* a, const double* b, double* out) {
+  double acc = 0.0;
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) acc += a[i] * b[i];
+  __shared__ double s[8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double x = 0.0;
+    for (int w = 0; w < 8; w++) x += s[w];
+    out[blockIdx.x] = x;
+  }
+}
+
+// y = a x + b y
+__global__ void k_axpby(int n, double a, const double* x, double b, double* y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = a * x[i] + b * y[i];
+}
+
+// the e1 part of the hyper-dual forces, negated: H t1
+__global__ void k_extract_hv(int nv, const double* fhd, double* hv) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nv) {
+    hv[2 * v] = -fhd[(size_t)v * 8 + 1];
+    hv[2 * v + 1] = -fhd[(size_t)v * 8 + 5];
+  }
+}
+
+// remove the mean of x and y components (the uniform translations, which
+// span the Hessian's null space of a periodic system)
+__global__ void k_sub_mean(int nv, double* x, double mx, double my) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < nv) {
+    x[2 * v] -= mx;
+    x[2 * v + 1] -= my;
+  }
+}
+
+void launch_dot_partials(cudaStream_t st, int n, const double* a, const double* b, double* out, int nblocks) {
+  k_dot_partials<<<nblocks, 256, 0, st>>>(n, a, b, out);
+}
+void launch_axpby(cudaStream_t st, int n, double a, const double* x, double b, double* y) {
+  k_axpby<<<(n + 255) / 256, 256, 0, st>>>(n, a, x, b, y);
+}
+void launch_extract_hv(cudaStream_t st, int nv, const double* fhd, double* hv) {
+  k_extract_hv<<<(nv + 255) / 256, 256, 0, st>>>(nv, fhd, hv);
+}
+void launch_sub_mean(cudaStream_t st, int nv, double* x, double mx, double my) {
+  k_sub_mean<<<(nv + 255) / 256, 256, 0, st>>>(nv, x, mx, my);
+}
+
+}  // namespace cr

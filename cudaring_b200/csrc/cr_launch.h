@@ -66,6 +66,32 @@ void launch_rigid_drift(const LaunchCfg& c, const SysParams& p, const SysArrays&
 void launch_rigid_inject(cudaStream_t st, int np, double2* p_vel, double amp, unsigned long long seed,
                          unsigned long long stream);
 
+// cr_diff.cu: forces and energies in hyper-dual arithmetic (cr_hd.cuh)
+struct DiffArgs {
+  SysParams p;
+  const double2* pos;
+  const double2* t1;   // position tangent e1 (nullable)
+  const double2* t2;   // position tangent e2 (nullable)
+  double s1, s2;       // box tangents: L (1 + s1 e1 + s2 e2)
+  double pe1[3], pe2[3];  // tangents of ea, el, eb
+  double c1, c2;       // tangents of ln(calA0): l0, rad ~ sqrt(calA0)
+  const double* rad;
+  const double* l0;
+  const double* theta0;
+  const double* a0;
+  const int2* vtopo;
+  const int* nbr;
+  const int* nbr_cnt;
+  int nbr_cap;
+  double* force_out;   // [nv][8]: Fx (a, b, c, d), Fy (a, b, c, d)
+  double* energy_out;  // [nv][4]
+};
+void launch_diff(cudaStream_t st, int pot, const DiffArgs& g);
+void launch_dot_partials(cudaStream_t st, int n, const double* a, const double* b, double* out, int nblocks);
+void launch_axpby(cudaStream_t st, int n, double a, const double* x, double b, double* y);
+void launch_extract_hv(cudaStream_t st, int nv, const double* fhd, double* hv);
+void launch_sub_mean(cudaStream_t st, int nv, double* x, double mx, double my);
+
 // cr_nbr.cu
 struct CellGrid {
   int ncx, ncy;       // cells per dimension (>= 3 each), or 0 for brute force

@@ -210,6 +210,37 @@ class DPM2D:
 
     def getFIREState(self): return self._get("cr_get_fire_state", 3)
 
+    # ------------------------------------------------------------ derivatives
+    def hvp(self, v):
+        """Hessian-vector product of the potential energy at the current positions."""
+        out = np.empty(2 * self.numVertices)
+        self._call("cr_hvp", _f64(v).ctypes.data, out.ctypes.data)
+        return out
+
+    def hvpDevice(self, v_ptr, hv_ptr):
+        """cr_hvp_device: v and hv are device pointers (e.g. torch tensors' data_ptr())."""
+        self._call("cr_hvp_device", C.c_void_p(v_ptr), C.c_void_p(hv_ptr))
+
+    def calcPressure(self): return self._scalar("cr_calc_pressure")
+
+    PARAMS = {"ea": 0, "el": 1, "eb": 2, "lnCalA0": 3}
+
+    def paramDerivatives(self, param):
+        """(dU, dP, dF, dP/dx) along one parameter at fixed positions."""
+        dU, dP = C.c_double(), C.c_double()
+        dF = np.empty(2 * self.numVertices)
+        dPdx = np.empty(2 * self.numVertices)
+        self._call("cr_param_derivatives", int(self.PARAMS.get(param, param)), C.byref(dU), C.byref(dP),
+                   dF.ctypes.data, dPdx.ctypes.data)
+        return dU.value, dP.value, dF, dPdx
+
+    def hessianSolve(self, b, tol=1e-10, maxIter=100000):
+        x = np.empty(2 * self.numVertices)
+        it, rr = C.c_long(), C.c_double()
+        self._call("cr_hessian_solve", _f64(b).ctypes.data, x.ctypes.data, float(tol), int(maxIter), C.byref(it),
+                   C.byref(rr))
+        return x, it.value, rr.value
+
     # ------------------------------------------------------------ rigid rings
     def calcRigidForceEnergy(self): self._call("cr_calc_rigid_force_energy")
     def initRigidNVE(self, T, readState=False): self._call("cr_init_rigid_nve", T, int(bool(readState)))

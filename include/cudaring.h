@@ -303,6 +303,31 @@ int cr_neighbor_list_noalloc(const double* pos, const double* rad, const int* ri
                              const double* boxSize, double maxRad, double cutDistance, long capacity,
                              int* neighbors, int* counts, long* maxCount, void* stream);
 
+/* ---- derivatives ---------------------------------------------------------
+ * No reference counterpart (the reference has no derivatives beyond forces).
+ * Evaluated at the current positions with the current neighbour list, for
+ * deformable rings with the vertex-vertex interaction and harmonic monomers
+ * (other settings return CR_ENOTSUP).  U is the total potential energy. */
+enum { CR_PARAM_EA = 0, CR_PARAM_EL = 1, CR_PARAM_EB = 2, CR_PARAM_LN_CALA0 = 3 };
+/* Hessian-vector product hv = (d^2 U / dx^2) v, v and hv of 2 Nv values */
+int cr_hvp(cr_ctx* ctx, const double* v, double* hv);
+/* the same with v and hv in device memory of the context's device */
+int cr_hvp_device(cr_ctx* ctx, const double* v_dev, double* hv_dev);
+/* pressure P = -dU/dA for an affine dilation of positions and box (the
+ * virial pressure of every interaction and shape term; the reference's
+ * stress kernel, include/cudaKernel.cuh:1513-1568, covers pair terms only) */
+int cr_calc_pressure(cr_ctx* ctx, double* P);
+/* derivatives along one parameter at fixed positions: dU, dP (scalars), dF
+ * = dForce/dparam and dPdx = dP/dx (2 Nv each; any output may be NULL).
+ * CR_PARAM_LN_CALA0 differentiates along ln(calA0), with rest lengths and
+ * vertex radii proportional to sqrt(calA0) (DPM2D.cu:1577-1581 conventions). */
+int cr_param_derivatives(cr_ctx* ctx, int param, double* dU, double* dP, double* dF, double* dPdx);
+/* conjugate-gradient solve of H x = b (H the Hessian at the current
+ * positions) on the complement of the uniform translations, to relative
+ * residual tol */
+int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double tol, long maxIter, long* iterations,
+                     double* relres);
+
 /* ---- batches of independent systems -------------------------------------
  * No single reference counterpart: the reference holds one system per process
  * (its parameters live in __constant__ symbols, include/cudaKernel.cuh:17-67)

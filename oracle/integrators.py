@@ -200,3 +200,31 @@ class OracleRigid:
 def philox_noise(seed: int, stream: int, num_rings: int) -> np.ndarray:
     """(Np, 2) standard normals of one Philox stream, one pair per ring."""
     return np.stack([normal2(seed, stream, q) for q in range(num_rings)])
+
+
+def nve_adjoint_reference(sys_: System, pk, nsteps: int, dt: float, eps: float = 1e-6):
+    """dJ/dx0 of J = U + K after ``nsteps`` velocity-Verlet steps, by the
+    adjoint of the Verlet map with Hessian-vector products taken as central
+    differences of the oracle's forces: an FP64 reference gradient that uses
+    no derivative code.  Returns (J, dJ/dx0, dJ/dv0)."""
+    st = OracleState(sys_, pk)
+    xs = [st.pos.copy()]
+    for _ in range(nsteps):
+        st.nve_step(dt)
+        xs.append(st.pos.copy())
+    J = float(st.out["potential_energy"]) + 0.5 * float(np.dot(st.vel, st.vel))
+
+    def force(x):
+        sys_.neighbor_list(x, pk.rad, st.cut_distance)
+        return sys_.force_energy(x, pk.rad, pk.a0, pk.l0, pk.theta0)["force"]
+
+    def hvp(x, v):
+        return -(force(x + eps * v) - force(x - eps * v)) / (2 * eps)
+
+    xb = -force(xs[-1])
+    vb = st.vel.copy()
+    for n in reversed(range(nsteps)):
+        xb = xb - 0.5 * dt * hvp(xs[n + 1], vb)
+        vb = vb + dt * xb
+        xb = xb - 0.5 * dt * hvp(xs[n], vb)
+    return J, xb, vb
