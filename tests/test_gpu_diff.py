@@ -185,7 +185,7 @@ def jammed_packing(cuda_device):
 def test_minimized_gradients_match_central_differences(jammed_packing):
     theta = torch.tensor([1.0, 1.0, 0.01, 1.0], dtype=torch.float64, requires_grad=True)
     out = MinimizedEnergyPressure.apply(theta, jammed_packing)
-    U, P = float(out[0]), float(out[1])
+    U, P = float(out[0].detach()), float(out[1].detach())
     assert U > 0 and P > 0  # above jamming
     gU = torch.autograd.grad(out[0], theta, retain_graph=True)[0].numpy()
     gP = torch.autograd.grad(out[1], theta)[0].numpy()
