@@ -213,8 +213,8 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
 
   // ---- phase 3: pair forces ------------------------------------------------
   // L lanes per vertex stride over its list slots; each slot's list entries
-  // (neighbour id and packed predecessor offsets) are fetched one slot ahead,
-  // the neighbour's three positions together.
+  // (neighbour id and packed predecessor offsets) are fetched two slots ahead
+  // and the neighbour's three positions one slot ahead, all three together.
   {
     const int lv = t / L, lane = t % L;
     using T = typename std::conditional<PREC == PREC_MIXED, float, double>::type;
@@ -232,13 +232,29 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
         jn = __ldg(a.nbr + (size_t)sl * stride + i);
         if constexpr (INTER == INT_SMOOTH) pkn = __ldg(a.nbr_pq + (size_t)sl * stride + i);
       }
+      // two-stage pipeline: list entries two slots ahead, the neighbour's
+      // positions one slot ahead of the slot being evaluated
+      int j2 = 0, pk2 = 0;
+      if (sl + L < cnt) {
+        j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
+        if constexpr (INTER == INT_SMOOTH) pk2 = __ldg(a.nbr_pq + (size_t)(sl + L) * stride + i);
+      }
       if constexpr (INTER == INT_VV) {
+        double2 nxj = make_double2(0.0, 0.0);
+        double nr = 0.0;
+        if (sl < cnt) {
+          nxj = __ldg(a.pos + jn);
+          nr = __ldg(a.rad + jn);
+        }
         while (sl < cnt) {
-          const int j = jn;
-          const double2 xj = __ldg(a.pos + j);
-          const double rj = __ldg(a.rad + j);
+          const double2 xj = nxj;
+          const double rj = nr;
           sl += L;
-          if (sl < cnt) jn = __ldg(a.nbr + (size_t)sl * stride + i);
+          if (sl < cnt) {
+            nxj = __ldg(a.pos + j2);
+            nr = __ldg(a.rad + j2);
+            if (sl + L < cnt) j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
+          }
           if constexpr (PREC == PREC_MIXED) pair_own_f<POT>(p, f2(pbc2(bx, xi, xj)), (float)(ri + rj), fi, ei);
           else pair_own<POT>(p, pbc2(bx, xi, xj), ri + rj, fi, ei);
         }
@@ -257,16 +273,27 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
         const float len_i = sqrtf((float)len2_i);
         const float range = pot_range_f<POT>(p);
         T2 dummy{0, 0};
+        double2 nxj = make_double2(0.0, 0.0), nxjq = nxj, nxjqq = nxj;
+        double nr = 0.0;
+        if (sl < cnt) {
+          nxj = __ldg(a.pos + jn);
+          nxjq = __ldg(a.pos + jn + pq_first(pkn));
+          nxjqq = __ldg(a.pos + jn + pq_second(pkn));
+          nr = __ldg(a.rad + jn);
+        }
         while (sl < cnt) {
-          const int j = jn, pk = pkn;
-          const double2 xj = __ldg(a.pos + j);
-          const double2 xjq = __ldg(a.pos + j + pq_first(pk));
-          const double2 xjqq = __ldg(a.pos + j + pq_second(pk));
-          const double rsum64 = ri + __ldg(a.rad + j);
+          const double2 xj = nxj, xjq = nxjq, xjqq = nxjqq;
+          const double rsum64 = ri + nr;
           sl += L;
           if (sl < cnt) {
-            jn = __ldg(a.nbr + (size_t)sl * stride + i);
-            pkn = __ldg(a.nbr_pq + (size_t)sl * stride + i);
+            nxj = __ldg(a.pos + j2);
+            nxjq = __ldg(a.pos + j2 + pq_first(pk2));
+            nxjqq = __ldg(a.pos + j2 + pq_second(pk2));
+            nr = __ldg(a.rad + j2);
+            if (sl + L < cnt) {
+              j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
+              pk2 = __ldg(a.nbr_pq + (size_t)(sl + L) * stride + i);
+            }
           }
           const T rsum = (T)rsum64;
           const T inv_rsum = T(1) / rsum;
