@@ -85,8 +85,20 @@ def prepared_state(args, rank):
         d.resetLastPositions()
         d.calcForceEnergy()
         info = {"config": c, "fire_iterations": int(z["fire_iterations"]), "phi": d.getPreferredPhi()}
-    else:
-        d, info = workloads.prepared_deformable(1, args.rings, seed=20261203 + rank)
+    elif args.rings > 1024 and args.rings % 1024 == 0 and int(round((args.rings // 1024) ** 0.5)) ** 2 * 1024 == args.rings:
+        # large systems: the prepared 1024-ring packing replicated k x k times
+        # (a periodic image tiling is itself a packing at the same phi); the
+        # thermal velocities drawn afterwards decorrelate the copies
+        d0, info = workloads.prepared_deformable(1, 1024, seed=20261203 + rank)
+        k = int(round((args.rings // 1024) ** 0.5))
+        d = workloads.tile_system(d0, k, info["config"])
+        d0.close()
+        info = dict(info, tiled=f"{k}x{k} copies of the 1024-ring packing")
+        if args.save_state:
+            nvl = d.numVertexInParticleList
+            np.savez(args.save_state, nv_list=nvl, pos=d.getVertexPositions(), vel=d.getVertexVelocities(),
+                     rad=d.getVertexRadii(), l0=d.getRestLengths(), a0=d.getRestAreas(), theta0=d.getRestAngles(),
+                     box=d.getBoxSize(), fire_iterations=info["fire_iterations"])
         if args.save_state:
             nvl = d.numVertexInParticleList
             np.savez(args.save_state, nv_list=nvl, pos=d.getVertexPositions(), vel=d.getVertexVelocities(),

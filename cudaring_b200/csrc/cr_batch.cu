@@ -634,9 +634,9 @@ void enqueue_build(cr_batch* b, cudaStream_t st, int all) {
   na.pq_pack = b->pq_pack;
   na.nbr_pq = b->nbr_pq;
   na.cell_pq = b->cell_pq;
-  launch_cell_sort(st, b->ncells, na);
+  launch_cell_sort(st, b->ncells, b->nv, na);
   k_bnbr<<<nb, 256, 0, st>>>(n);
-  b->launches += 6;
+  b->launches += 7;
 }
 
 int alloc_lists(cr_batch* b, int cap) {

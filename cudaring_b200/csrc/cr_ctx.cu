@@ -324,7 +324,7 @@ int build_list(cr_ctx* ctx, int buf, double cut) {
   if ((rc = setup_grid(ctx, cut))) return rc;
   for (int pass = 0; pass < 3; pass++) {
     launch_nbr_build(ctx->stream, ctx->p, ctx->grid, nbr_args(ctx, buf, cut));
-    ctx->launches += (ctx->grid.ncx ? 6 : 2);
+    ctx->launches += (ctx->grid.ncx ? 7 : 2);
     CR_TRY(cudaGetLastError());
     if ((rc = read_status(ctx))) return rc;
     const int mc = ctx->status_h->max_count;
@@ -638,7 +638,7 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
   if (ctx->status_h->max_ever > 0)
     ctx->list_size_ref = std::max<long long>(ctx->list_size_ref, pow2ceil(ctx->status_h->max_ever));
   // kernels of the rebuilds that ran inside conditional nodes
-  ctx->launches += (ctx->status_h->update_count - upd0) * (ctx->grid.ncx ? 6 : 2);
+  ctx->launches += (ctx->status_h->update_count - upd0) * (ctx->grid.ncx ? 7 : 2);
   return CR_OK;
 }
 

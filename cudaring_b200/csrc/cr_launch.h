@@ -127,6 +127,6 @@ struct NbrArgs {
 void launch_nbr_build(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n);
 // building blocks shared with the batched build (cr_batch.cu)
 void launch_cell_scan(cudaStream_t st, int ncells, int* cell_cnt, int* cell_start);
-void launch_cell_sort(cudaStream_t st, int ncells, const NbrArgs& n);
+void launch_cell_sort(cudaStream_t st, int ncells, int nv, const NbrArgs& n);
 
 }  // namespace cr

@@ -13,8 +13,10 @@
 //   k_cell_count   cell of each vertex + slot inside the cell (atomic)
 //   k_cell_scan    exclusive scan of the cell counts (one CTA), zeroes counts
 //   k_cell_fill    scatter vertex ids by cell
-//   k_cell_sort    sort each cell's ids ascending and copy pos/rad/ring (SoA)
-//   k_nbr_cells    stencil search -> slot-major list (and its companion of
+//   k_cell_sort    sort each cell's ids ascending (in registers up to 16)
+//   k_cell_gather  copy pos/rad/ring/offsets into cell order (SoA)
+//   k_nbr_cells    stencil search, 16 lanes per vertex (one stencil cell per
+//                  lane, counts scanned across lanes) -> slot-major list (and its companion of
 //                  packed ring-predecessor offsets), counts, overflow flag,
 //                  lastPos = pos; the last CTA publishes the build to status
 #include "cr_launch.h"
@@ -43,28 +45,37 @@ __global__ void k_cell_count(const __grid_constant__ SysParams p, int ncx, int n
 
 // One CTA of 1024 threads: chunked exclusive scan over ncells counts.
 __global__ void __launch_bounds__(1024) k_cell_scan(int ncells, int* cell_cnt, int* cell_start) {
-  __shared__ int s_tot[1024];
-  const int t = threadIdx.x;
+  __shared__ int s_w[32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int chunk = (ncells + 1023) / 1024;
   const int b = t * chunk, e = min(ncells, b + chunk);
   int sum = 0;
   for (int c = b; c < e; c++) sum += cell_cnt[c];
-  s_tot[t] = sum;
-  __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    int y = (t >= off) ? s_tot[t - off] : 0;
-    __syncthreads();
-    s_tot[t] += y;
-    __syncthreads();
+  // block-wide inclusive scan of the chunk sums: warp shuffles, then the 32 warp totals
+  int incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
   }
-  int run = s_tot[t] - sum;  // exclusive prefix of this chunk
+  if (lane == 31) s_w[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = s_w[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    s_w[lane] = w;
+  }
+  __syncthreads();
+  int run = incl - sum + (warp > 0 ? s_w[warp - 1] : 0);  // exclusive prefix of this chunk
   for (int c = b; c < e; c++) {
     const int n = cell_cnt[c];
     cell_start[c] = run;
     run += n;
     cell_cnt[c] = 0;
   }
-  if (t == 1023) cell_start[ncells] = s_tot[1023];
+  if (t == 1023) cell_start[ncells] = s_w[31];
 }
 
 __global__ void k_cell_fill(int nv, const int* cell_of, const int* slot, const int* cell_start, int* cell_vid) {
@@ -72,29 +83,53 @@ __global__ void k_cell_fill(int nv, const int* cell_of, const int* slot, const i
   if (v < nv) cell_vid[cell_start[cell_of[v]] + slot[v]] = v;
 }
 
-__global__ void k_cell_sort(int ncells, const int* cell_start, int* cell_vid, const double2* pos, const double* rad,
-                            const int* ring_of, const int* pq_pack, double2* cell_pos, double* cell_rad,
-                            int* cell_ring, int* cell_pq) {
+// Ascending ids in every cell (the atomic slots of k_cell_count come in
+// scheduling order): cells of up to 16 vertices are sorted in registers.
+__global__ void k_cell_sort(int ncells, const int* cell_start, int* cell_vid) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < ncells) {
-    const int b = cell_start[c], e = cell_start[c + 1];
-    for (int i = b + 1; i < e; i++) {  // insertion sort: cells hold a handful of vertices
-      const int key = cell_vid[i];
-      int j = i - 1;
-      while (j >= b && cell_vid[j] > key) {
-        cell_vid[j + 1] = cell_vid[j];
-        j--;
+  if (c >= ncells) return;
+  const int b = cell_start[c], e = cell_start[c + 1], n = e - b;
+  if (n <= 1) return;
+  if (n <= 16) {
+    int ids[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) ids[i] = (i < n) ? cell_vid[b + i] : 0x7fffffff;
+#pragma unroll
+    for (int i = 1; i < 16; i++) {
+#pragma unroll
+      for (int j = i; j > 0; j--) {
+        const int lo = min(ids[j - 1], ids[j]), hi = max(ids[j - 1], ids[j]);
+        ids[j - 1] = lo;
+        ids[j] = hi;
       }
-      cell_vid[j + 1] = key;
     }
-    for (int i = b; i < e; i++) {
-      const int v = cell_vid[i];
-      cell_pos[i] = pos[v];
-      cell_rad[i] = rad[v];
-      cell_ring[i] = ring_of[v];
-      if (cell_pq) cell_pq[i] = pq_pack[v];
-    }
+#pragma unroll
+    for (int i = 0; i < 16; i++)
+      if (i < n) cell_vid[b + i] = ids[i];
+    return;
   }
+  for (int i = b + 1; i < e; i++) {
+    const int key = cell_vid[i];
+    int j = i - 1;
+    while (j >= b && cell_vid[j] > key) {
+      cell_vid[j + 1] = cell_vid[j];
+      j--;
+    }
+    cell_vid[j + 1] = key;
+  }
+}
+
+// SoA copies in cell order for the stencil search, one thread per entry.
+__global__ void k_cell_gather(int nv, const int* cell_start_end, const int* cell_vid, const double2* pos,
+                              const double* rad, const int* ring_of, const int* pq_pack, double2* cell_pos,
+                              double* cell_rad, int* cell_ring, int* cell_pq) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nv || i >= *cell_start_end) return;
+  const int v = cell_vid[i];
+  cell_pos[i] = pos[v];
+  cell_rad[i] = rad[v];
+  cell_ring[i] = ring_of[v];
+  if (cell_pq) cell_pq[i] = pq_pack[v];
 }
 
 __device__ __forceinline__ bool is_neighbor(const SysParams& p, double2 xi, double2 xj, double rsum, double cut) {
@@ -125,50 +160,88 @@ __device__ __forceinline__ void publish_build(const NbrArgs& n, int my_max, int 
   }
 }
 
+// 16 lanes per vertex (two vertices per warp): lane l < 9 scans stencil cell
+// l (dy = l / 3 - 1, dx = l % 3 - 1, the sequential order), counts its
+// neighbours, and after an exclusive scan of the counts over the lanes writes
+// them at its offset, so a vertex's list has the sequential scan's order.
+constexpr int kNbrLanes = 16;
+
 __global__ void __launch_bounds__(256) k_nbr_cells(const __grid_constant__ SysParams p, int ncx, int ncy,
                                                    const __grid_constant__ NbrArgs n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int cnt = 0;
-  if (i < p.nv) {
-    const double2 xi = n.pos[i];
-    const double ri = n.rad[i];
-    const int ring = n.ring_of[i];
-    const int c = n.cell_of[i];
+  const int g = blockIdx.x * (256 / kNbrLanes) + threadIdx.x / kNbrLanes;  // vertex
+  const int lane = threadIdx.x % kNbrLanes;
+  int mine = 0, kb = 0, ke = 0;
+  unsigned int hits = 0u;  // neighbours among the cell's first 32 entries
+  double2 xi = make_double2(0.0, 0.0);
+  double ri = 0.0;
+  int ring = -1;
+  const bool valid = g < p.nv;
+  if (valid && lane < 9) {
+    xi = n.pos[g];
+    ri = n.rad[g];
+    ring = n.ring_of[g];
+    const int c = n.cell_of[g];
     const int cx = c % ncx, cy = c / ncx;
-    for (int dy = -1; dy <= 1; dy++) {
-      int yy = cy + dy;
-      yy += (yy < 0) ? ncy : 0;
-      yy -= (yy >= ncy) ? ncy : 0;
-      for (int dx = -1; dx <= 1; dx++) {
-        int xx = cx + dx;
-        xx += (xx < 0) ? ncx : 0;
-        xx -= (xx >= ncx) ? ncx : 0;
-        const int cc = yy * ncx + xx;
-        const int b = n.cell_start[cc], e = n.cell_start[cc + 1];
-        for (int k = b; k < e; k++) {
-          if (n.cell_ring[k] == ring) continue;
-          if (is_neighbor(p, xi, n.cell_pos[k], ri + n.cell_rad[k], n.cut_distance)) {
-            if (cnt < n.cap) {
-              n.nbr[(size_t)cnt * p.nv + i] = n.cell_vid[k];
-              if (n.nbr_pq) n.nbr_pq[(size_t)cnt * p.nv + i] = n.cell_pq[k];
-            }
-            cnt++;
+    int yy = cy + lane / 3 - 1;
+    yy += (yy < 0) ? ncy : 0;
+    yy -= (yy >= ncy) ? ncy : 0;
+    int xx = cx + lane % 3 - 1;
+    xx += (xx < 0) ? ncx : 0;
+    xx -= (xx >= ncx) ? ncx : 0;
+    const int cc = yy * ncx + xx;
+    kb = n.cell_start[cc];
+    ke = n.cell_start[cc + 1];
+    for (int k = kb; k < ke; k++) {
+      if (n.cell_ring[k] != ring && is_neighbor(p, xi, n.cell_pos[k], ri + n.cell_rad[k], n.cut_distance)) {
+        if (k - kb < 32) hits |= 1u << (k - kb);
+        mine++;
+      }
+    }
+  }
+  // exclusive scan of the lane counts inside the 16-lane group
+  int incl = mine;
+  for (int o = 1; o < kNbrLanes; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o, kNbrLanes);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, kNbrLanes - 1, kNbrLanes);
+  int slot = incl - mine;
+  if (valid && lane < 9 && mine > 0) {
+    if (ke - kb <= 32) {
+      while (hits) {
+        const int k = kb + __ffs(hits) - 1;
+        hits &= hits - 1u;
+        if (slot < n.cap) {
+          n.nbr[(size_t)slot * p.nv + g] = n.cell_vid[k];
+          if (n.nbr_pq) n.nbr_pq[(size_t)slot * p.nv + g] = n.cell_pq[k];
+        }
+        slot++;
+      }
+    } else {
+      for (int k = kb; k < ke; k++) {
+        if (n.cell_ring[k] != ring && is_neighbor(p, xi, n.cell_pos[k], ri + n.cell_rad[k], n.cut_distance)) {
+          if (slot < n.cap) {
+            n.nbr[(size_t)slot * p.nv + g] = n.cell_vid[k];
+            if (n.nbr_pq) n.nbr_pq[(size_t)slot * p.nv + g] = n.cell_pq[k];
           }
+          slot++;
         }
       }
     }
-    n.nbr_cnt[i] = cnt;
-    n.last_pos[i] = xi;
+  }
+  if (valid && lane == 0) {
+    n.nbr_cnt[g] = total;
+    n.last_pos[g] = n.pos[g];
   }
   // CTA max and overflow, then publish
-  int m = cnt;
+  int m = (valid && lane == 0) ? total : 0;
   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
   __shared__ int s_max[8];
   if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
   __syncthreads();
   int bm = 0;
   if (threadIdx.x == 0)
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) bm = max(bm, s_max[w]);
+    for (int w = 0; w < 8; w++) bm = max(bm, s_max[w]);
   publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap);
 }
 
@@ -217,10 +290,11 @@ void launch_cell_scan(cudaStream_t st, int ncells, int* cell_cnt, int* cell_star
   k_cell_scan<<<1, 1024, 0, st>>>(ncells, cell_cnt, cell_start);
 }
 
-void launch_cell_sort(cudaStream_t st, int ncells, const NbrArgs& n) {
-  k_cell_sort<<<(ncells + 255) / 256, 256, 0, st>>>(ncells, n.cell_start, n.cell_vid, n.pos, n.rad, n.ring_of,
-                                                    n.nbr_pq ? n.pq_pack : nullptr, n.cell_pos, n.cell_rad,
-                                                    n.cell_ring, n.nbr_pq ? n.cell_pq : nullptr);
+void launch_cell_sort(cudaStream_t st, int ncells, int nv, const NbrArgs& n) {
+  k_cell_sort<<<(ncells + 127) / 128, 128, 0, st>>>(ncells, n.cell_start, n.cell_vid);
+  k_cell_gather<<<(nv + 255) / 256, 256, 0, st>>>(nv, n.cell_start + ncells, n.cell_vid, n.pos, n.rad, n.ring_of,
+                                                  n.nbr_pq ? n.pq_pack : nullptr, n.cell_pos, n.cell_rad,
+                                                  n.cell_ring, n.nbr_pq ? n.cell_pq : nullptr);
 }
 
 void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g, const NbrArgs& n) {
@@ -231,10 +305,8 @@ void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g
     k_cell_count<<<nb, 256, 0, stream>>>(p, g.ncx, g.ncy, n.pos, n.cell_of, n.slot, n.cell_cnt);
     k_cell_scan<<<1, 1024, 0, stream>>>(ncells, n.cell_cnt, n.cell_start);
     k_cell_fill<<<nb, 256, 0, stream>>>(p.nv, n.cell_of, n.slot, n.cell_start, n.cell_vid);
-    k_cell_sort<<<(ncells + 255) / 256, 256, 0, stream>>>(ncells, n.cell_start, n.cell_vid, n.pos, n.rad, n.ring_of,
-                                                          n.nbr_pq ? n.pq_pack : nullptr, n.cell_pos, n.cell_rad,
-                                                          n.cell_ring, n.nbr_pq ? n.cell_pq : nullptr);
-    k_nbr_cells<<<nb, 256, 0, stream>>>(p, g.ncx, g.ncy, n);
+    launch_cell_sort(stream, ncells, p.nv, n);
+    k_nbr_cells<<<(p.nv + 256 / kNbrLanes - 1) / (256 / kNbrLanes), 256, 0, stream>>>(p, g.ncx, g.ncy, n);
   } else {
     k_nbr_brute<<<nb, 256, 0, stream>>>(p, n);
   }

@@ -128,3 +128,29 @@ def prepared_deformable(index: int = 1, rings: int | None = None, seed: int = 20
     d.calcForceEnergy()
     info.update(config=c, placement=placement, phi=d.getPreferredPhi(), cut_distance=cut, seed=seed)
     return d, info
+
+
+def tile_system(d: DPM2D, k: int, config: dict) -> DPM2D:
+    """A k x k periodic tiling of the system held by ``d`` (positions,
+    velocities, radii, rest lengths / areas / angles, box) as a new context
+    with the workload ``config``'s potential and constants; lists built and
+    forces evaluated.  A tiling of a periodic packing is itself a packing at
+    the same packing fraction."""
+    nvl = d.numVertexInParticleList
+    box = d.getBoxSize()
+    pos = d.getVertexPositions().reshape(-1, 2)
+    copies = [(pos + np.array([ix * box[0], iy * box[1]])).reshape(-1) for iy in range(k) for ix in range(k)]
+    n = k * k
+    pk = synth.Packing(nv_list=np.tile(nvl, n), pos=np.concatenate(copies), vel=np.tile(d.getVertexVelocities(), n),
+                       rad=np.tile(d.getVertexRadii(), n), l0=np.tile(d.getRestLengths(), n),
+                       theta0=np.tile(d.getRestAngles(), n), a0=np.tile(d.getRestAreas(), n), box=box * k,
+                       centres=np.zeros((n * d.numParticles, 2)))
+    kw = {key: config[key] for key in ("potential", "interaction", "ea", "el", "eb", "ec", "dt") if key in config}
+    if "LJcutoff" in config:
+        kw["LJcutoff"] = config["LJcutoff"]
+    t = DPM2D.from_packing(pk, **kw)
+    cut = t.setDisplacementCutoff(0.5, 2.0 * t.getMeanVertexRadius())
+    t.calcNeighborList(cut)
+    t.resetLastPositions()
+    t.calcForceEnergy()
+    return t
