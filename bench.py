@@ -94,17 +94,13 @@ def prepared_state(args, rank):
         d = workloads.tile_system(d0, k, info["config"])
         d0.close()
         info = dict(info, tiled=f"{k}x{k} copies of the 1024-ring packing")
-        if args.save_state:
-            nvl = d.numVertexInParticleList
-            np.savez(args.save_state, nv_list=nvl, pos=d.getVertexPositions(), vel=d.getVertexVelocities(),
-                     rad=d.getVertexRadii(), l0=d.getRestLengths(), a0=d.getRestAreas(), theta0=d.getRestAngles(),
-                     box=d.getBoxSize(), fire_iterations=info["fire_iterations"])
-        if args.save_state:
-            nvl = d.numVertexInParticleList
-            np.savez(args.save_state, nv_list=nvl, pos=d.getVertexPositions(), vel=d.getVertexVelocities(),
-                     rad=d.getVertexRadii(), l0=d.getRestLengths(), a0=d.getRestAreas(),
-                     theta0=np.repeat(2 * np.pi / nvl, nvl).astype(np.float64), box=d.getBoxSize(),
-                     fire_iterations=info["fire_iterations"])
+    else:
+        d, info = workloads.prepared_deformable(1, args.rings, seed=20261203 + rank)
+    if args.save_state and not args.load_state:
+        nvl = d.numVertexInParticleList
+        np.savez(args.save_state, nv_list=nvl, pos=d.getVertexPositions(), vel=d.getVertexVelocities(),
+                 rad=d.getVertexRadii(), l0=d.getRestLengths(), a0=d.getRestAreas(), theta0=d.getRestAngles(),
+                 box=d.getBoxSize(), fire_iterations=info["fire_iterations"])
     if args.lanes:
         d.setLanes(args.lanes)
     elif not args.profile_kernel:

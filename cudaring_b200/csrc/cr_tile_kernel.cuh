@@ -24,11 +24,15 @@
 
 namespace cr {
 
-// Occupancy target in threads per SM: 512 leaves 128 registers per thread,
-// where the smooth-interaction body compiles without spills.
-constexpr int kTileThreadsPerSM = 512;
-
 enum Prec : int { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+// Occupancy target in threads per SM: 512 leaves 128 registers per thread,
+// where the FP64 smooth-interaction body compiles without spills; the mixed
+// body fits 96 registers (640 threads, five 128-thread CTAs per SM).
+template <int PREC>
+constexpr int tile_threads_per_sm() {
+  return PREC == PREC_MIXED ? 640 : 512;
+}
 
 template <typename T2> __device__ __forceinline__ T2 cvt2(double2 d);
 template <> __device__ __forceinline__ double2 cvt2<double2>(double2 d) { return d; }
@@ -65,7 +69,7 @@ __device__ __forceinline__ void tile_skip(const StepArgs& s, DevStatus* st) {
 // the system, whose box, displacement cutoff, FIRE scalars and flags come
 // from s.bsys, and whose last tile reduces the system's partial sums.
 template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH = false>
-__global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const __grid_constant__ SysParams p,
+__global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC>() / BLOCK) k_tile(const __grid_constant__ SysParams p,
                                                 const __grid_constant__ SysArrays a,
                                                 const __grid_constant__ StepArgs s) {
   constexpr int TV = BLOCK / L;
@@ -81,6 +85,8 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
   __shared__ double2 s_fpair[TV];   // pair force on v
   __shared__ double2 s_fprev[TV];   // smooth: force on prev(v) gathered by v
   __shared__ double s_epair[TV];
+  __shared__ double2 s_fsh[TV];     // shape force on v, parked across the pair phase
+  __shared__ double s_esh[TV];      // shape energy booked on v
   __shared__ int s_lp[TV];
   __shared__ __align__(16) double2 s_vel[TS];
   __shared__ __align__(16) double2 s_last[TS];
@@ -209,6 +215,8 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
     fsh.x += p.eb * (pvar * ps.y + nvar * ns.y);
     fsh.y += p.eb * (pvar * (-ps.x) + nvar * (-ns.x));
     esh += 0.5 * p.eb * thisAD * thisAD;
+    s_fsh[t] = fsh;
+    s_esh[t] = esh;
   }
 
   // ---- phase 3: pair forces ------------------------------------------------
@@ -354,7 +362,16 @@ __global__ void __launch_bounds__(BLOCK, kTileThreadsPerSM / BLOCK) k_tile(const
   double evtx = 0.0;  // per-vertex energy as the reference stores it
   double epair = 0.0;
   if (t < nvt) {
+    // ring topology again (an L1 hit) rather than registers held across phase 3
+    const int2 tp = __ldg(a.vtopo + v0 + t);
+    ring = tp.x;
+    k = tp.y & 0xffff;
+    nvr = tp.y >> 16;
+    lf = t - k;
+    ln = lf + (k + 1 == nvr ? 0 : k + 1);
     const double2 fp = s_fpair[t];
+    const double2 fsh = s_fsh[t];
+    const double esh = s_esh[t];
     F.x = fsh.x + fp.x;
     F.y = fsh.y + fp.y;
     if constexpr (INTER == INT_SMOOTH) {
