@@ -176,6 +176,8 @@ struct DevStatus {
   long long fire_iters;    // FIRE iterations actually performed
   long long rng_step;      // integrator steps since init: noise of step s uses Philox streams 2s, 2s+1
   double sums[8];     // final reductions written by the last block
+  unsigned int bar_count;  // grid barrier of the one-launch build: arrivals
+  int stalled;        // a grid-barrier wait gave up (the build did not finish)
 };
 
 }  // namespace cr

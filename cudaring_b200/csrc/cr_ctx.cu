@@ -36,6 +36,7 @@ struct Op {
 struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
+  long long launches = 0;  // kernel launches per graph launch
 };
 
 long long pow2ceil(long long x) {
@@ -49,7 +50,6 @@ long long pow2ceil(long long x) {
 struct cr_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
-  cudaStream_t side = nullptr;  // capture stream for conditional bodies
   std::string err;
   long long launches = 0;
 
@@ -90,6 +90,8 @@ struct cr_ctx {
   int ncells_alloc = 0;
   int *cell_of = nullptr, *slot = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_vid = nullptr,
       *cell_ring = nullptr, *cell_pq = nullptr;
+  int* block_sum = nullptr;  // per-CTA totals of the one-launch build
+  int fused_max = 0;         // CTAs of the one-launch build resident at once
   double2* cell_pos = nullptr;
   double* cell_rad = nullptr;
   double* partials = nullptr;
@@ -282,6 +284,7 @@ NbrArgs nbr_args(cr_ctx* ctx, int buf, double cut) {
   n.status = ctx->status;
   n.count_op = 0;
   n.count_update = 0;
+  n.block_sum = ctx->block_sum;
   return n;
 }
 
@@ -302,6 +305,8 @@ int clear_flags(cr_ctx* ctx) {
   s.converged = 0;
   s.nonfinite = 0;
   s.done_ctr = 0;
+  s.bar_count = 0;
+  s.stalled = 0;
   *ctx->status_h = s;
   CR_TRY(cudaMemcpyAsync(ctx->status, ctx->status_h, sizeof(DevStatus), cudaMemcpyHostToDevice, ctx->stream));
   CR_TRY(cudaStreamSynchronize(ctx->stream));
@@ -323,10 +328,12 @@ int build_list(cr_ctx* ctx, int buf, double cut) {
   int rc;
   if ((rc = setup_grid(ctx, cut))) return rc;
   for (int pass = 0; pass < 3; pass++) {
-    launch_nbr_build(ctx->stream, ctx->p, ctx->grid, nbr_args(ctx, buf, cut));
-    ctx->launches += (ctx->grid.ncx ? 7 : 2);
+    launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nbr_args(ctx, buf, cut), nbr_fused_blocks(ctx->nv, ctx->fused_max),
+                     1);
+    ctx->launches += 1;
     CR_TRY(cudaGetLastError());
     if ((rc = read_status(ctx))) return rc;
+    if (ctx->status_h->stalled) return ctx->fail(CR_ECUDA, "neighbour-list build: a grid barrier timed out");
     const int mc = ctx->status_h->max_count;
     if (!ctx->status_h->overflow) {
       ctx->list_size_ref = std::max<long long>(ctx->list_size_ref, mc > 0 ? pow2ceil(mc) : 0);
@@ -474,46 +481,30 @@ void enqueue_op(cr_ctx* ctx, cudaStream_t st, const Op& op, int kind, bool use_c
   ctx->launches++;
 }
 
+// A step sequence as one graph.  Every op that may arm a rebuild (its
+// displacement check) is followed by the one-launch build, which returns at
+// once unless the check fired (DPM2D::checkDisplacement, src/DPM2D.cu:1397-1405,
+// rebuilds and counts an update).
 int capture_graph(cr_ctx* ctx, const std::vector<Op>& ops, int kind, GraphEntry& ge) {
-  cudaGraph_t graph;
-  CR_TRY(cudaGraphCreate(&graph, 0));
-  CR_TRY(cudaStreamBeginCaptureToGraph(ctx->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  CR_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  const int fb = nbr_fused_blocks(ctx->nv, ctx->fused_max);
+  ge.launches = 0;
   for (const Op& op : ops) {
-    cudaGraphConditionalHandle h = 0;
+    enqueue_op(ctx, ctx->stream, op, kind, false, 0);
+    ge.launches++;
     if (op.check_after) {
-      cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
-      if (e != cudaSuccess) {
-        cudaGraph_t dummy;
-        cudaStreamEndCapture(ctx->stream, &dummy);
-        cudaGraphDestroy(graph);
-        return ctx->fail(CR_ECUDA, std::string("cudaGraphConditionalHandleCreate: ") + cudaGetErrorString(e));
-      }
-    }
-    enqueue_op(ctx, ctx->stream, op, kind, op.check_after != 0, h);
-    if (op.check_after) {
-      cudaStreamCaptureStatus cs;
-      cudaGraph_t cg;
-      const cudaGraphNode_t* deps = nullptr;
-      size_t ndeps = 0;
-      CR_TRY(cudaStreamGetCaptureInfo(ctx->stream, &cs, nullptr, &cg, &deps, &ndeps));
-      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-      cp.conditional.handle = h;
-      cp.conditional.type = cudaGraphCondTypeIf;
-      cp.conditional.size = 1;
-      cudaGraphNode_t node;
-      CR_TRY(cudaGraphAddNode(&node, cg, deps, ndeps, &cp));
-      CR_TRY(cudaStreamUpdateCaptureDependencies(ctx->stream, &node, 1, cudaStreamSetCaptureDependencies));
-      cudaGraph_t body = cp.conditional.phGraph_out[0];
-      CR_TRY(cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
       NbrArgs nb = nbr_args(ctx, op.check_buf, ctx->cut_distance);
-      nb.count_update = 1;  // DPM2D::checkDisplacement's updateCount (src/DPM2D.cu:1397-1405)
-      launch_nbr_build(ctx->side, ctx->p, ctx->grid, nb);
-      cudaGraph_t body_out;
-      CR_TRY(cudaStreamEndCapture(ctx->side, &body_out));
+      nb.count_update = 1;
+      launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nb, fb, 0);
+      ge.launches++;
     }
   }
-  cudaGraph_t out;
-  CR_TRY(cudaStreamEndCapture(ctx->stream, &out));
+  cudaGraph_t out = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &out);
+  if (e != cudaSuccess) {
+    if (out) cudaGraphDestroy(out);
+    return ctx->fail(CR_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  }
   CR_TRY(cudaGraphInstantiate(&ge.exec, out, 0));
   ge.graph = out;
   return CR_OK;
@@ -553,7 +544,7 @@ int launch_chunk(cr_ctx* ctx, const std::vector<Op>& ops, int kind, long n) {
     }
     if (ctx->use_graphs) {
       CR_TRY(cudaGraphLaunch(it->second.exec, ctx->stream));
-      ctx->launches += (long long)ops.size();
+      ctx->launches += it->second.launches;
       return CR_OK;
     }
   }
@@ -583,7 +574,6 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
     CR_TRY(cudaGetLastError());
   }
   if ((rc = clear_flags(ctx))) return rc;
-  const long long upd0 = ctx->status_h->update_count;
   const long chunk = 128;
   std::vector<std::vector<Op>> plan;
   std::vector<long> sizes;
@@ -613,6 +603,7 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
     }
     if ((rc = read_status(ctx))) return rc;
     if (ctx->status_h->abort) {
+      if (ctx->status_h->stalled) return ctx->fail(CR_ECUDA, "neighbour-list build: a grid barrier timed out");
       if (ctx->status_h->nonfinite) return ctx->fail(CR_ENONFINITE, "non-finite force during the step sequence");
       if (!ctx->status_h->overflow) return ctx->fail(CR_ECUDA, "step sequence aborted");
       // locate the op after which the failed build ran (builds are not ops)
@@ -637,8 +628,6 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
   ctx->cur = plan[std::min(c, plan.size()) - 1].back().out_buf;
   if (ctx->status_h->max_ever > 0)
     ctx->list_size_ref = std::max<long long>(ctx->list_size_ref, pow2ceil(ctx->status_h->max_ever));
-  // kernels of the rebuilds that ran inside conditional nodes
-  ctx->launches += (ctx->status_h->update_count - upd0) * (ctx->grid.ncx ? 7 : 2);
   return CR_OK;
 }
 
@@ -734,8 +723,13 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
     }
   }
   make_tiles(ctx);
-  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess ||
-      (e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking)) != cudaSuccess) {
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+    delete ctx;
+    return CR_ECUDA;
+  }
+  ctx->fused_max = nbr_fused_max_blocks();
+  if (ctx->fused_max <= 0) {
+    cudaStreamDestroy(ctx->stream);
     delete ctx;
     return CR_ECUDA;
   }
@@ -758,6 +752,7 @@ int cr_create(long numParticles, const long* nvList, cr_ctx** out) {
       (rc = dalloc(ctx, &ctx->pq_pack, nv)) ||
       (rc = dalloc(ctx, &ctx->cell_pos, nv)) || (rc = dalloc(ctx, &ctx->cell_rad, nv)) ||
       (rc = dalloc(ctx, &ctx->status, 1)) || (rc = dalloc(ctx, &ctx->fire_state, 8)) ||
+      (rc = dalloc(ctx, &ctx->block_sum, std::max(1, ctx->fused_max))) ||
       (rc = dalloc(ctx, &ctx->p_vel, np)) || (rc = dalloc(ctx, &ctx->p_force, np)) ||
       (rc = dalloc(ctx, &ctx->p_angvel, np)) || (rc = dalloc(ctx, &ctx->p_torque, np)) ||
       (rc = dalloc(ctx, &ctx->p_moi, np)) || (rc = dalloc(ctx, &ctx->v_torque, nv)) ||
@@ -813,12 +808,11 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
                   ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
                   ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec,
-                  ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle};
+                  ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  if (ctx->side) cudaStreamDestroy(ctx->side);
   delete ctx;
   return CR_OK;
 }

@@ -123,8 +123,18 @@ struct NbrArgs {
   DevStatus* status;
   int count_op;       // 1: the build is one op of a step sequence (ops_done += 1)
   int count_update;   // 1: a displacement-triggered rebuild (DPM2D::updateCount += 1)
+  int* block_sum = nullptr;  // [grid] per-CTA cell totals of the one-launch build
 };
 void launch_nbr_build(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n);
+// The whole build in one launch of `blocks` CTAs (at most nbr_fused_max_blocks()).
+// force = 0: return at once unless the status block armed a rebuild (and no
+// abort or convergence is pending), so it can follow every step op in a graph.
+void launch_nbr_fused(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n, int blocks,
+                      int force);
+// CTAs of the one-launch build that the current device holds at once.
+int nbr_fused_max_blocks();
+// Grid of the one-launch build for nv vertices.
+int nbr_fused_blocks(int nv, int max_blocks);
 // building blocks shared with the batched build (cr_batch.cu)
 void launch_cell_scan(cudaStream_t st, int ncells, int* cell_cnt, int* cell_start);
 void launch_cell_sort(cudaStream_t st, int ncells, int nv, const NbrArgs& n);
