@@ -15,10 +15,11 @@
 //   k_cell_fill    scatter vertex ids by cell
 //   k_cell_sort    sort each cell's ids ascending (in registers up to 16)
 //   k_cell_gather  copy pos/rad/ring/offsets into cell order (SoA)
-//   k_nbr_cells    stencil search, 16 lanes per vertex (one stencil cell per
-//                  lane, counts scanned across lanes) -> slot-major list (and its companion of
-//                  packed ring-predecessor offsets), counts, overflow flag,
-//                  lastPos = pos; the last CTA publishes the build to status
+//   k_nbr_cells    stencil search, one warp per home cell (candidates one per
+//                  lane, home vertices staged in shared memory) -> slot-major
+//                  list (and its companion of packed ring-predecessor
+//                  offsets), counts, overflow flag, lastPos = pos; the last
+//                  CTA publishes the build to status
 #include <algorithm>
 
 #include "cr_launch.h"
@@ -137,10 +138,31 @@ __global__ void k_cell_gather(int nv, const int* cell_start_end, const int* cell
   if (cell_pq) cell_pq[i] = pq_pack[v];
 }
 
+// -calcOverlap(thisPos, otherPos, radSum) < cutDistance
+// (include/cudaKernel.cuh:1752), i.e. d < (1 + cut) * rsum.  The squared
+// distance decides every pair outside a relative band of 1e-9 around the
+// threshold (rounding moves either side by ~1e-16), the reference expression
+// decides the pairs inside it, so the decisions are those of the reference
+// expression while most pairs skip its square root and division.
+__device__ __forceinline__ double pair_sq(const SysParams& p, double2 xi, double2 xj) {
+  const double2 dl = pbc2(p, xi, xj);
+  double sq = dl.x * dl.x;
+  return fma(dl.y, dl.y, sq);
+}
+// 1: neighbour, 0: not, -1: inside the band (the reference expression decides)
+__device__ __forceinline__ int pre_test(double sq, double rsum, double cut) {
+  if (!(cut > -0.5)) return -1;
+  const double t = (1.0 + cut) * rsum;
+  const double t2 = t * t;
+  return (sq < t2 * (1.0 - 1e-9)) ? 1 : ((sq > t2 * (1.0 + 1e-9)) ? 0 : -1);
+}
+__device__ __forceinline__ bool exact_test(double sq, double rsum, double cut) {
+  return -(1.0 - sqrt(sq) / rsum) < cut;
+}
 __device__ __forceinline__ bool is_neighbor(const SysParams& p, double2 xi, double2 xj, double rsum, double cut) {
-  // -calcOverlap(thisPos, otherPos, radSum) < cutDistance (include/cudaKernel.cuh:1752)
-  const double d = dist_of(pbc2(p, xi, xj));
-  return -(1.0 - d / rsum) < cut;
+  const double sq = pair_sq(p, xi, xj);
+  const int pt = pre_test(sq, rsum, cut);
+  return pt >= 0 ? pt == 1 : exact_test(sq, rsum, cut);
 }
 
 __device__ __forceinline__ void publish_build(const NbrArgs& n, int my_max, int my_overflow) {
@@ -166,29 +188,56 @@ __device__ __forceinline__ void publish_build(const NbrArgs& n, int my_max, int 
   }
 }
 
-// 16 lanes per vertex (two vertices per warp): lane l < 9 scans stencil cell
-// l (dy = l / 3 - 1, dx = l % 3 - 1, the sequential order), counts its
-// neighbours, and after an exclusive scan of the counts over the lanes writes
-// them at its offset, so a vertex's list has the sequential scan's order.
-constexpr int kNbrLanes = 16;
+// Per-warp shared staging of the home vertices (32 at a time): positions
+// relative to the home cell's corner and radii in single precision for the
+// pre-test, ring and id.
+struct HomeStage {
+  float2 x[32];
+  float r[32];
+  int ring[32];
+  int id[32];
+};
 
-// The stencil search of vertex g by the 16 lanes of its group (all 16 lanes
-// call it; valid = g < nv); ids[k] is the vertex at cell-order entry k.
-// Writes the list, count and lastPos; returns the count on lane 0, 0
-// elsewhere.
-__device__ __forceinline__ int stencil_vertex(const SysParams& p, int ncx, int ncy, const NbrArgs& n,
-                                              const int* ids, int g, int lane, bool valid) {
-  int mine = 0, kb = 0, ke = 0;
-  unsigned int hits = 0u;  // neighbours among the cell's first 32 entries
-  double2 xi = make_double2(0.0, 0.0);
-  double ri = 0.0;
-  int ring = -1;
-  if (valid && lane < 9) {
-    xi = n.pos[g];
-    ri = n.rad[g];
-    ring = n.ring_of[g];
-    const int c = n.cell_of[g];
-    const int cx = c % ncx, cy = c / ncx;
+// Single-precision pre-test.  Positions are taken relative to the home
+// cell's corner o (each candidate shifted by the box length its stencil
+// cell was wrapped by, which is its minimum image whenever it lies within
+// range: cells are no smaller than the largest neighbour distance and there
+// are at least three per side), so every coordinate is below R = 3 cells in
+// magnitude and carries an absolute rounding error below e = 2^-22 R after
+// the conversion.  With t = (1 + cut) rsum, the squared distance then lies
+// within M = 1e-5 t^2 + 4 t e + 4 e^2 of the exact one wherever the exact
+// one is below (t^2 + M): pairs with sq < t^2 - M are neighbours, pairs with
+// sq > t^2 + M are not, and the few in between take the double-precision
+// test, whose decisions are the reference expression's.
+struct PreTest {
+  double ox, oy;     // home cell corner
+  float e4, ee4;     // 4 e, 4 e^2
+  float opc;         // 1 + cut
+  bool on;           // cut > -0.5 (else every pair takes the exact test)
+};
+
+__device__ __forceinline__ float2 rel_f(const SysParams& p, const PreTest& pt, double2 x, double sx, double sy) {
+  const double wx = x.x - p.lx * floor(x.x * p.inv_lx) + sx;
+  const double wy = x.y - p.ly * floor(x.y * p.inv_ly) + sy;
+  return make_float2((float)(wx - pt.ox), (float)(wy - pt.oy));
+}
+
+// One warp per home cell.  The candidates are the entries of the 3x3 stencil
+// cells concatenated in the sequential scan's order (stencil cell l = 0..8,
+// dy = l / 3 - 1, dx = l % 3 - 1; inside a cell, cell order), 32 at a time,
+// one per lane.  For each home vertex h of the cell (staged in shared
+// memory) the lanes test their candidate, a ballot marks the hits, and hit
+// lanes write at h's running count plus the hits on lower lanes, so every
+// vertex's list has the sequential scan's order.  ids[k] is the vertex at
+// cell-order entry k.  Writes lists, counts and lastPos of the cell's
+// vertices; returns the largest count on the lanes that held a home vertex
+// (0 elsewhere).
+__device__ __forceinline__ int stencil_cell(const SysParams& p, int ncx, int ncy, const NbrArgs& n, const int* ids,
+                                            int c, int lane, HomeStage& hs) {
+  constexpr unsigned kAll = 0xffffffffu;
+  const int cx = c % ncx, cy = c / ncx;
+  int sb = 0, se = 0;
+  if (lane < 9) {
     int yy = cy + lane / 3 - 1;
     yy += (yy < 0) ? ncy : 0;
     yy -= (yy >= ncy) ? ncy : 0;
@@ -196,68 +245,142 @@ __device__ __forceinline__ int stencil_vertex(const SysParams& p, int ncx, int n
     xx += (xx < 0) ? ncx : 0;
     xx -= (xx >= ncx) ? ncx : 0;
     const int cc = yy * ncx + xx;
-    kb = n.cell_start[cc];
-    ke = n.cell_start[cc + 1];
-    // entries in groups of four, loaded before any is tested (the last
-    // group re-reads entry ke - 1 in its unused slots and ignores it)
-    for (int k0 = kb; k0 < ke; k0 += 4) {
-      int rj[4];
-      double2 xj[4];
-      double rr[4];
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int k = min(k0 + u, ke - 1);
-        rj[u] = n.cell_ring[k];
-        xj[u] = n.cell_pos[k];
-        rr[u] = n.cell_rad[k];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; u++) {
-        const int k = k0 + u;
-        if (k < ke && rj[u] != ring && is_neighbor(p, xi, xj[u], ri + rr[u], n.cut_distance)) {
-          if (k - kb < 32) hits |= 1u << (k - kb);
-          mine++;
-        }
-      }
-    }
+    sb = n.cell_start[cc];
+    se = n.cell_start[cc + 1];
   }
-  // exclusive scan of the lane counts inside the 16-lane group
-  int incl = mine;
-  for (int o = 1; o < kNbrLanes; o <<= 1) {
-    const int y = __shfl_up_sync(0xffffffffu, incl, o, kNbrLanes);
+  const int len = se - sb;
+  int incl = len;  // inclusive offsets of the nine segments
+  for (int o = 1; o < 16; o <<= 1) {
+    const int y = __shfl_up_sync(kAll, incl, o);
     if (lane >= o) incl += y;
   }
-  const int total = __shfl_sync(0xffffffffu, incl, kNbrLanes - 1, kNbrLanes);
-  int slot = incl - mine;
-  if (valid && lane < 9 && mine > 0) {
-    if (ke - kb <= 32) {
-      while (hits) {
-        const int k = kb + __ffs(hits) - 1;
-        hits &= hits - 1u;
-        if (slot < n.cap) {
-          n.nbr[(size_t)slot * p.nv + g] = ids[k];
-          if (n.nbr_pq) n.nbr_pq[(size_t)slot * p.nv + g] = n.cell_pq[k];
-        }
-        slot++;
-      }
-    } else {
-      for (int k = kb; k < ke; k++) {
-        if (n.cell_ring[k] != ring && is_neighbor(p, xi, n.cell_pos[k], ri + n.cell_rad[k], n.cut_distance)) {
-          if (slot < n.cap) {
-            n.nbr[(size_t)slot * p.nv + g] = ids[k];
-            if (n.nbr_pq) n.nbr_pq[(size_t)slot * p.nv + g] = n.cell_pq[k];
-          }
-          slot++;
-        }
+  const int total = __shfl_sync(kAll, incl, 8);
+  const int off = incl - len;
+  const int hb = __shfl_sync(kAll, sb, 4), he = __shfl_sync(kAll, se, 4);  // the home cell
+  PreTest pt;
+  {
+    const double cw = p.lx / ncx, ch = p.ly / ncy;
+    pt.ox = cx * cw;
+    pt.oy = cy * ch;
+    const float e = (float)(3.0 * fmax(cw, ch) * 0x1p-22);
+    pt.e4 = 4.0f * e;
+    pt.ee4 = 4.0f * e * e;
+    pt.opc = (float)(1.0 + n.cut_distance);
+    pt.on = n.cut_distance > -0.5;
+  }
+  // candidate q of the concatenated stencil list (k = -1 past its end)
+  auto load = [&](int q, int& k, int& rj, float2& xf, float& rf, int& idj, int& pqj) {
+    k = -1;
+    int seg = 0;
+#pragma unroll
+    for (int sg = 0; sg < 9; sg++) {
+      const int o_s = __shfl_sync(kAll, off, sg), b_s = __shfl_sync(kAll, sb, sg), l_s = __shfl_sync(kAll, len, sg);
+      if (q >= o_s && q < o_s + l_s) {
+        k = b_s + (q - o_s);
+        seg = sg;
       }
     }
+    rj = -1;
+    idj = 0;
+    pqj = 0;
+    xf = make_float2(0.0f, 0.0f);
+    rf = 0.0f;
+    if (k >= 0) {
+      const int ux = cx + seg % 3 - 1, uy = cy + seg / 3 - 1;  // unwrapped stencil cell
+      const double sx = ux < 0 ? -p.lx : (ux >= ncx ? p.lx : 0.0);
+      const double sy = uy < 0 ? -p.ly : (uy >= ncy ? p.ly : 0.0);
+      rj = n.cell_ring[k];
+      xf = rel_f(p, pt, n.cell_pos[k], sx, sy);
+      rf = (float)n.cell_rad[k];
+      idj = ids[k];
+      if (n.nbr_pq) pqj = n.cell_pq[k];
+    }
+  };
+  int maxc = 0;
+  for (int h0 = hb; h0 < he; h0 += 32) {
+    const int nh = min(32, he - h0);
+    double2 xh = make_double2(0.0, 0.0);
+    double rh = 0.0;
+    int ringh = -1, gh = 0;
+    // the home vertices and the first 32 candidates are loaded together,
+    // and every later group of 32 while the one before is tested
+    if (lane < nh) {
+      xh = n.cell_pos[h0 + lane];
+      rh = n.cell_rad[h0 + lane];
+      ringh = n.cell_ring[h0 + lane];
+      gh = ids[h0 + lane];
+    }
+    int k, rj, idj, pqj;
+    float2 xf;
+    float rf;
+    load(lane, k, rj, xf, rf, idj, pqj);
+    __syncwarp();  // the previous chunk's readers are done with hs
+    if (lane < nh) {
+      hs.x[lane] = rel_f(p, pt, xh, 0.0, 0.0);
+      hs.r[lane] = (float)rh;
+      hs.ring[lane] = ringh;
+      hs.id[lane] = gh;
+    }
+    __syncwarp();
+    int cnt = 0;  // on lane h: neighbours of home vertex h so far
+    for (int q0 = 0; q0 < total; q0 += 32) {
+      int k2 = -1, rj2 = -1, idj2 = 0, pqj2 = 0;
+      float2 xf2 = make_float2(0.0f, 0.0f);
+      float rf2 = 0.0f;
+      if (q0 + 32 < total) load(q0 + 32 + lane, k2, rj2, xf2, rf2, idj2, pqj2);
+      // four home vertices at a time: their tests are independent
+      for (int h4 = 0; h4 < nh; h4 += 4) {
+        int dec[4];  // 1 neighbour, 0 not, -1 exact test
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int h = min(h4 + u, nh - 1);
+          const float2 xi = hs.x[h];
+          const float dx = xf.x - xi.x, dy = xf.y - xi.y;
+          const float sq = fmaf(dy, dy, dx * dx);
+          const float t = (hs.r[h] + rf) * pt.opc;
+          const float t2 = t * t;
+          const float m = fmaf(1e-5f, t2, fmaf(pt.e4, t, pt.ee4));
+          const int d = !pt.on ? -1 : (sq < t2 - m ? 1 : (sq > t2 + m ? 0 : -1));
+          dec[u] = (k >= 0 && h4 + u < nh && rj != hs.ring[h]) ? d : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          const int h = h4 + u;
+          if (dec[u] < 0) {
+            // inside the band: the reference expression on double positions
+            dec[u] = is_neighbor(p, n.cell_pos[h0 + h], n.cell_pos[k], n.cell_rad[h0 + h] + n.cell_rad[k],
+                                 n.cut_distance) ? 1 : 0;
+          }
+          const bool hit = dec[u] == 1;
+          const unsigned int m = __ballot_sync(kAll, hit);
+          if (m) {
+            const int base = __shfl_sync(kAll, cnt, h & 31);
+            if (hit) {
+              const int g = hs.id[h];
+              const int slot = base + __popc(m & ((1u << lane) - 1u));
+              if (slot < n.cap) {
+                n.nbr[(size_t)slot * p.nv + g] = idj;
+                if (n.nbr_pq) n.nbr_pq[(size_t)slot * p.nv + g] = pqj;
+              }
+            }
+            if (lane == h) cnt += __popc(m);
+          }
+        }
+      }
+      k = k2;
+      rj = rj2;
+      xf = xf2;
+      rf = rf2;
+      idj = idj2;
+      pqj = pqj2;
+    }
+    if (lane < nh) {
+      n.nbr_cnt[gh] = cnt;
+      n.last_pos[gh] = xh;
+      maxc = max(maxc, cnt);
+    }
   }
-  if (valid && lane == 0) {
-    n.nbr_cnt[g] = total;
-    n.last_pos[g] = n.pos[g];
-    return total;
-  }
-  return 0;
+  return maxc;
 }
 
 // CTA-wide maximum of m (every thread calls it); the result on thread 0.
@@ -274,14 +397,14 @@ __device__ __forceinline__ int block_max(int m) {
 
 __global__ void __launch_bounds__(256) k_nbr_cells(const __grid_constant__ SysParams p, int ncx, int ncy,
                                                    const __grid_constant__ NbrArgs n) {
-  const int g = blockIdx.x * (256 / kNbrLanes) + threadIdx.x / kNbrLanes;  // vertex
-  const int lane = threadIdx.x % kNbrLanes;
-  const int m = stencil_vertex(p, ncx, ncy, n, n.cell_vid, g, lane, g < p.nv);
+  __shared__ HomeStage s_home[8];
+  const int c = blockIdx.x * 8 + threadIdx.x / 32;  // home cell of this warp
+  const int m =
+      (c < ncx * ncy) ? stencil_cell(p, ncx, ncy, n, n.cell_vid, c, threadIdx.x & 31, s_home[threadIdx.x / 32]) : 0;
   const int bm = block_max(m);
   publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap);
 }
 
-// Brute force for boxes with fewer than three cells per side.
 __device__ __forceinline__ int brute_vertex(const SysParams& p, const NbrArgs& n, int i) {
   const double2 xi = n.pos[i];
   const double ri = n.rad[i];
@@ -337,7 +460,7 @@ void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g
     k_cell_scan<<<1, 1024, 0, stream>>>(ncells, n.cell_cnt, n.cell_start);
     k_cell_fill<<<nb, 256, 0, stream>>>(p.nv, n.cell_of, n.slot, n.cell_start, n.cell_vid);
     launch_cell_sort(stream, ncells, p.nv, n);
-    k_nbr_cells<<<(p.nv + 256 / kNbrLanes - 1) / (256 / kNbrLanes), 256, 0, stream>>>(p, g.ncx, g.ncy, n);
+    k_nbr_cells<<<(ncells + 7) / 8, 256, 0, stream>>>(p, g.ncx, g.ncy, n);
   } else {
     k_nbr_brute<<<nb, 256, 0, stream>>>(p, n);
   }
@@ -356,7 +479,7 @@ void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g
 //   4 scatter ids by cell                     (k_cell_fill)
 //   5 per vertex: rank in its cell by id, copy to that entry
 //                                             (k_cell_sort + k_cell_gather)
-//   6 stencil search, 16 lanes per vertex     (k_nbr_cells)
+//   6 stencil search, one warp per home cell  (k_nbr_cells)
 // and the last CTA publishes the build exactly as the multi-kernel path does,
 // so both paths produce the same list.  The grid never exceeds the CTAs the
 // GPU holds at once (occupancy x SMs, nbr_fused_max_blocks), so every CTA is
@@ -511,15 +634,11 @@ __global__ void __launch_bounds__(kFusedBlock, kFusedMinBlocks)
     if (n.nbr_pq) n.cell_pq[k] = n.pq_pack[v];
   }
   if (!grid_barrier(st)) return;
-  // 6: stencil search; the loop bound is uniform over a warp (two vertices
-  // per warp) so the 16-lane shuffles see full warps
-  const int lane = threadIdx.x % kNbrLanes, half = (threadIdx.x / kNbrLanes) & 1;
-  const int nwarps = nthreads / 32;
+  // 6: stencil search, one warp per home cell
+  __shared__ HomeStage s_home[kFusedBlock / 32];
   int m = 0;
-  for (int g0 = 2 * (gt / 32); g0 < nv; g0 += 2 * nwarps) {
-    const int g = g0 + half;
-    m = max(m, stencil_vertex(p, ncx, ncy, n, n.slot, g, lane, g < nv));
-  }
+  for (int c = gt / 32; c < ncells; c += nthreads / 32)
+    m = max(m, stencil_cell(p, ncx, ncy, n, n.slot, c, gt & 31, s_home[threadIdx.x / 32]));
   const int bm = block_max(m);
   publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap);
 }
@@ -533,7 +652,7 @@ int nbr_fused_max_blocks() {
 }
 
 int nbr_fused_blocks(int nv, int max_blocks) {
-  const long want = ((long)nv * kNbrLanes + kFusedBlock - 1) / kFusedBlock;
+  const long want = ((long)nv * 4 + kFusedBlock - 1) / kFusedBlock;
   return (int)std::max(1L, std::min<long>(want, max_blocks));
 }
 
