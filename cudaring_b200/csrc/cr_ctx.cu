@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -107,6 +108,22 @@ struct cr_ctx {
   // rigid rings
   double2 *p_vel = nullptr, *p_force = nullptr;
   double *p_angvel = nullptr, *p_torque = nullptr, *p_moi = nullptr, *v_torque = nullptr, *sp_angle = nullptr;
+  // soft-disk pre-packing (allocated on first use)
+  bool soft_ready = false;
+  double* prad = nullptr;       // particle radii
+  double2* plast = nullptr;     // particle positions at the last list build
+  int* pid = nullptr;           // identity: every particle is its own "ring" for the list build
+  int *pnbr = nullptr, *pnbr_cnt = nullptr;
+  int pcap = 0;
+  bool pnbr_built = false;
+  long long plist_size_ref = 0;
+  CellGrid pgrid{0, 0, 0.0, 0.0};
+  DevStatus* pstatus = nullptr;
+  SoftFire* pfire = nullptr;
+  bool pfire_ready = false;
+  double* pdraws = nullptr;     // 2 nv caller-supplied draws for initVerticesOnParticles
+  std::map<long, GraphEntry> soft_graphs;
+  double soft_key[3] = {0.0, 0.0, 0.0};  // cutDistance, cutoff, cells of the captured minimisation graphs
 
   // integrators
   int sim_kind = -1;  // Kind
@@ -145,6 +162,11 @@ void drop_graphs(cr_ctx* ctx) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   ctx->graphs.clear();
+  for (auto& kv : ctx->soft_graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+  }
+  ctx->soft_graphs.clear();
 }
 
 void refresh_params(cr_ctx* ctx) {
@@ -808,7 +830,8 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
                   ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
                   ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec,
-                  ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum};
+                  ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum,
+                  ctx->prad, ctx->plast, ctx->pid, ctx->pnbr, ctx->pnbr_cnt, ctx->pstatus, ctx->pfire, ctx->pdraws};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
@@ -1911,6 +1934,483 @@ extern "C" int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double 
 int cr_get_launch_count(const cr_ctx* ctx, long long* out) {
   if (!ctx || !out) return CR_EINVAL;
   *out = ctx->launches;
+  return CR_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------- soft-disk pre-packing
+// The particle-level stage of compressFIRE.cpp:53-90 (kernels in cr_soft.cu).
+
+static int soft_ensure(cr_ctx* ctx) {
+  if (ctx->soft_ready) return CR_OK;
+  int rc;
+  if ((rc = dalloc(ctx, &ctx->prad, ctx->np)) || (rc = dalloc(ctx, &ctx->plast, ctx->np)) ||
+      (rc = dalloc(ctx, &ctx->pid, ctx->np)) || (rc = dalloc(ctx, &ctx->pnbr_cnt, ctx->np)) ||
+      (rc = dalloc(ctx, &ctx->pnbr, (size_t)16 * ctx->np)) || (rc = dalloc(ctx, &ctx->pstatus, 1)) ||
+      (rc = dalloc(ctx, &ctx->pfire, 1)))
+    return rc;
+  ctx->pcap = 16;
+  std::vector<int> id(ctx->np);
+  for (int i = 0; i < ctx->np; i++) id[i] = i;
+  if ((rc = upload(ctx, ctx->pid, id.data(), id.size() * sizeof(int)))) return rc;
+  ctx->soft_ready = true;
+  return CR_OK;
+}
+
+static int soft_read_status(cr_ctx* ctx, DevStatus* out) { return download(ctx, out, ctx->pstatus, sizeof(DevStatus)); }
+static int soft_clear_status(cr_ctx* ctx) {
+  DevStatus s;
+  int rc = soft_read_status(ctx, &s);
+  if (rc) return rc;
+  s.abort = 0;
+  s.overflow = 0;
+  s.rebuild = 0;
+  s.done_ctr = 0;
+  s.bar_count = 0;
+  s.stalled = 0;
+  return upload(ctx, ctx->pstatus, &s, sizeof(DevStatus));
+}
+
+static SysParams soft_params(cr_ctx* ctx) {
+  SysParams sp = ctx->p;
+  sp.nv = ctx->np;  // list stride and loop bound of the build: one entry per particle
+  return sp;
+}
+
+static double soft_rmax(cr_ctx* ctx, int* rc) {
+  std::vector<double> r(ctx->np);
+  *rc = download(ctx, r.data(), ctx->prad, CR_NP1);
+  double m = 0.0;
+  for (double x : r) m = std::max(m, x);
+  return m;
+}
+
+static NbrArgs soft_nbr_args(cr_ctx* ctx, double cut) {
+  NbrArgs n;
+  n.pos = ctx->ppos;
+  n.rad = ctx->prad;
+  n.ring_of = ctx->pid;
+  n.nbr = ctx->pnbr;
+  n.nbr_cnt = ctx->pnbr_cnt;
+  n.cap = ctx->pcap;
+  n.cut_distance = cut;
+  n.last_pos = ctx->plast;
+  n.cell_of = ctx->cell_of;
+  n.slot = ctx->slot;
+  n.cell_cnt = ctx->cell_cnt;
+  n.cell_start = ctx->cell_start;
+  n.cell_vid = ctx->cell_vid;
+  n.cell_pos = ctx->cell_pos;
+  n.cell_rad = ctx->cell_rad;
+  n.cell_ring = ctx->cell_ring;
+  n.status = ctx->pstatus;
+  n.count_op = 0;
+  n.count_update = 0;
+  n.block_sum = ctx->block_sum;
+  n.self_rsum = 1;
+  return n;
+}
+
+// cells no smaller than (1 + cut) * 2 * max particle radius, as for vertices
+static int soft_setup_grid(cr_ctx* ctx, double cut) {
+  int rc = CR_OK;
+  const double rmax = soft_rmax(ctx, &rc);
+  if (rc) return rc;
+  const double cmin = (1.0 + cut) * 2.0 * rmax * (1.0 + 1e-9);
+  int ncx = cmin > 0 ? (int)std::min(4096.0, std::floor(ctx->p.lx / cmin)) : 0;
+  int ncy = cmin > 0 ? (int)std::min(4096.0, std::floor(ctx->p.ly / cmin)) : 0;
+  if (ncx < 3 || ncy < 3) {
+    ctx->pgrid = CellGrid{0, 0, 0.0, 0.0};
+    return CR_OK;
+  }
+  ctx->pgrid = CellGrid{ncx, ncy, ctx->p.lx / ncx, ctx->p.ly / ncy};
+  if (ncx * ncy > ctx->ncells_alloc) {
+    drop_graphs(ctx);
+    if ((rc = dalloc(ctx, &ctx->cell_cnt, ncx * ncy))) return rc;
+    if ((rc = dalloc(ctx, &ctx->cell_start, ncx * ncy + 1))) return rc;
+    ctx->ncells_alloc = ncx * ncy;
+  }
+  return CR_OK;
+}
+
+// DPM2D::calcParticleNeighborList (DPM2D.cu:3521-3545): the list size only
+// grows, to the next power of two of the largest count.
+static int soft_build(cr_ctx* ctx, double cut) {
+  int rc;
+  if ((rc = soft_setup_grid(ctx, cut))) return rc;
+  for (int pass = 0; pass < 3; pass++) {
+    if ((rc = soft_clear_status(ctx))) return rc;
+    launch_nbr_fused(ctx->stream, soft_params(ctx), ctx->pgrid, soft_nbr_args(ctx, cut),
+                     nbr_fused_blocks(ctx->np, ctx->fused_max), 1);
+    ctx->launches += 1;
+    CR_TRY(cudaGetLastError());
+    DevStatus st;
+    if ((rc = soft_read_status(ctx, &st))) return rc;
+    if (st.stalled) return ctx->fail(CR_ECUDA, "particle list build: a grid barrier timed out");
+    if (!st.overflow) {
+      if (st.max_count > 0) ctx->plist_size_ref = std::max<long long>(ctx->plist_size_ref, pow2ceil(st.max_count));
+      ctx->pnbr_built = true;
+      return soft_clear_status(ctx);
+    }
+    const int newcap = (int)std::max<long long>(16, pow2ceil(2LL * st.max_count));
+    if ((rc = dalloc(ctx, &ctx->pnbr, (size_t)newcap * ctx->np))) return rc;
+    ctx->pcap = newcap;
+    drop_graphs(ctx);
+  }
+  return ctx->fail(CR_ENBR_OVERFLOW, "particle neighbour list kept overflowing");
+}
+
+static SoftArgs soft_args(cr_ctx* ctx, double cutoff) {
+  SoftArgs a;
+  a.pos = ctx->ppos;
+  a.vel = ctx->p_vel;
+  a.force = ctx->p_force;
+  a.energy = ctx->p_energy;
+  a.rad = ctx->prad;
+  a.nbr = ctx->pnbr;
+  a.cnt = ctx->pnbr_built ? ctx->pnbr_cnt : ctx->zero_cnt;
+  a.cap = ctx->pcap;
+  a.last_pos = ctx->plast;
+  a.cutoff = cutoff;
+  a.fire = ctx->pfire;
+  a.status = ctx->pstatus;
+  a.partials = ctx->partials;
+  return a;
+}
+
+extern "C" {
+
+int cr_set_particle_radii(cr_ctx* ctx, const double* rad) {
+  if (!ctx || !rad) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  ctx->pnbr_built = false;
+  return upload(ctx, ctx->prad, rad, CR_NP1);
+}
+int cr_get_particle_radii(const cr_ctx* cctx, double* rad) {
+  cr_ctx* ctx = const_cast<cr_ctx*>(cctx);
+  if (!ctx || !rad) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  return download(ctx, rad, ctx->prad, CR_NP1);
+}
+int cr_get_mean_particle_sigma(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  std::vector<double> r(ctx->np);
+  if ((rc = download(ctx, r.data(), ctx->prad, CR_NP1))) return rc;
+  double s = 0.0;
+  for (double x : r) s += x;
+  *out = s / ctx->np;
+  return CR_OK;
+}
+int cr_get_min_particle_sigma(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  std::vector<double> r(ctx->np);
+  if ((rc = download(ctx, r.data(), ctx->prad, CR_NP1))) return rc;
+  double m = 1.0;  // thrust::reduce with init 1 (DPM2D.cu:766-768)
+  for (double x : r) m = std::min(m, x);
+  *out = m;
+  return CR_OK;
+}
+
+int cr_set_random_particles(cr_ctx* ctx, double phi0, double extraRad, long seed) {
+  if (!ctx || !(phi0 > 0)) return ctx ? ctx->fail(CR_EINVAL, "bad packing fraction") : CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  double phi;
+  if ((rc = cr_get_preferred_phi(ctx, &phi))) return rc;
+  const double scale = std::sqrt(phi / phi0);
+  const double box[2] = {1.0, 1.0};
+  if ((rc = cr_set_box_size(ctx, box))) return rc;
+  std::vector<double> a0(ctx->np), l0(ctx->nv), rad(ctx->nv), pr(ctx->np), pp(2 * (size_t)ctx->np);
+  if ((rc = download(ctx, a0.data(), ctx->a0, CR_NP1)) || (rc = download(ctx, l0.data(), ctx->l0, CR_NV1)) ||
+      (rc = download(ctx, rad.data(), ctx->rad, CR_NV1)))
+    return rc;
+  // the drand48() stream of srand48(seed)
+  unsigned short xs[3] = {0x330E, (unsigned short)(seed & 0xFFFF), (unsigned short)((seed >> 16) & 0xFFFF)};
+  for (int q = 0; q < ctx->np; q++) {
+    a0[q] /= (scale * scale);
+    for (int dim = 0; dim < 2; dim++) pp[2 * (size_t)q + dim] = box[dim] * erand48(xs);
+    const long n = ctx->ring_nv_h[q];
+    pr[q] = extraRad * std::sqrt((2. * a0[q]) / (n * std::sin(2. * kPi / n)));
+  }
+  for (int v = 0; v < ctx->nv; v++) {
+    l0[v] /= scale;
+    rad[v] /= scale;
+  }
+  if ((rc = upload(ctx, ctx->a0, a0.data(), CR_NP1)) || (rc = upload(ctx, ctx->area, a0.data(), CR_NP1)) ||
+      (rc = upload(ctx, ctx->l0, l0.data(), CR_NV1)) || (rc = upload(ctx, ctx->rad, rad.data(), CR_NV1)) ||
+      (rc = upload(ctx, ctx->prad, pr.data(), CR_NP1)) || (rc = upload(ctx, ctx->ppos, pp.data(), 2 * CR_NP1)))
+    return rc;
+  update_rmax(ctx, rad.data());
+  ctx->nbr_built = false;
+  ctx->pnbr_built = false;
+  drop_graphs(ctx);
+  return CR_OK;
+}
+
+int cr_calc_particle_neighbor_list(cr_ctx* ctx, double cutDistance) {
+  if (!ctx || !(cutDistance > -1.0)) return ctx ? ctx->fail(CR_EINVAL, "bad cutDistance") : CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  return soft_build(ctx, cutDistance);
+}
+int cr_get_particle_neighbor_list_size(const cr_ctx* ctx, long* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  *out = (long)ctx->plist_size_ref;
+  return CR_OK;
+}
+int cr_get_particle_max_neighbor_list(const cr_ctx* cctx, long* out) {
+  cr_ctx* ctx = const_cast<cr_ctx*>(cctx);
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  std::vector<int> cnt(ctx->np);
+  if ((rc = download(ctx, cnt.data(), ctx->pnbr_built ? ctx->pnbr_cnt : ctx->zero_cnt, ctx->np * sizeof(int))))
+    return rc;
+  for (int i = 0; i < ctx->np; i++) out[i] = cnt[i];
+  return CR_OK;
+}
+int cr_get_particle_neighbors(const cr_ctx* cctx, long* out) {
+  cr_ctx* ctx = const_cast<cr_ctx*>(cctx);
+  if (!ctx || !out) return CR_EINVAL;
+  const long ls = ctx->plist_size_ref;
+  if (ls == 0 || !ctx->pnbr_built) return CR_OK;
+  std::vector<int> cnt(ctx->np), nb((size_t)ctx->pcap * ctx->np);
+  int rc;
+  if ((rc = download(ctx, cnt.data(), ctx->pnbr_cnt, ctx->np * sizeof(int)))) return rc;
+  if ((rc = download(ctx, nb.data(), ctx->pnbr, nb.size() * sizeof(int)))) return rc;
+  std::vector<int> row;
+  for (int i = 0; i < ctx->np; i++) {
+    row.clear();
+    for (int k = 0; k < std::min(cnt[i], ctx->pcap); k++) row.push_back(nb[(size_t)k * ctx->np + i]);
+    std::sort(row.begin(), row.end());
+    for (long k = 0; k < ls; k++) out[(size_t)i * ls + k] = k < (long)row.size() ? row[k] : -1;
+  }
+  return CR_OK;
+}
+
+int cr_calc_particle_force_energy(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  launch_soft_force(ctx->stream, ctx->potential, ctx->p, soft_args(ctx, 0.0), false);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+int cr_get_particle_potential_energy(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  std::vector<double> e(ctx->np);
+  int rc = download(ctx, e.data(), ctx->p_energy, CR_NP1);
+  if (rc) return rc;
+  double s = 0.0;
+  for (double x : e) s += x;
+  *out = s;
+  return CR_OK;
+}
+int cr_get_particle_max_unbalanced_force(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  std::vector<double> f(2 * (size_t)ctx->np);
+  int rc = download(ctx, f.data(), ctx->p_force, 2 * CR_NP1);
+  if (rc) return rc;
+  double m = -1.0;
+  for (double x : f) m = std::max(m, x * x);
+  *out = std::sqrt(m);
+  return CR_OK;
+}
+int cr_reset_particle_last_positions(cr_ctx* ctx) {
+  if (!ctx) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  CR_TRY(cudaMemcpyAsync(ctx->plast, ctx->ppos, 2 * CR_NP1, cudaMemcpyDeviceToDevice, ctx->stream));
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+int cr_get_particle_max_displacement(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  std::vector<double> x(2 * (size_t)ctx->np), y(2 * (size_t)ctx->np);
+  if ((rc = download(ctx, x.data(), ctx->ppos, 2 * CR_NP1)) || (rc = download(ctx, y.data(), ctx->plast, 2 * CR_NP1)))
+    return rc;
+  double m = -1.0;
+  for (int q = 0; q < ctx->np; q++) {
+    double d2 = 0.0;
+    for (int dim = 0; dim < 2; dim++) {
+      const double L = dim ? ctx->p.ly : ctx->p.lx;
+      double d = x[2 * (size_t)q + dim] - y[2 * (size_t)q + dim];
+      d -= L * std::round(d / L);  // pbcDistance (include/cudaKernel.cuh:70-74)
+      d2 += d * d;
+    }
+    m = std::max(m, std::sqrt(d2));
+  }
+  *out = m;
+  return CR_OK;
+}
+
+int cr_init_particle_fire(cr_ctx* ctx, const double* p7, long minStep, long numStep) {
+  if (!ctx || !p7) return CR_EINVAL;
+  int rc = soft_ensure(ctx);
+  if (rc) return rc;
+  SoftFire f;
+  memset(&f, 0, sizeof(f));
+  f.a_start = p7[0];
+  f.f_dec = p7[1];
+  f.f_inc = p7[2];
+  f.f_a = p7[3];
+  f.dt = p7[4];
+  f.dt_max = p7[5];
+  f.a = p7[6];
+  f.min_step = minStep;
+  f.num_step = numStep;
+  f.tol = -1.0;  // no convergence stop unless a minimisation sets one
+  if ((rc = upload(ctx, ctx->pfire, &f, sizeof(f)))) return rc;
+  ctx->pfire_ready = true;
+  return cr_reset_particle_last_positions(ctx);  // DPM2D::initFIRE (DPM2D.cu:3672)
+}
+int cr_get_particle_fire_state(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  if (!ctx->pfire_ready) return ctx->fail(CR_EINVAL, "particle FIRE not initialised");
+  SoftFire f;
+  int rc = download(ctx, &f, ctx->pfire, sizeof(f));
+  if (rc) return rc;
+  out[0] = f.dt;
+  out[1] = f.a;
+  out[2] = (double)f.num_step;
+  return CR_OK;
+}
+
+// FIRE::minimizerParticleLoop (FIRE.cu:156-171) nsteps times
+int cr_particle_fire_loop(cr_ctx* ctx, long nsteps) {
+  if (!ctx || nsteps < 0) return CR_EINVAL;
+  if (!ctx->pfire_ready) return ctx->fail(CR_EINVAL, "particle FIRE not initialised");
+  int rc;
+  if ((rc = ensure_partials(ctx))) return rc;
+  if (soft_blocks(ctx->np) * 4 > ctx->partials_n) return ctx->fail(CR_EINVAL, "too many particles for the partials");
+  if ((rc = soft_clear_status(ctx))) return rc;
+  SoftFire f;
+  if ((rc = download(ctx, &f, ctx->pfire, sizeof(f)))) return rc;
+  f.converged = 0;
+  f.tol = -1.0;
+  if ((rc = upload(ctx, ctx->pfire, &f, sizeof(f)))) return rc;
+  const SoftArgs a = soft_args(ctx, 0.0);
+  const SysParams sp = soft_params(ctx);
+  for (long s = 0; s < nsteps; s++) {
+    launch_soft_move(ctx->stream, sp, a, 0);
+    launch_soft_force(ctx->stream, ctx->potential, sp, a, true);
+    ctx->launches += 2;
+  }
+  launch_soft_bend(ctx->stream, ctx->np, a);
+  ctx->launches += 1;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  return CR_OK;
+}
+
+// compressFIRE.cpp:66-78: FIRE until max |F_d| <= tol or maxIterations,
+// the particle list rebuilt after an iteration that moved a particle by more
+// than (1 + cutDistance) * getMinParticleSigma / 3 since the last build.  The
+// caller has built the list and computed the forces, as the driver does.
+int cr_particle_fire_minimize(cr_ctx* ctx, double cutDistance, double tol, long maxIterations, long* iterations) {
+  if (!ctx || maxIterations < 0) return CR_EINVAL;
+  if (!ctx->pfire_ready) return ctx->fail(CR_EINVAL, "particle FIRE not initialised");
+  int rc;
+  if ((rc = ensure_partials(ctx))) return rc;
+  if (soft_blocks(ctx->np) * 4 > ctx->partials_n) return ctx->fail(CR_EINVAL, "too many particles for the partials");
+  if (!ctx->pnbr_built && (rc = soft_build(ctx, cutDistance))) return rc;
+  if ((rc = soft_setup_grid(ctx, cutDistance))) return rc;
+  double minsig, fmax;
+  if ((rc = cr_get_min_particle_sigma(ctx, &minsig))) return rc;
+  if ((rc = cr_get_particle_max_unbalanced_force(ctx, &fmax))) return rc;
+  const double cutoff = (1 + cutDistance) * minsig;
+  SoftFire f;
+  if ((rc = download(ctx, &f, ctx->pfire, sizeof(f)))) return rc;
+  const long long it0 = f.iters;
+  f.tol = tol;
+  f.converged = !(fmax > tol) ? 1 : 0;
+  if ((rc = upload(ctx, ctx->pfire, &f, sizeof(f)))) return rc;
+  if ((rc = soft_clear_status(ctx))) return rc;
+  const double key[3] = {cutDistance, cutoff, (double)ctx->pgrid.ncx * 8192.0 + ctx->pgrid.ncy};
+  if (key[0] != ctx->soft_key[0] || key[1] != ctx->soft_key[1] || key[2] != ctx->soft_key[2]) {
+    drop_graphs(ctx);
+    std::copy(key, key + 3, ctx->soft_key);
+  }
+  long done = 0;
+  const long chunk = 64;
+  while (!f.converged && done < maxIterations) {
+    const long n = std::min(chunk, maxIterations - done);
+    auto it = ctx->soft_graphs.find(n);
+    if (it == ctx->soft_graphs.end()) {
+      GraphEntry ge;
+      const SoftArgs a = soft_args(ctx, cutoff);
+      const SysParams sp = soft_params(ctx);
+      const NbrArgs na = soft_nbr_args(ctx, cutDistance);
+      const int fb = nbr_fused_blocks(ctx->np, ctx->fused_max);
+      CR_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      for (long s = 0; s < n; s++) {
+        launch_soft_move(ctx->stream, sp, a, 1);
+        launch_soft_force(ctx->stream, ctx->potential, sp, a, true);
+        launch_nbr_fused(ctx->stream, sp, ctx->pgrid, na, fb, 0);
+      }
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return ctx->fail(CR_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+      }
+      CR_TRY(cudaGraphInstantiate(&ge.exec, g, 0));
+      ge.graph = g;
+      ge.launches = 3 * n;
+      it = ctx->soft_graphs.emplace(n, ge).first;
+    }
+    CR_TRY(cudaGraphLaunch(it->second.exec, ctx->stream));
+    ctx->launches += it->second.launches;
+    DevStatus st;
+    if ((rc = soft_read_status(ctx, &st))) return rc;
+    if ((rc = download(ctx, &f, ctx->pfire, sizeof(f)))) return rc;
+    done = (long)(f.iters - it0);
+    if (st.abort) {
+      if (st.stalled) return ctx->fail(CR_ECUDA, "particle list build: a grid barrier timed out");
+      if (!st.overflow) return ctx->fail(CR_ECUDA, "particle FIRE aborted");
+      // the list outgrew its capacity after iteration `done`: grow, rebuild
+      // from the same positions and carry on
+      if ((rc = soft_clear_status(ctx))) return rc;
+      if ((rc = soft_build(ctx, cutDistance))) return rc;  // regrows and drops the graphs
+    }
+  }
+  launch_soft_bend(ctx->stream, ctx->np, soft_args(ctx, cutoff));
+  ctx->launches += 1;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  if ((rc = download(ctx, &f, ctx->pfire, sizeof(f)))) return rc;
+  if (iterations) *iterations = (long)(f.iters - it0);
+  return CR_OK;
+}
+
+// DPM2D::initVerticesOnParticles (DPM2D.cu:1678-1691).  draws: the 2 nv
+// uniforms on [0, 1) of the jitter (x then y of each vertex, the order of the
+// reference's drand48 calls), or NULL for the context's Philox stream.
+int cr_init_vertices_on_particles(cr_ctx* ctx, const double* draws) {
+  if (!ctx) return CR_EINVAL;
+  int rc;
+  if (draws) {
+    if (!ctx->pdraws && (rc = dalloc(ctx, &ctx->pdraws, 2 * (size_t)ctx->nv))) return rc;
+    if ((rc = upload(ctx, ctx->pdraws, draws, 2 * CR_NV1))) return rc;
+  }
+  launch_soft_vertices(ctx->stream, ctx->nv, ctx->ring_of, ctx->ring_nv, ctx->a0, ctx->l0, ctx->ppos,
+                       draws ? ctx->pdraws : nullptr, ctx->seed, (1ull << 61) + ctx->rng_calls++, ctx->pos[ctx->cur],
+                       ctx->vel, ctx->force, ctx->energy);
+  ctx->launches++;
+  CR_TRY(cudaGetLastError());
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  ctx->nbr_built = false;  // DPM2D::initNeighbors + syncNeighborsToDevice (DPM2D.cu:1689-1690)
   return CR_OK;
 }
 

@@ -124,6 +124,11 @@ struct NbrArgs {
   int count_op;       // 1: the build is one op of a step sequence (ops_done += 1)
   int count_update;   // 1: a displacement-triggered rebuild (DPM2D::updateCount += 1)
   int* block_sum = nullptr;  // [grid] per-CTA cell totals of the one-launch build
+  // 1: the pair's radius sum is twice the listing vertex's own radius (the
+  // particle list rule of kernelCalcParticleNeighborList, whose
+  // extractOtherParticle returns the particle's own radius,
+  // include/cudaKernel.cuh:289-296, 1765-1789)
+  int self_rsum = 0;
 };
 void launch_nbr_build(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n);
 // The whole build in one launch of `blocks` CTAs (at most nbr_fused_max_blocks()).
@@ -135,6 +140,43 @@ void launch_nbr_fused(cudaStream_t st, const SysParams& p, const CellGrid& g, co
 int nbr_fused_max_blocks();
 // Grid of the one-launch build for nv vertices.
 int nbr_fused_blocks(int nv, int max_blocks);
+
+// ------------------------------------------------ soft-disk pre-packing (cr_soft.cu)
+// FIRE scalars of the particle minimiser (FIRE.h:31-42) plus the bend that the
+// last force op computed and the next move op applies.
+struct SoftFire {
+  double dt, dt_max, a, a_start, f_dec, f_inc, f_a;
+  double ratio;    // sqrt(|v|^2 / |F|^2) of the pending bend
+  double tol;      // convergence: max |F_d| <= tol
+  double max_f2;   // max F_d^2 after the last force op
+  long long min_step, num_step, iters;
+  int zero;        // the pending bend zeroes every velocity
+  int pending;     // a bend is waiting
+  int converged;
+  int pad;
+};
+struct SoftArgs {
+  double2* pos;       // particle positions
+  double2* vel;
+  double2* force;
+  double* energy;     // per particle
+  const double* rad;  // particle radii
+  const int* nbr;     // [cap][np] slot-major particle list
+  const int* cnt;
+  int cap;
+  double2* last_pos;  // positions at the last list build
+  double cutoff;      // rebuild when 3 |x - last| > cutoff
+  SoftFire* fire;
+  DevStatus* status;
+  double* partials;   // [blocks][4]
+};
+int soft_blocks(int np);
+void launch_soft_force(cudaStream_t st, int pot, const SysParams& p, const SoftArgs& a, bool fire);
+void launch_soft_move(cudaStream_t st, const SysParams& p, const SoftArgs& a, int check);
+void launch_soft_bend(cudaStream_t st, int np, const SoftArgs& a);
+void launch_soft_vertices(cudaStream_t st, int nv, const int* ring_of, const int* ring_nv, const double* a0,
+                          const double* l0, const double2* ppos, const double* draws, unsigned long long seed,
+                          unsigned long long stream, double2* pos, double2* vel, double2* force, double* energy);
 // building blocks shared with the batched build (cr_batch.cu)
 void launch_cell_scan(cudaStream_t st, int ncells, int* cell_cnt, int* cell_start);
 void launch_cell_sort(cudaStream_t st, int ncells, int nv, const NbrArgs& n);

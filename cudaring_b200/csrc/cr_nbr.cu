@@ -337,7 +337,7 @@ __device__ __forceinline__ int stencil_cell(const SysParams& p, int ncx, int ncy
           const float2 xi = hs.x[h];
           const float dx = xf.x - xi.x, dy = xf.y - xi.y;
           const float sq = fmaf(dy, dy, dx * dx);
-          const float t = (hs.r[h] + rf) * pt.opc;
+          const float t = (hs.r[h] + (n.self_rsum ? hs.r[h] : rf)) * pt.opc;
           const float t2 = t * t;
           const float m = fmaf(1e-5f, t2, fmaf(pt.e4, t, pt.ee4));
           const int d = !pt.on ? -1 : (sq < t2 - m ? 1 : (sq > t2 + m ? 0 : -1));
@@ -348,7 +348,8 @@ __device__ __forceinline__ int stencil_cell(const SysParams& p, int ncx, int ncy
           const int h = h4 + u;
           if (dec[u] < 0) {
             // inside the band: the reference expression on double positions
-            dec[u] = is_neighbor(p, n.cell_pos[h0 + h], n.cell_pos[k], n.cell_rad[h0 + h] + n.cell_rad[k],
+            const double rh = n.cell_rad[h0 + h];
+            dec[u] = is_neighbor(p, n.cell_pos[h0 + h], n.cell_pos[k], rh + (n.self_rsum ? rh : n.cell_rad[k]),
                                  n.cut_distance) ? 1 : 0;
           }
           const bool hit = dec[u] == 1;
@@ -412,7 +413,7 @@ __device__ __forceinline__ int brute_vertex(const SysParams& p, const NbrArgs& n
   int cnt = 0;
   for (int j = 0; j < p.nv; j++) {
     if (n.ring_of[j] == ring) continue;
-    if (is_neighbor(p, xi, n.pos[j], ri + n.rad[j], n.cut_distance)) {
+    if (is_neighbor(p, xi, n.pos[j], ri + (n.self_rsum ? ri : n.rad[j]), n.cut_distance)) {
       if (cnt < n.cap) {
         n.nbr[(size_t)cnt * p.nv + i] = j;
         if (n.nbr_pq) n.nbr_pq[(size_t)cnt * p.nv + i] = n.pq_pack[j];

@@ -84,10 +84,10 @@ __device__ __forceinline__ double dist_of(double2 dl) {
   return sqrt(sq);
 }
 
-// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) -> two standard normals
-// by Box-Muller.  counter = (index, stream), key = seed.
-__device__ __forceinline__ double2 philox_normal2(unsigned long long seed, unsigned long long stream,
-                                                  unsigned long long index) {
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11): four 32-bit words for
+// counter = (index, stream), key = seed.
+__device__ __forceinline__ uint4 philox4x32(unsigned long long seed, unsigned long long stream,
+                                            unsigned long long index) {
   uint32_t c0 = (uint32_t)index, c1 = (uint32_t)(index >> 32), c2 = (uint32_t)stream, c3 = (uint32_t)(stream >> 32);
   uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
 #pragma unroll
@@ -98,6 +98,23 @@ __device__ __forceinline__ double2 philox_normal2(unsigned long long seed, unsig
     c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
     k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
   }
+  return make_uint4(c0, c1, c2, c3);
+}
+
+// Two uniforms on [0, 1) with 53-bit resolution from one Philox block.
+__device__ __forceinline__ double2 philox_uniform2(unsigned long long seed, unsigned long long stream,
+                                                   unsigned long long index) {
+  const uint4 w = philox4x32(seed, stream, index);
+  const unsigned long long a = (unsigned long long)w.x | ((unsigned long long)w.y << 32);
+  const unsigned long long b = (unsigned long long)w.z | ((unsigned long long)w.w << 32);
+  return make_double2((double)(a >> 11) * (1.0 / 9007199254740992.0), (double)(b >> 11) * (1.0 / 9007199254740992.0));
+}
+
+// Two standard normals by Box-Muller from one Philox block.
+__device__ __forceinline__ double2 philox_normal2(unsigned long long seed, unsigned long long stream,
+                                                  unsigned long long index) {
+  const uint4 w = philox4x32(seed, stream, index);
+  const uint32_t c0 = w.x, c1 = w.y, c2 = w.z, c3 = w.w;
   unsigned long long a = (unsigned long long)c0 | ((unsigned long long)c1 << 32);
   unsigned long long b = (unsigned long long)c2 | ((unsigned long long)c3 << 32);
   double u1 = ((double)(a >> 11) + 0.5) * (1.0 / 9007199254740992.0);

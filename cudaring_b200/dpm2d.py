@@ -266,6 +266,89 @@ class DPM2D:
     def getVertexTorques(self): return self._get("cr_get_vertex_torques", self.numVertices)
     def getParticleKineticEnergy(self): return self._scalar("cr_get_particle_kinetic_energy")
 
+    # ------------------------------------------- soft-disk pre-packing
+    # The particle-level stage of compressFIRE.cpp:53-90: soft disks at the
+    # particle positions, FIRE on the disks, vertices placed on the circles.
+    def setParticleRadii(self, a): self._call("cr_set_particle_radii", _f64(a).ctypes.data)
+    def getParticleRadii(self): return self._get("cr_get_particle_radii", self.numParticles)
+    def getMeanParticleSigma(self): return self._scalar("cr_get_mean_particle_sigma")
+    def getMinParticleSigma(self): return self._scalar("cr_get_min_particle_sigma")
+
+    def setRandomParticles(self, phi0, extraRad, seed):
+        """DPM2D::setRandomParticles (src/DPM2D.cu:1601-1629) on the drand48()
+        stream that srand48(seed) starts."""
+        self._call("cr_set_random_particles", float(phi0), float(extraRad), int(seed))
+
+    def calcParticleNeighborList(self, cutDistance): self._call("cr_calc_particle_neighbor_list", float(cutDistance))
+
+    def getParticleNeighborListSize(self):
+        out = C.c_long()
+        self._call("cr_get_particle_neighbor_list_size", C.byref(out))
+        return out.value
+
+    def getParticleNeighbors(self):
+        return self._get("cr_get_particle_neighbors", self.numParticles * self.getParticleNeighborListSize(), np.int64)
+
+    def getParticleMaxNeighborList(self):
+        return self._get("cr_get_particle_max_neighbor_list", self.numParticles, np.int64)
+
+    def calcParticleForceEnergy(self): self._call("cr_calc_particle_force_energy")
+    def getParticlePotentialEnergy(self): return self._scalar("cr_get_particle_potential_energy")
+    def getParticleMaxUnbalancedForce(self): return self._scalar("cr_get_particle_max_unbalanced_force")
+    def resetParticleLastPositions(self): self._call("cr_reset_particle_last_positions")
+    def getParticleMaxDisplacement(self): return self._scalar("cr_get_particle_max_displacement")
+
+    def initParticleFIRE(self, params, minStep=20, numStep=0):
+        """DPM2D::initFIRE + setParticleMassFIRE: params = [a_start, f_dec,
+        f_inc, f_a, dt, dt_max, a]."""
+        p = _f64(params)
+        if p.size != 7:
+            raise ValueError("FIRE takes 7 parameters")
+        self._call("cr_init_particle_fire", p.ctypes.data, int(minStep), int(numStep))
+
+    def getParticleFIREState(self):
+        """(dt, a, numStep) of the particle minimiser."""
+        out = self._get("cr_get_particle_fire_state", 3)
+        return float(out[0]), float(out[1]), int(out[2])
+
+    def particleFIRELoop(self, nsteps=1): self._call("cr_particle_fire_loop", int(nsteps))
+
+    def particleFIREMinimize(self, cutDistance, tol, maxIterations):
+        """The driver loop of compressFIRE.cpp:66-78; returns the iterations."""
+        out = C.c_long()
+        self._call("cr_particle_fire_minimize", float(cutDistance), float(tol), int(maxIterations), C.byref(out))
+        return out.value
+
+    def initVerticesOnParticles(self, draws=None):
+        """DPM2D::initVerticesOnParticles; draws: 2 nv uniforms in the
+        reference's drand48() call order, or None for the context's stream."""
+        if draws is None:
+            self._call("cr_init_vertices_on_particles", None)
+        else:
+            d = _f64(draws)
+            if d.size != 2 * self.numVertices:
+                raise ValueError("draws must hold 2 * numVertices values")
+            self._call("cr_init_vertices_on_particles", d.ctypes.data)
+
+    def softPrepack(self, phi0, extraRad=1.1, seed=1, dt=1e-2, minStep=20, cutDistance=1.0, tol0=1e-10,
+                    maxIterations=5000000, draws=None):
+        """compressFIRE.cpp:53-86 from setRandomParticles to
+        initVerticesOnParticles: random soft disks at phi0, particle FIRE to
+        max |F| < tol0 / meanParticleSigma, vertices on the disk circles.
+        Returns the FIRE iterations."""
+        self.setRandomParticles(phi0, extraRad, seed)
+        sigma = self.getMeanParticleSize()
+        step = 10 * dt * sigma
+        self.setTimeStep(step)
+        self.initParticleFIRE([0.2, 0.5, 1.1, 0.99, step, 10 * step, 0.2], minStep, 0)
+        self.calcParticleNeighborList(cutDistance)
+        self.calcParticleForceEnergy()
+        self.resetParticleLastPositions()
+        tol = tol0 / self.getMeanParticleSigma()
+        it = self.particleFIREMinimize(cutDistance, tol, maxIterations)
+        self.initVerticesOnParticles(draws)
+        return it
+
     def setLanes(self, lanes): self._call("cr_set_lanes", int(lanes))
 
     def getLanes(self):

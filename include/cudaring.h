@@ -245,9 +245,70 @@ int cr_get_vertex_torques(const cr_ctx* ctx, double* out);
 /* DPM2D::getParticleKineticEnergy (include/DPM2D.h:415): 1/2 sum |v_ring|^2 */
 int cr_get_particle_kinetic_energy(cr_ctx* ctx, double* out);
 
+/* ---- soft-disk pre-packing (compressFIRE.cpp:53-90) --------------------- */
+/* The particle-level stage before vertex FIRE: every ring is a soft disk of
+ * radius particleRad at its particle position (cr_set/get_particle_positions),
+ * minimised by FIRE, after which the vertices are placed on circles about the
+ * disk centres.  Forces use the potential set by cr_set_potential_type with
+ * radSum = r_i + r_j; forces, velocities and energies per particle are read
+ * with cr_get_particle_forces / _velocities / _energies. */
+/* DPM2D::setParticleRadii / getParticleRadii (src/DPM2D.cu:814-822) */
+int cr_set_particle_radii(cr_ctx* ctx, const double* particleRad);
+int cr_get_particle_radii(const cr_ctx* ctx, double* particleRad);
+/* DPM2D::getMeanParticleSigma / getMinParticleSigma (src/DPM2D.cu:762-768);
+ * the minimum starts from 1, as the reference's reduction does. */
+int cr_get_mean_particle_sigma(cr_ctx* ctx, double* out);
+int cr_get_min_particle_sigma(cr_ctx* ctx, double* out);
+/* DPM2D::setRandomParticles (src/DPM2D.cu:1601-1629): box 1 x 1, rest areas,
+ * lengths and vertex radii scaled by sqrt(preferred phi / phi0), disk
+ * centres uniform in the box and radii extraRad * sqrt(2 a0 / (nv sin(2 pi / nv))),
+ * drawing from the drand48() stream that srand48(seed) starts. */
+int cr_set_random_particles(cr_ctx* ctx, double phi0, double extraRad, long seed);
+/* DPM2D::calcParticleNeighborList (src/DPM2D.cu:3521-3545): j != i is listed
+ * when -(1 - d_ij / (2 r_i)) < cutDistance (the reference's particle rule
+ * sums the listing particle's own radius twice, include/cudaKernel.cuh:289-296,
+ * 1765-1789).  Size, counts and rows (ascending, -1 padded) as for vertices. */
+int cr_calc_particle_neighbor_list(cr_ctx* ctx, double cutDistance);
+int cr_get_particle_neighbor_list_size(const cr_ctx* ctx, long* out);
+int cr_get_particle_max_neighbor_list(const cr_ctx* ctx, long* partMaxNeighborList);
+int cr_get_particle_neighbors(const cr_ctx* ctx, long* partNeighborList);
+/* DPM2D::calcParticleForceEnergy for the periodic box (src/DPM2D.cu:3611-3622;
+ * kernelCalcParticleInteraction, include/cudaKernel.cuh:1185-1219) */
+int cr_calc_particle_force_energy(cr_ctx* ctx);
+/* DPM2D::getParticlePotentialEnergy / getParticleMaxUnbalancedForce
+ * (src/DPM2D.cu:1097-1099, 3633-3638) */
+int cr_get_particle_potential_energy(cr_ctx* ctx, double* out);
+int cr_get_particle_max_unbalanced_force(cr_ctx* ctx, double* out);
+/* DPM2D::resetParticleLastPositions / getParticleMaxDisplacement
+ * (src/DPM2D.cu:838-840, 1435-1441) */
+int cr_reset_particle_last_positions(cr_ctx* ctx);
+int cr_get_particle_max_displacement(cr_ctx* ctx, double* out);
+/* DPM2D::initFIRE + setParticleMassFIRE (src/DPM2D.cu:3660-3684): p7 =
+ * {a_start, f_dec, f_inc, f_a, dt, dt_max, a}, masses pi / r^2 per particle. */
+int cr_init_particle_fire(cr_ctx* ctx, const double* p7, long minStep, long numStep);
+/* {dt, a, numStep} of the particle minimiser (FIRE.h:31-42) */
+int cr_get_particle_fire_state(cr_ctx* ctx, double* out3);
+/* DPM2D::particleFIRELoop (src/DPM2D.cu:3692-3694; FIRE::minimizerParticleLoop,
+ * src/FIRE.cu:156-171), nsteps iterations; the particle list is not rebuilt. */
+int cr_particle_fire_loop(cr_ctx* ctx, long nsteps);
+/* The driver loop of compressFIRE.cpp:66-78: iterations until max |F_d| <= tol
+ * or maxIterations, the particle list rebuilt (and the last positions reset)
+ * after any iteration in which a particle moved more than
+ * (1 + cutDistance) * getMinParticleSigma / 3 since the last build.  Call it,
+ * as the driver does, after building the list and computing the forces.
+ * Runs on the device in captured chunks of 64 iterations. */
+int cr_particle_fire_minimize(cr_ctx* ctx, double cutDistance, double tol, long maxIterations, long* iterations);
+/* DPM2D::initVerticesOnParticles (src/DPM2D.cu:1678-1691): vertex v of ring q
+ * at R (cos 2 pi v / nv, sin 2 pi v / nv) + particlePos_q + 1e-3 l0_v (u, u'),
+ * R = sqrt(2 a0 / (nv sin(2 pi / nv))), v the global vertex index; velocities,
+ * forces and energies zeroed, the vertex list marked stale.  draws: the 2 nv
+ * uniforms u in the reference's drand48() call order, or NULL for the
+ * context's Philox stream. */
+int cr_init_vertices_on_particles(cr_ctx* ctx, const double* draws);
+
 /* ---- run statistics and measurement ------------------------------------ */
-/* Kernels this context has run since creation (direct launches, graph-node
- * kernels per replay and the rebuild kernels of conditional nodes). */
+/* Kernels this context has run since creation (direct launches and
+ * graph-node kernels per replay). */
 int cr_get_launch_count(const cr_ctx* ctx, long long* out);
 /* The context's CUDA stream (cudaStream_t), for recording timing events. */
 int cr_get_stream(const cr_ctx* ctx, void** out);

@@ -132,6 +132,36 @@ class DPM2D {
   }
   void vertexFIRELoop(long nsteps = 1) { ok(cr_vertex_fire_loop(ctx_, nsteps), "vertexFIRELoop"); }
 
+  // soft-disk pre-packing (compressFIRE.cpp:53-90)
+  void setRandomParticles(double phi0, double extraRad, long seed) {
+    ok(cr_set_random_particles(ctx_, phi0, extraRad, seed), "setRandomParticles");
+  }
+  void calcParticleNeighborList(double cutDistance) {
+    ok(cr_calc_particle_neighbor_list(ctx_, cutDistance), "calcParticleNeighborList");
+  }
+  void calcParticleForceEnergy() { ok(cr_calc_particle_force_energy(ctx_), "calcParticleForceEnergy"); }
+  double getParticlePotentialEnergy() { return scalar(cr_get_particle_potential_energy, "getParticlePotentialEnergy"); }
+  double getParticleMaxUnbalancedForce() {
+    return scalar(cr_get_particle_max_unbalanced_force, "getParticleMaxUnbalancedForce");
+  }
+  double getMeanParticleSigma() { return scalar(cr_get_mean_particle_sigma, "getMeanParticleSigma"); }
+  double getMinParticleSigma() { return scalar(cr_get_min_particle_sigma, "getMinParticleSigma"); }
+  void resetParticleLastPositions() { ok(cr_reset_particle_last_positions(ctx_), "resetParticleLastPositions"); }
+  double getParticleMaxDisplacement() { return scalar(cr_get_particle_max_displacement, "getParticleMaxDisplacement"); }
+  // DPM2D::initFIRE followed by setParticleMassFIRE, for particle FIRE
+  void initParticleFIRE(std::vector<double>& params, long minStep, long numStep) {
+    ok(cr_init_particle_fire(ctx_, params.data(), minStep, numStep), "initParticleFIRE");
+  }
+  void particleFIRELoop(long nsteps = 1) { ok(cr_particle_fire_loop(ctx_, nsteps), "particleFIRELoop"); }
+  long particleFIREMinimize(double cutDistance, double tol, long maxIterations) {
+    long it = 0;
+    ok(cr_particle_fire_minimize(ctx_, cutDistance, tol, maxIterations, &it), "particleFIREMinimize");
+    return it;
+  }
+  void initVerticesOnParticles(const double* draws = nullptr) {
+    ok(cr_init_vertices_on_particles(ctx_, draws), "initVerticesOnParticles");
+  }
+
  private:
   cr_ctx* ctx_ = nullptr;
   void ok(int rc, const char* what) {

@@ -122,6 +122,24 @@ def ref():
         R.ref_fire_loop.argtypes = [C.c_long]
         R.ref_scale_vertices.argtypes = [C.c_double]
         R.ref_rigid_nve_loop.argtypes = [C.c_long]
+        # soft-disk pre-packing
+        R.ref_set_soft_particles.argtypes = [C.c_void_p, C.c_void_p]
+        R.ref_get_particle_radii.argtypes = [_dp]
+        R.ref_get_geometry.argtypes = [_dp]
+        R.ref_calc_particle_neighbor_list.argtypes = [C.c_double]
+        R.ref_particle_neighbor_list_size.restype = C.c_long
+        R.ref_get_particle_neighbors.argtypes = [_lp]
+        R.ref_get_particle_max_neighbor_list.argtypes = [_lp]
+        for fn in ("ref_particle_max_unbalanced_force", "ref_particle_potential_energy",
+                   "ref_particle_max_displacement"):
+            getattr(R, fn).restype = C.c_double
+        R.ref_particle_fire_init.argtypes = [_dp, C.c_long, C.c_long]
+        R.ref_particle_fire_loop.argtypes = [C.c_long]
+        R.ref_particle_fire_minimize.argtypes = [C.c_double, C.c_double, C.c_long]
+        R.ref_particle_fire_minimize.restype = C.c_long
+        R.ref_init_vertices_on_particles.argtypes = [_dp]
+        R.ref_set_random_particles.argtypes = [C.c_double, C.c_double, C.c_long]
+        R.ref_drand48_stream.argtypes = [C.c_long, C.c_long, C.c_long, _dp]
         _REF = R
     return _REF
 

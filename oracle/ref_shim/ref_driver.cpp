@@ -19,6 +19,8 @@
 #include "cudaKernel.cuh"
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <vector>
 #include <omp.h>
 
@@ -55,6 +57,10 @@ struct RefModel {
   // rigid state
   std::vector<double> torque, particleForce, particleTorque, momentOfInertia;
   std::vector<double> particleVel, particleAngle, particleAngvel, particleLastPos, particleLastAngle;
+  // soft-disk pre-packing state: particle radii, list, FIRE masses
+  std::vector<double> particleRad, particleMass;
+  std::vector<long> partNeighborList, partMaxNeighborList;
+  long partNeighborListSize = 0;
 };
 
 RefModel M;
@@ -77,6 +83,9 @@ void sync_symbols() {
   d_neighborListPtr = M.neighborList.data();
   d_maxNeighborListPtr = M.maxNeighborList.data();
   d_neighborListSize = M.neighborListSize;
+  d_partNeighborListPtr = M.partNeighborList.data();
+  d_partMaxNeighborListPtr = M.partMaxNeighborList.data();
+  d_partNeighborListSize = M.partNeighborListSize;
 }
 
 // DPM2D::calcNeighborList (DPM2D.cu:3479-3507): fill, run, grow to the next
@@ -186,6 +195,8 @@ int ref_create(long np, const long* nvList) {
   M.torque.assign(count, 0.0); M.particleForce.assign(2 * np, 0.0); M.particleTorque.assign(np, 0.0);
   M.momentOfInertia.assign(np, 0.0); M.particleVel.assign(2 * np, 0.0); M.particleAngle.assign(np, 0.0);
   M.particleAngvel.assign(np, 0.0); M.particleLastPos.assign(2 * np, 0.0); M.particleLastAngle.assign(np, 0.0);
+  M.particleRad.assign(np, 0.0); M.particleMass.assign(2 * np, 1.0);
+  M.partNeighborList.assign(np, -1L); M.partMaxNeighborList.assign(np, 0L); M.partNeighborListSize = 0;
   M.sc.simulationType = simControlStruct::simulationEnum::gpu;
   M.sc.geometryType = simControlStruct::geometryEnum::normal;
   M.sc.particleType = simControlStruct::particleEnum::passive;
@@ -531,6 +542,209 @@ void ref_rigid_nve_loop(long nsteps) {
       M.particleAngvel[p] += 0.5 * M.dt * M.particleTorque[p];
     }
   }
+}
+
+// ------------------------------------------------------- soft-disk pre-packing
+// The soft-particle stage before vertex FIRE (compressFIRE.cpp:53-90): random
+// disks, particle neighbour list, particle forces, particle FIRE, vertices
+// placed on the particle circles.
+
+void ref_set_soft_particles(const double* pPos, const double* pRad) {
+  if (pPos) std::copy(pPos, pPos + 2 * M.np, M.particlePos.begin());
+  if (pRad) std::copy(pRad, pRad + M.np, M.particleRad.begin());
+}
+
+void ref_get_particle_radii(double* out) { std::copy(M.particleRad.begin(), M.particleRad.end(), out); }
+void ref_get_geometry(double* out) {  // a0[np], l0[nv], rad[nv], box[2]
+  std::copy(M.a0.begin(), M.a0.end(), out);
+  std::copy(M.l0.begin(), M.l0.end(), out + M.np);
+  std::copy(M.rad.begin(), M.rad.end(), out + M.np + M.nv);
+  out[M.np + 2 * M.nv] = M.boxSize[0];
+  out[M.np + 2 * M.nv + 1] = M.boxSize[1];
+}
+
+// DPM2D::calcParticleNeighborList (DPM2D.cu:3521-3545)
+void ref_calc_particle_neighbor_list(double cutDistance) {
+  std::fill(M.partMaxNeighborList.begin(), M.partMaxNeighborList.end(), 0L);
+  std::fill(M.partNeighborList.begin(), M.partNeighborList.end(), -1L);
+  sync_symbols();
+  REF_RUN(M.np, kernelCalcParticleNeighborList(M.particlePos.data(), M.particleRad.data(), cutDistance));
+  long maxNeighbors = -1;
+  for (long p = 0; p < M.np; p++) maxNeighbors = std::max(maxNeighbors, M.partMaxNeighborList[p]);
+  if (maxNeighbors > M.partNeighborListSize) {
+    M.partNeighborListSize = (long)std::pow(2, std::ceil(std::log2((double)maxNeighbors)));
+    M.partNeighborList.assign(M.np * M.partNeighborListSize, -1L);
+    sync_symbols();
+    REF_RUN(M.np, kernelCalcParticleNeighborList(M.particlePos.data(), M.particleRad.data(), cutDistance));
+  }
+}
+long ref_particle_neighbor_list_size(void) { return M.partNeighborListSize; }
+void ref_get_particle_neighbors(long* out) { std::copy(M.partNeighborList.begin(), M.partNeighborList.end(), out); }
+void ref_get_particle_max_neighbor_list(long* out) {
+  std::copy(M.partMaxNeighborList.begin(), M.partMaxNeighborList.end(), out);
+}
+
+// DPM2D::calcParticleForceEnergy for periodic geometry (DPM2D.cu:3611-3622, 3582-3588)
+void ref_calc_particle_force_energy(void) {
+  sync_symbols();
+  REF_RUN(M.np, kernelCalcParticleInteraction(M.particleRad.data(), M.particlePos.data(), M.particleForce.data(),
+                                              M.particleEnergy.data()));
+}
+
+// DPM2D::getParticleMaxUnbalancedForce (DPM2D.cu:3633-3638)
+double ref_particle_max_unbalanced_force(void) {
+  double m = -1;
+  for (double f : M.particleForce) m = std::max(m, f * f);
+  return std::sqrt(m);
+}
+double ref_particle_potential_energy(void) {
+  double e = 0;
+  for (double x : M.particleEnergy) e += x;
+  return e;
+}
+void ref_reset_particle_last_positions(void) { M.particleLastPos = M.particlePos; }
+// DPM2D::getParticleMaxDisplacement (DPM2D.cu:1435-1441)
+double ref_particle_max_displacement(void) {
+  sync_symbols();
+  std::vector<double> disp(M.np, 0.0);
+  REF_RUN(M.np, kernelCalcParticleDisplacement(M.particlePos.data(), M.particleLastPos.data(), disp.data()));
+  double m = -1;
+  for (double d : disp) m = std::max(m, d);
+  return m;
+}
+
+// DPM2D::initFIRE (DPM2D.cu:3660-3674) + DPM2D::setParticleMassFIRE (:3676-3684)
+void ref_particle_fire_init(const double* p7, long minStep, long numStep) {
+  ref_fire_init(p7, minStep, numStep);
+  M.particleLastPos = M.particlePos;
+  for (long p = 0; p < M.np; p++)
+    for (long dim = 0; dim < 2; dim++) M.particleMass[p * 2 + dim] = PI / (M.particleRad[p] * M.particleRad[p]);
+}
+
+// FIRE::minimizerParticleLoop (FIRE.cu:156-171) repeated nsteps times, with
+// FIRE::updateParticlePositionAndVelocity (:45-71), updateParticleVelocity
+// (:74-97) and bendParticleVelocityTowardsForce (:100-141).  The reference's
+// checkParticleNeighbors call inside the loop rebuilds the *vertex* list
+// (DPM2D.cu:1425-1433), which no particle force reads; it is left out.
+void ref_particle_fire_loop(long nsteps) {
+  const long n2 = 2 * M.np;
+  for (long s = 0; s < nsteps; s++) {
+    for (long p = 0; p < M.np; p++) {
+      double totalForce = 0;
+      for (long dim = 0; dim < 2; dim++) {
+        const long i = p * 2 + dim;
+        M.particleVel[i] += 0.5 * M.fire_dt * M.particleForce[i] / M.particleMass[i];
+        M.particlePos[i] += M.fire_dt * M.particleVel[i];
+        totalForce += M.particleForce[i];
+      }
+      if (totalForce == 0)
+        for (long dim = 0; dim < 2; dim++) M.particleVel[p * 2 + dim] = 0;
+    }
+    ref_calc_particle_force_energy();
+    for (long p = 0; p < M.np; p++) {
+      double totalForce = 0;
+      for (long dim = 0; dim < 2; dim++) {
+        const long i = p * 2 + dim;
+        M.particleVel[i] += 0.5 * M.fire_dt * M.particleForce[i] / M.particleMass[i];
+        totalForce += M.particleForce[i];
+      }
+      if (totalForce == 0)
+        for (long dim = 0; dim < 2; dim++) M.particleVel[p * 2 + dim] = 0;
+    }
+    double vDotF = 0;
+    for (long i = 0; i < n2; i++) vDotF += M.particleVel[i] * M.particleForce[i];
+    if (vDotF < 0) {
+      std::fill(M.particleVel.begin(), M.particleVel.end(), 0.0);
+      M.numStep = 0;
+      M.fire_dt = std::max(M.fire_dt * M.f_dec, M.fire_dt_max / 10);
+      M.fire_a = M.a_start;
+    } else if (M.numStep > M.minStep) {
+      M.fire_dt = std::min(M.fire_dt * M.f_inc, M.fire_dt_max);
+      M.fire_a *= M.f_a;
+    }
+    double vv = 0, ff = 0;
+    for (long i = 0; i < n2; i++) { vv += M.particleVel[i] * M.particleVel[i]; ff += M.particleForce[i] * M.particleForce[i]; }
+    if (ff == 0) {
+      std::fill(M.particleVel.begin(), M.particleVel.end(), 0.0);
+    } else {
+      const double ratio = std::sqrt(vv / ff);
+      const double a = M.fire_a;
+      for (long i = 0; i < n2; i++) M.particleVel[i] = (1 - a) * M.particleVel[i] + a * M.particleForce[i] * ratio;
+    }
+    M.numStep++;
+  }
+}
+
+// compressFIRE.cpp:66-78: particle FIRE to max |F| <= tol, the particle list
+// rebuilt whenever 3 * (largest displacement since the last build) exceeds
+// (1 + cutDistance) * (smallest particle radius).  Returns the iterations.
+long ref_particle_fire_minimize(double cutDistance, double tol, long maxIterations) {
+  double minRad = 1.0;  // DPM2D::getMinParticleSigma (DPM2D.cu:766-768)
+  for (double r : M.particleRad) minRad = std::min(minRad, r);
+  const double cutoff = (1 + cutDistance) * minRad;
+  long iteration = 0;
+  while (ref_particle_max_unbalanced_force() > tol && iteration != maxIterations) {
+    ref_particle_fire_loop(1);
+    if (3 * ref_particle_max_displacement() > cutoff) {
+      ref_calc_particle_neighbor_list(cutDistance);
+      M.particleLastPos = M.particlePos;
+    }
+    iteration += 1;
+  }
+  return iteration;
+}
+
+// DPM2D::initVerticesOnParticles (DPM2D.cu:1678-1691) with the 2 * nv
+// drand48() draws supplied in call order (x then y of each vertex).
+void ref_init_vertices_on_particles(const double* draws) {
+  for (long v = 0; v < M.nv; v++) {
+    const long p = M.particleId[v];
+    const long n = M.nvList[p];
+    const double rad = std::sqrt((2. * M.a0[p]) / (n * std::sin(2. * PI / n)));
+    M.pos[v * 2] = rad * std::cos((2. * PI * v) / n) + M.particlePos[p * 2] + 1e-03 * M.l0[v] * draws[2 * v];
+    M.pos[v * 2 + 1] = rad * std::sin((2. * PI * v) / n) + M.particlePos[p * 2 + 1] + 1e-03 * M.l0[v] * draws[2 * v + 1];
+  }
+  std::fill(M.vel.begin(), M.vel.end(), 0.0);
+  std::fill(M.force.begin(), M.force.end(), 0.0);
+  std::fill(M.energy.begin(), M.energy.end(), 0.0);
+}
+
+// DPM2D::getPreferredPhi (DPM2D.cu:1222-1238) for the periodic box.
+static double preferred_phi(void) {
+  double phi = 0;
+  for (double a : M.a0) phi += a;
+  std::vector<double> vertexArea(M.np, 0.0);
+  sync_symbols();
+  REF_RUN(M.np, kernelCalcVertexArea(M.rad.data(), vertexArea.data()));
+  double va = 0;
+  for (double x : vertexArea) va += x;
+  phi += PI * va;
+  return phi / (M.boxSize[0] * M.boxSize[1]);
+}
+
+// DPM2D::setRandomParticles (DPM2D.cu:1601-1629) with the drand48() stream
+// of srand48(seed): erand48 on the state srand48 would set.
+void ref_set_random_particles(double phi0, double extraRad, long seed) {
+  unsigned short xs[3] = {0x330E, (unsigned short)(seed & 0xFFFF), (unsigned short)((seed >> 16) & 0xFFFF)};
+  const double scale = std::sqrt(preferred_phi() / phi0);
+  M.boxSize = {1.0, 1.0};
+  for (long p = 0; p < M.np; p++) {
+    M.a0[p] /= (scale * scale);
+    M.area[p] = M.a0[p];
+    for (long dim = 0; dim < 2; dim++) M.particlePos[p * 2 + dim] = M.boxSize[dim] * erand48(xs);
+    M.particleRad[p] = extraRad * std::sqrt((2. * M.a0[p]) / (M.nvList[p] * std::sin(2. * PI / M.nvList[p])));
+  }
+  for (long v = 0; v < M.nv; v++) {
+    M.l0[v] /= scale;
+    M.rad[v] /= scale;
+  }
+}
+
+// the drand48() draws that follow n earlier ones on srand48(seed)
+void ref_drand48_stream(long seed, long skip, long n, double* out) {
+  unsigned short xs[3] = {0x330E, (unsigned short)(seed & 0xFFFF), (unsigned short)((seed >> 16) & 0xFFFF)};
+  for (long i = 0; i < skip; i++) erand48(xs);
+  for (long i = 0; i < n; i++) out[i] = erand48(xs);
 }
 
 }  // extern "C"

@@ -321,10 +321,90 @@ def rescale_cases():
     print(f"traj_nverescale_harmonic_vv: updates={int(d['out_update_count'])}")
 
 
+def soft_cases():
+    # Soft-disk pre-packing (compressFIRE.cpp:53-90) from a unit box, as the
+    # reference driver starts: setRandomParticles, the particle list, forces,
+    # 10 FIRE iterations, the full FIRE minimisation and initVerticesOnParticles.
+    cases = [("harmonic", 0, 1.0, 0.8, dict(), True), ("wca", 3, 1.0, 0.35, dict(), False),
+             ("lj", 1, 3.0, 0.35, dict(lj=2.5), False)]
+    for name, pot, cut, phi0, extra, full in cases:
+        pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 301)
+        extra_rad, seed = 1.1, 4242
+        R = oracle.ref()
+        R.ref_create(pk.num_particles, pk.nv_list)
+        R.ref_set_box(1.0, 1.0)
+        R.ref_set_types(pot, 0, 0, 0)
+        R.ref_set_energy_costs(1.0, 1.0, 0.01, 1.0)
+        R.ref_set_lj_cutoff(extra.get("lj", 2.5))
+        R.ref_set_state(pk.pos.ctypes.data, pk.vel.ctypes.data, pk.rad.ctypes.data, pk.l0.ctypes.data,
+                        pk.theta0.ctypes.data, pk.a0.ctypes.data)
+        R.ref_set_random_particles(phi0, extra_rad, seed)
+        n_p, n_v = pk.num_particles, pk.num_vertices
+        geo = np.zeros(n_p + 2 * n_v + 2)
+        R.ref_get_geometry(geo)
+        d = dict(in_nv_list=np.asarray(pk.nv_list), in_a0=pk.a0, in_l0=pk.l0, in_rad=pk.rad, in_theta0=pk.theta0,
+                 in_pos=pk.pos, param_potential=np.asarray(pot), param_lj_cutoff=np.asarray(extra.get("lj", 2.5)),
+                 param_phi0=np.asarray(phi0), param_extra_rad=np.asarray(extra_rad), param_seed=np.asarray(seed),
+                 param_cut=np.asarray(cut))
+        d["out_a0"], d["out_l0"], d["out_rad"] = geo[:n_p], geo[n_p:n_p + n_v], geo[n_p + n_v:n_p + 2 * n_v]
+        d["out_box"] = geo[-2:]
+        d["out_ppos"] = np.zeros(2 * n_p)
+        R.ref_get(9, d["out_ppos"])
+        d["out_prad"] = np.zeros(n_p)
+        R.ref_get_particle_radii(d["out_prad"])
+        R.ref_calc_particle_neighbor_list(cut)
+        ls = R.ref_particle_neighbor_list_size()
+        d["out_plist_size"] = np.asarray(ls)
+        d["out_pneighbors"] = np.zeros(n_p * ls, dtype=np.int64)
+        R.ref_get_particle_neighbors(d["out_pneighbors"])
+        d["out_pmax"] = np.zeros(n_p, dtype=np.int64)
+        R.ref_get_particle_max_neighbor_list(d["out_pmax"])
+        R.ref_calc_particle_force_energy()
+        d["out_pforce"], d["out_penergy"] = np.zeros(2 * n_p), np.zeros(n_p)
+        R.ref_get(12, d["out_pforce"])
+        R.ref_get(4, d["out_penergy"])
+        # FIRE as compressFIRE.cpp:58-65 sets it up: dt = 10 * 1e-2 * mean particle size
+        sigma = 2 * np.sqrt(d["out_a0"].sum() / (np.pi * n_p))
+        step = 10 * 1e-2 * sigma
+        p7 = np.array([0.2, 0.5, 1.1, 0.99, step, 10 * step, 0.2])
+        d["param_fire"] = p7
+        d["param_min_step"] = np.asarray(20)
+        R.ref_particle_fire_init(p7, 20, 0)
+        R.ref_particle_fire_loop(10)
+        d["out_fire10_ppos"], d["out_fire10_pvel"] = np.zeros(2 * n_p), np.zeros(2 * n_p)
+        R.ref_get(9, d["out_fire10_ppos"])
+        R.ref_get(16, d["out_fire10_pvel"])
+        d["out_fire10_state"] = np.zeros(3)
+        R.ref_fire_state(d["out_fire10_state"])
+        if full:
+            # restart from the random state for the driver loop
+            R.ref_set_soft_particles(d["out_ppos"].ctypes.data, d["out_prad"].ctypes.data)
+            R.ref_set_particle_state(None, np.zeros(2 * n_p).ctypes.data, None, None)
+            R.ref_calc_particle_neighbor_list(cut)
+            R.ref_calc_particle_force_energy()
+            R.ref_particle_fire_init(p7, 20, 0)
+            tol = 1e-10 / d["out_prad"].mean()
+            d["param_tol"] = np.asarray(tol)
+            d["out_min_iters"] = np.asarray(R.ref_particle_fire_minimize(cut, tol, 1000000))
+            d["out_min_ppos"] = np.zeros(2 * n_p)
+            R.ref_get(9, d["out_min_ppos"])
+            d["out_min_maxf"] = np.asarray(R.ref_particle_max_unbalanced_force())
+            d["out_min_pe"] = np.asarray(R.ref_particle_potential_energy())
+            draws = np.zeros(2 * n_v)
+            R.ref_drand48_stream(7, 0, 2 * n_v, draws)
+            d["in_draws"] = draws
+            R.ref_init_vertices_on_particles(draws)
+            d["out_vpos"] = np.zeros(2 * n_v)
+            R.ref_get(0, d["out_vpos"])
+        np.savez_compressed(os.path.join(OUT, f"soft_{name}.npz"), **d)
+        print(f"soft_{name}: np={n_p} list={ls} maxF={np.abs(d['out_pforce']).max():.3e}"
+              + (f" iters={int(d['out_min_iters'])}" if full else ""))
+
+
 if __name__ == "__main__":
     if not oracle.ref_available():
         oracle.build()
-    which = sys.argv[1:] or ["force", "traj", "stochastic", "rigid", "rescale"]
+    which = sys.argv[1:] or ["force", "traj", "stochastic", "rigid", "rescale", "soft"]
     if "force" in which:
         force_cases()
     if "traj" in which:
@@ -335,3 +415,5 @@ if __name__ == "__main__":
         rigid_cases()
     if "rescale" in which:
         rescale_cases()
+    if "soft" in which:
+        soft_cases()
