@@ -28,10 +28,12 @@ enum Prec : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 
 // Occupancy target in threads per SM: 512 leaves 128 registers per thread,
 // where the FP64 smooth-interaction body compiles without spills; the mixed
-// body fits 96 registers (640 threads, five 128-thread CTAs per SM).
-template <int PREC>
+// body fits 96 registers (640 threads, five 128-thread CTAs per SM) with one
+// lane per vertex and 80 with two or more (768 threads), so that the twice as
+// many CTAs of two lanes per vertex still run as one wave.
+template <int PREC, int L = 1>
 constexpr int tile_threads_per_sm() {
-  return PREC == PREC_MIXED ? 640 : 512;
+  return PREC == PREC_MIXED ? (L >= 2 ? 768 : 640) : 512;
 }
 
 template <typename T2> __device__ __forceinline__ T2 cvt2(double2 d);
@@ -69,7 +71,7 @@ __device__ __forceinline__ void tile_skip(const StepArgs& s, DevStatus* st) {
 // the system, whose box, displacement cutoff, FIRE scalars and flags come
 // from s.bsys, and whose last tile reduces the system's partial sums.
 template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH = false>
-__global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC>() / BLOCK) k_tile(const __grid_constant__ SysParams p,
+__global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK) k_tile(const __grid_constant__ SysParams p,
                                                 const __grid_constant__ SysArrays a,
                                                 const __grid_constant__ StepArgs s) {
   constexpr int TV = BLOCK / L;
