@@ -507,7 +507,7 @@ int inter_kind(const cr_batch* b) {
                                                                                                   : INT_SMOOTH;
 }
 
-int tile_capacity(int lanes) { return lanes >= 4 ? 256 / lanes : 128 / lanes; }
+int tile_capacity(int lanes) { return tile_vertices(lanes); }  // the single-system tiles' capacity
 
 // Tiles of whole rings that never cross a system.
 void make_tiles(cr_batch* b) {

@@ -358,7 +358,7 @@ static void launch_rigid_t(const LaunchCfg& c, const SysParams& p, const SysArra
   if (c.lanes == 1) k_rigid<POT, MODE, 128, 1><<<c.grid, 128, 0, c.stream>>>(p, a, s, r);
   else if (c.lanes == 4) k_rigid<POT, MODE, 256, 4><<<c.grid, 256, 0, c.stream>>>(p, a, s, r);
   else if (c.lanes == 8) k_rigid<POT, MODE, 256, 8><<<c.grid, 256, 0, c.stream>>>(p, a, s, r);
-  else k_rigid<POT, MODE, 128, 2><<<c.grid, 128, 0, c.stream>>>(p, a, s, r);
+  else k_rigid<POT, MODE, 192, 2><<<c.grid, 192, 0, c.stream>>>(p, a, s, r);  // tiles of up to 96 vertices
 }
 
 void launch_rigid(const LaunchCfg& c, int pot, int mode, const SysParams& p, const SysArrays& a, const StepArgs& s,

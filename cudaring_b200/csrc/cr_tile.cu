@@ -10,7 +10,7 @@ static void launch_tile_t(const LaunchCfg& c, const SysParams& p, const SysArray
   if (c.lanes == 1) k_tile<POT, INTER, MODE, 128, 1, PREC_FP64><<<c.grid, 128, 0, c.stream>>>(p, a, s);
   else if (c.lanes == 4) k_tile<POT, INTER, MODE, 256, 4, PREC_FP64><<<c.grid, 256, 0, c.stream>>>(p, a, s);
   else if (c.lanes == 8) k_tile<POT, INTER, MODE, 256, 8, PREC_FP64><<<c.grid, 256, 0, c.stream>>>(p, a, s);
-  else k_tile<POT, INTER, MODE, 128, 2, PREC_FP64><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+  else k_tile<POT, INTER, MODE, 192, 2, PREC_FP64><<<c.grid, 192, 0, c.stream>>>(p, a, s);
 }
 
 void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p_in, const SysArrays& a,
@@ -42,7 +42,7 @@ void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysPara
 }
 
 // Tile capacity (vertices of whole rings per CTA) for a lane count:
-// 1 -> 128 threads x 1, 2 -> 128 x 2, 4 -> 256 x 4, 8 -> 256 x 8.
-int tile_vertices(int lanes) { return lanes >= 4 ? 256 / lanes : 128 / (lanes <= 0 ? 2 : lanes); }
+// 1 -> 128 threads x 1, 2 -> 192 x 2, 4 -> 256 x 4, 8 -> 256 x 8.
+int tile_vertices(int lanes) { return lanes >= 4 ? 256 / lanes : (lanes == 2 ? 96 : 128); }
 
 }  // namespace cr

@@ -9,7 +9,7 @@ template <int POT, int INTER, int MODE, int PREC>
 static void launch_batch_t(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s) {
   if (c.lanes == 1) k_tile<POT, INTER, MODE, 128, 1, PREC, true><<<c.grid, 128, 0, c.stream>>>(p, a, s);
   else if (c.lanes == 4) k_tile<POT, INTER, MODE, 256, 4, PREC, true><<<c.grid, 256, 0, c.stream>>>(p, a, s);
-  else k_tile<POT, INTER, MODE, 128, 2, PREC, true><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+  else k_tile<POT, INTER, MODE, 192, 2, PREC, true><<<c.grid, 192, 0, c.stream>>>(p, a, s);
 }
 
 template <int PREC>

@@ -26,14 +26,16 @@ namespace cr {
 
 enum Prec : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 
-// Occupancy target in threads per SM: 512 leaves 128 registers per thread,
-// where the FP64 smooth-interaction body compiles without spills; the mixed
-// body fits 96 registers (640 threads, five 128-thread CTAs per SM) with one
-// lane per vertex and 80 with two or more (768 threads), so that the twice as
-// many CTAs of two lanes per vertex still run as one wave.
+// Occupancy target in threads per SM.  One lane per vertex: 512 leaves 128
+// registers per thread, where the FP64 smooth-interaction body compiles
+// without spills, and the mixed body fits 96 (640 threads).  Two lanes per
+// vertex (192-thread CTAs, tiles of up to 96 vertices): 576 threads (three
+// CTAs, 112 registers) for FP64 and 768 (four CTAs, 80 registers) for mixed,
+// so that the grid of a 39,424-vertex system (about 430 tiles) runs as one
+// wave; four or more lanes: 768 for mixed.
 template <int PREC, int L = 1>
 constexpr int tile_threads_per_sm() {
-  return PREC == PREC_MIXED ? (L >= 2 ? 768 : 640) : 512;
+  return PREC == PREC_MIXED ? (L >= 2 ? 768 : 640) : (L == 2 ? 576 : 512);
 }
 
 template <typename T2> __device__ __forceinline__ T2 cvt2(double2 d);

@@ -11,7 +11,7 @@ static void launch_mixed_t(const LaunchCfg& c, const SysParams& p, const SysArra
   if (c.lanes == 1) k_tile<POT, INTER, MODE, 128, 1, PREC_MIXED><<<c.grid, 128, 0, c.stream>>>(p, a, s);
   else if (c.lanes == 4) k_tile<POT, INTER, MODE, 256, 4, PREC_MIXED><<<c.grid, 256, 0, c.stream>>>(p, a, s);
   else if (c.lanes == 8) k_tile<POT, INTER, MODE, 256, 8, PREC_MIXED><<<c.grid, 256, 0, c.stream>>>(p, a, s);
-  else k_tile<POT, INTER, MODE, 128, 2, PREC_MIXED><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+  else k_tile<POT, INTER, MODE, 192, 2, PREC_MIXED><<<c.grid, 192, 0, c.stream>>>(p, a, s);
 }
 
 void launch_tile_mixed(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
