@@ -1740,8 +1740,6 @@ int cr_set_use_graphs(cr_ctx* ctx, int on) {
 
 static int diff_ready(cr_ctx* ctx) {
   if (ctx->shape == CR_SHAPE_RIGID) return ctx->fail(CR_ENOTSUP, "derivatives are for deformable rings");
-  if (inter_kind(ctx) != INT_VV) return ctx->fail(CR_ENOTSUP, "derivatives cover the vertex-vertex interaction");
-  if (ctx->monomer != CR_MONOMER_HARMONIC) return ctx->fail(CR_ENOTSUP, "derivatives cover harmonic monomers");
   int rc;
   if (!ctx->nbr_built && (rc = build_list(ctx, ctx->cur, ctx->cut_distance))) return rc;
   if (!ctx->diff_f) {
@@ -1771,7 +1769,7 @@ static DiffArgs diff_args(cr_ctx* ctx) {
 }
 
 static int diff_launch(cr_ctx* ctx, const DiffArgs& g) {
-  launch_diff(ctx->stream, ctx->potential, g);
+  launch_diff(ctx->stream, ctx->potential, inter_kind(ctx), g);
   ctx->launches++;
   CR_TRY(cudaGetLastError());
   return CR_OK;

@@ -4,9 +4,10 @@
 //
 // One thread per vertex evaluates the same per-vertex force and energy as the
 // fused kernel (shape terms of kernelCalcShapeForceEnergy,
-// include/cudaKernel.cuh:474-529, harmonic monomers, and the vertex-vertex
-// pair terms of kernelCalcVertexInteraction, :690-722) with every input a
-// hyper-dual number: positions x + t1 e1 + t2 e2, box L (1 + s1 e1 + s2 e2),
+// include/cudaKernel.cuh:474-529, with harmonic or FENE monomers, and the pair
+// terms: vertex-vertex, kernelCalcVertexInteraction :690-722, or smooth
+// vertex-segment, kernelCalcSmoothInteraction :922-975, in the gather form of
+// the fused kernel) with every input a hyper-dual number: positions x + t1 e1 + t2 e2, box L (1 + s1 e1 + s2 e2),
 // and the shape constants and rest lengths / radii along parameter tangents.
 // The e1 part of the force is then D_t1 F = -H t1 (the Hessian-vector
 // product), the e1 part of the energy along the affine dilation t1 = x,
@@ -99,7 +100,74 @@ __device__ __forceinline__ HD norm(const HD2& a) { return hsqrt(dot(a, a)); }
 // calcAngle(nextSegment, previousSegment) (include/cudaKernel.cuh:423-427)
 __device__ __forceinline__ HD angle(const HD2& ns, const HD2& ps) { return hatan2(cross(ns, ps), dot(ns, ps)); }
 
-template <int POT>
+// One smooth unit (calcGradMultipleAndEnergy / calcVertexSegmentInteraction /
+// calcVertexVertexInteraction, include/cudaKernel.cuh:806-912): vertex t
+// against the segment q -> o, with tq = t - q, w = t - o, seg = o - q and
+// pseg = q - qq.  WHO = 1 adds the force on t, 2 the force on o, 3 the force
+// on q; the unit energy is booked for WHO 1 and 2 (each unit is evaluated
+// once in each role, as the fused kernel gathers it).  The branches are taken
+// on the real parts.
+template <int POT, int WHO>
+__device__ void smooth_hd(const DiffArgs& g, const HD2& tq, const HD2& w, const HD2& seg, const HD2& pseg,
+                          const HD& rsum, HD2& f, HD& e) {
+  const HD len2 = dot(seg, seg);
+  const HD inv_len = 1.0 / hsqrt(len2);
+  const HD inv_lsq = inv_len * inv_len;
+  const HD proj = dot(tq, seg) * inv_lsq;
+  const HD pc = dot(tq, pseg);
+  const HD pl2 = dot(pseg, pseg);
+  auto corner = [&](double sgn) {  // sgn +1: convex (added), -1: concave (removed)
+    const HD d2 = norm(tq);
+    HD g2, ep2;
+    if (pair_hd<POT>(g, d2, rsum, g2, ep2) && g2.a != 0.0) {
+      const HD s2 = g2 / d2;
+      if (WHO == 1) {
+        f.x += sgn * (s2 * tq.x);
+        f.y += sgn * (s2 * tq.y);
+      } else if (WHO == 3) {
+        f.x -= sgn * (s2 * tq.x);
+        f.y -= sgn * (s2 * tq.y);
+      }
+      if (WHO != 3) e += sgn * ep2;
+    }
+  };
+  if (proj.a >= 0.0 && proj.a < 1.0) {
+    const HD2 dp{tq.x - proj * seg.x, tq.y - proj * seg.y};
+    const HD d = norm(dp);
+    HD gm, ep;
+    if (pair_hd<POT>(g, d, rsum, gm, ep) && gm.a != 0.0) {
+      const HD cr = seg.x * w.y - w.x * seg.y;
+      const double sign = cr.a > 0.0 ? 1.0 : (cr.a < 0.0 ? -1.0 : __longlong_as_double(0x7ff8000000000000LL));
+      const HD gg = gm * inv_len;
+      if (WHO == 1) {
+        f.x += gg * (sign * (-1.0) * seg.y);
+        f.y += gg * (sign * seg.x);
+      } else {
+        const HD a = habs(cr) * inv_lsq;
+        if (WHO == 2) {
+          f.x += gg * (sign * tq.y - a * seg.x);
+          f.y += gg * ((-sign) * tq.x - a * seg.y);
+        } else {
+          f.x += gg * ((-sign) * w.y + a * seg.x);
+          f.y += gg * (sign * w.x + a * seg.y);
+        }
+      }
+      if (WHO != 3) e += ep;
+    }
+    if (pc.a >= -pl2.a && pc.a < 0.0) corner(-1.0);
+  } else if (proj.a < 0.0 && pc.a >= 0.0) {
+    corner(1.0);
+  }
+}
+
+// ring predecessor of vertex j from its topology
+__device__ __forceinline__ int prev_of(const DiffArgs& g, int j, int back) {
+  const int2 tp = g.vtopo[j];
+  const int k = tp.y & 0xffff, n = tp.y >> 16;
+  return j - k + (k - back + 2 * n) % n;
+}
+
+template <int POT, int INTER>
 __global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= g.p.nv) return;
@@ -139,13 +207,22 @@ __global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g
   F.x += 0.5 * gmA * (-npd.y);
   F.y += 0.5 * gmA * npd.x;
   E += (0.5 * ea * dA * dA) / (double)nvr;
-  // segment lengths (harmonic monomers)
+  // segment lengths: harmonic or FENE monomers (include/cudaKernel.cuh:442-471)
   const HD plen = norm(ps), nlen = norm(ns);
   const HD tl0 = scaled_length(g, g.l0[v]), pl0 = scaled_length(g, g.l0[vp]);
-  const HD pd = plen / pl0 - 1.0, nd = nlen / tl0 - 1.0;
-  F.x += el * (nd * ns.x / (tl0 * nlen) - pd * ps.x / (pl0 * plen));
-  F.y += el * (nd * ns.y / (tl0 * nlen) - pd * ps.y / (pl0 * plen));
-  E += 0.5 * el * pd * pd;
+  if (p.monomer == 0) {
+    const HD pd = plen / pl0 - 1.0, nd = nlen / tl0 - 1.0;
+    F.x += el * (nd * ns.x / (tl0 * nlen) - pd * ps.x / (pl0 * plen));
+    F.y += el * (nd * ns.y / (tl0 * nlen) - pd * ps.y / (pl0 * plen));
+    E += 0.5 * el * pd * pd;
+  } else {
+    const HD c = (2.0 * p.stiff * p.ext_sq) * el;
+    const HD an = nlen / (p.ext_sq * tl0 * tl0 - nlen * nlen);
+    const HD ap = plen / (p.ext_sq * pl0 * pl0 - plen * plen);
+    F.x += c * (an * ns.x / nlen - ap * ps.x / plen);
+    F.y += c * (an * ns.y / nlen - ap * ps.y / plen);
+    E += (p.stiff * p.ext_sq) * el * hlog(1.0 - plen * plen / (p.ext_sq * pl0 * pl0));
+  }
   // bending
   const HD prevAD = thp - g.theta0[vp], thisAD = th - g.theta0[v], nextAD = thn - g.theta0[vn];
   const HD pvar = (thisAD - prevAD) / dot(ps, ps);
@@ -154,20 +231,44 @@ __global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g
   F.y += eb * (pvar * (-ps.x) + nvar * (-ns.x));
   E += 0.5 * eb * thisAD * thisAD;
 
-  // vertex-vertex pairs
   const HD ri = scaled_length(g, g.rad[v]);
   const int cnt = min(g.nbr_cnt[v], g.nbr_cap);
-  for (int s = 0; s < cnt; s++) {
-    const int j = g.nbr[(size_t)s * p.nv + v];
-    const HD2 dl = pbc2_hd(x, load_x(g, j), bx);
-    const HD d = norm(dl);
-    const HD rsum = ri + scaled_length(g, g.rad[j]);
-    HD gm, ep;
-    if (pair_hd<POT>(g, d, rsum, gm, ep)) {
-      const HD s2 = gm / d;
-      F.x += s2 * dl.x;
-      F.y += s2 * dl.y;
-      E += ep;
+  if constexpr (INTER == INT_VV) {
+    // vertex-vertex pairs
+    for (int s = 0; s < cnt; s++) {
+      const int j = g.nbr[(size_t)s * p.nv + v];
+      const HD2 dl = pbc2_hd(x, load_x(g, j), bx);
+      const HD d = norm(dl);
+      const HD rsum = ri + scaled_length(g, g.rad[j]);
+      HD gm, ep;
+      if (pair_hd<POT>(g, d, rsum, gm, ep)) {
+        const HD s2 = gm / d;
+        F.x += s2 * dl.x;
+        F.y += s2 * dl.y;
+        E += ep;
+      }
+    }
+  } else {
+    // smooth units gathered as the fused kernel gathers them: this vertex
+    // against each neighbour's segment prev(j) -> j (force on v), each
+    // neighbour against this vertex's segment prev(v) -> v (force on v as its
+    // end o), and each neighbour of next(v) against the segment v -> next(v)
+    // (force on v as its start q)
+    for (int s = 0; s < cnt; s++) {
+      const int j = g.nbr[(size_t)s * p.nv + v];
+      const HD2 xj = load_x(g, j), xjq = load_x(g, prev_of(g, j, 1)), xjqq = load_x(g, prev_of(g, j, 2));
+      const HD rsum = ri + scaled_length(g, g.rad[j]);
+      smooth_hd<POT, 1>(g, pbc2_hd(x, xjq, bx), pbc2_hd(x, xj, bx), pbc2_hd(xj, xjq, bx), pbc2_hd(xjq, xjqq, bx), rsum,
+                        F, E);
+      smooth_hd<POT, 2>(g, pbc2_hd(xj, xp, bx), pbc2_hd(xj, x, bx), ps, pps, rsum, F, E);
+    }
+    const HD rn = scaled_length(g, g.rad[vn]);
+    const int cntn = min(g.nbr_cnt[vn], g.nbr_cap);
+    HD none = hd(0.0);
+    for (int s = 0; s < cntn; s++) {
+      const int j = g.nbr[(size_t)s * p.nv + vn];
+      const HD2 xj = load_x(g, j);
+      smooth_hd<POT, 3>(g, pbc2_hd(xj, x, bx), pbc2_hd(xj, xn, bx), ns, ps, rn + scaled_length(g, g.rad[j]), F, none);
     }
   }
   double* fo = g.force_out + (size_t)v * 8;
@@ -179,14 +280,22 @@ __global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g
 
 }  // namespace
 
-void launch_diff(cudaStream_t st, int pot, const DiffArgs& g) {
+namespace {
+template <int INTER>
+void launch_diff_i(cudaStream_t st, int pot, const DiffArgs& g) {
   const int nb = (g.p.nv + 127) / 128;
   switch (pot) {
-    case POT_HARMONIC: k_diff<POT_HARMONIC><<<nb, 128, 0, st>>>(g); break;
-    case POT_LJ: k_diff<POT_LJ><<<nb, 128, 0, st>>>(g); break;
-    case POT_ADHESIVE: k_diff<POT_ADHESIVE><<<nb, 128, 0, st>>>(g); break;
-    default: k_diff<POT_WCA><<<nb, 128, 0, st>>>(g); break;
+    case POT_HARMONIC: k_diff<POT_HARMONIC, INTER><<<nb, 128, 0, st>>>(g); break;
+    case POT_LJ: k_diff<POT_LJ, INTER><<<nb, 128, 0, st>>>(g); break;
+    case POT_ADHESIVE: k_diff<POT_ADHESIVE, INTER><<<nb, 128, 0, st>>>(g); break;
+    default: k_diff<POT_WCA, INTER><<<nb, 128, 0, st>>>(g); break;
   }
+}
+}  // namespace
+
+void launch_diff(cudaStream_t st, int pot, int inter, const DiffArgs& g) {
+  if (inter == INT_VV) launch_diff_i<INT_VV>(st, pot, g);
+  else launch_diff_i<INT_SMOOTH>(st, pot, g);
 }
 
 // Fixed-order dot products for the Hessian solves: one partial per CTA, the

@@ -86,7 +86,7 @@ struct DiffArgs {
   double* force_out;   // [nv][8]: Fx (a, b, c, d), Fy (a, b, c, d)
   double* energy_out;  // [nv][4]
 };
-void launch_diff(cudaStream_t st, int pot, const DiffArgs& g);
+void launch_diff(cudaStream_t st, int pot, int inter, const DiffArgs& g);
 void launch_dot_partials(cudaStream_t st, int n, const double* a, const double* b, double* out, int nblocks);
 void launch_axpby(cudaStream_t st, int n, double a, const double* x, double b, double* y);
 void launch_extract_hv(cudaStream_t st, int nv, const double* fhd, double* hv);

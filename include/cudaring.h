@@ -367,8 +367,9 @@ int cr_neighbor_list_noalloc(const double* pos, const double* rad, const int* ri
 /* ---- derivatives ---------------------------------------------------------
  * No reference counterpart (the reference has no derivatives beyond forces).
  * Evaluated at the current positions with the current neighbour list, for
- * deformable rings with the vertex-vertex interaction and harmonic monomers
- * (other settings return CR_ENOTSUP).  U is the total potential energy. */
+ * deformable rings (harmonic or FENE monomers; vertex-vertex or smooth
+ * vertex-segment interaction; rigid rings return CR_ENOTSUP).  U is the total
+ * potential energy. */
 enum { CR_PARAM_EA = 0, CR_PARAM_EL = 1, CR_PARAM_EB = 2, CR_PARAM_LN_CALA0 = 3 };
 /* Hessian-vector product hv = (d^2 U / dx^2) v, v and hv of 2 Nv values */
 int cr_hvp(cr_ctx* ctx, const double* v, double* hv);

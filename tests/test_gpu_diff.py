@@ -19,9 +19,9 @@ pytestmark = pytest.mark.gpu
 KW = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
 
 
-def _system(n=16, phi=0.70, seed=4, rad_scale=1.3, **kw):
+def _system(n=16, phi=0.70, seed=4, rad_scale=1.3, placement="uniform", **kw):
     c = synth.workload_config(0, n)
-    pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=seed, placement="uniform")
+    pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=seed, placement=placement)
     pk.rad = pk.rad * rad_scale  # overlapping rings: every term of U acts
     args = dict(KW, **kw)
     d = DPM2D.from_packing(pk, **args)
@@ -57,6 +57,61 @@ def test_hvp_matches_force_differences(cuda_device, potential):
         S.neighbor_list(xs, pk.rad, S.cut_distance(0.5))
         ofd.append(S.force_energy(xs, pk.rad, pk.a0, pk.l0, pk.theta0)["force"])
     assert rel_inf(hv, -(ofd[0] - ofd[1]) / (2 * eps)) < 2e-6
+
+
+def _variant(case):
+    # smooth vertex-segment LJ / harmonic, or FENE monomers on vertex-vertex harmonic
+    if case == "lj_smooth":
+        # rings placed without overlap: LJ across the gaps, no r^-12 blow-up
+        d, pk, args = _system(potential="lennardJones", interaction="vertexSmooth", rad_scale=1.0, phi=0.5,
+                              placement="rsa")
+    elif case == "harmonic_smooth":
+        d, pk, args = _system(interaction="vertexSmooth")
+    else:
+        d, pk, args = _system()
+        from cudaring_b200.dpm2d import simControl
+        d.setMonomerType(simControl.monomerEnum.FENE)
+        d.setFENEconstants(1.0, 1.5)
+        d.calcForceEnergy()
+    return d, pk, args
+
+
+@pytest.mark.parametrize("case", ["lj_smooth", "harmonic_smooth", "fene"])
+def test_hvp_smooth_interaction_and_fene(cuda_device, case):
+    d, pk, args = _variant(case)
+    x = d.getVertexPositions()
+    v = np.random.default_rng(3).normal(size=x.shape)
+    hv = d.hvp(v)
+    eps = 1e-6
+    fp, _ = _forces_at(d, x + eps * v)
+    fm, _ = _forces_at(d, x - eps * v)
+    assert rel_inf(hv, -(fp - fm) / (2 * eps)) < 2e-6
+    # the same differences of the oracle's FP64 forces
+    S = oracle.System(pk.nv_list, pk.box, args["potential"], args["interaction"], args["ea"], args["el"], args["eb"],
+                      args["ec"], lj_cutoff=2.5, monomer=1 if case == "fene" else 0,
+                      stiff=1.0 if case == "fene" else 0.0, ext=1.5 if case == "fene" else 0.0)
+    ofd = []
+    for sgn in (+1, -1):
+        xs = x + sgn * eps * v
+        S.neighbor_list(xs, pk.rad, S.cut_distance(0.5))
+        ofd.append(S.force_energy(xs, pk.rad, pk.a0, pk.l0, pk.theta0)["force"])
+    assert rel_inf(hv, -(ofd[0] - ofd[1]) / (2 * eps)) < 2e-6
+
+
+@pytest.mark.parametrize("case", ["lj_smooth", "fene"])
+def test_pressure_smooth_interaction_and_fene(cuda_device, case):
+    d, pk, _ = _variant(case)
+    x, box = d.getVertexPositions(), d.getBoxSize()
+    P = d.calcPressure()
+    h = 1e-6
+    U = []
+    for lam in (1 + h, 1 - h):
+        d.setBoxSize(box * lam)
+        _, u = _forces_at(d, x * lam)
+        U.append(u)
+    d.setBoxSize(box)
+    fd = -(U[0] - U[1]) / (box[0] * box[1] * ((1 + h) ** 2 - (1 - h) ** 2))
+    assert P == pytest.approx(fd, rel=1e-6, abs=1e-9)
 
 
 def test_pressure_is_affine_energy_derivative(cuda_device):
@@ -238,7 +293,7 @@ def test_nve_gradient_through_checkpoints(cuda_device):
     q = synth.Packing(nv_list=pk.nv_list, pos=x0.copy(), vel=v0.copy(), rad=pk.rad, l0=pk.l0, theta0=pk.theta0,
                       a0=pk.a0, box=pk.box, centres=pk.centres)
     J_ref, g_ref, _ = nve_adjoint_reference(S, q, nsteps, dt)
-    assert float(J) == pytest.approx(J_ref, rel=1e-10)
+    assert float(J.detach()) == pytest.approx(J_ref, rel=1e-10)
     assert rel_inf(g, g_ref) < 1e-6
     rng = np.random.default_rng(7)
     h = 1e-6
