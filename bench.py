@@ -189,15 +189,7 @@ def dist_setup(args):
     return world, rank, local
 
 
-def max_over_ranks(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+from cudaring_b200.replicas import max_over_ranks  # noqa: E402  (device time of the slowest rank)
 
 
 def barrier(world: int):
