@@ -637,6 +637,10 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
       ctx->cap = 0;  // build_list grows from the measured count
       if ((rc = build_list(ctx, plan[j][(size_t)k - 1].check_buf, ctx->cut_distance))) return rc;
       if ((rc = clear_flags(ctx))) return rc;
+      // the failed build was a displacement-triggered rebuild: count it, as the
+      // in-graph build would have (DPM2D::checkDisplacement's updateCount)
+      ctx->status_h->update_count += 1;
+      if ((rc = upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus)))) return rc;
       if ((rc = run_direct(ctx, plan[j], (size_t)k, kind))) return rc;
       if (ctx->status_h->nonfinite)
         return ctx->fail(CR_ENONFINITE, "non-finite force after resuming from a neighbour-list overflow");
