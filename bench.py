@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--load-state", default=None, help="start from a state written by --save-state")
     ap.add_argument("--profile-kernel", action="store_true",
                     help="only time the fused step kernel (few launches; for ncu captures)")
+    ap.add_argument("--profile-build", action="store_true",
+                    help="only run full neighbour-list builds of the prepared state (for ncu captures)")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per vertex of the fused kernel (0: library default)")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
                     help="arithmetic of the timed run (the other one is timed for comparison)")
@@ -276,6 +278,24 @@ def main():
     t_prep = time.perf_counter()
     d, info = prepared_state(args, rank)
     nv, npr = d.numVertices, d.numParticles
+    if args.profile_build:
+        # forced one-launch builds of the list (the rebuild a step sequence
+        # runs when the displacement check fires), timed with CUDA events
+        import torch
+
+        cut = d.setDisplacementCutoff(0.5, 2.0 * d.getMeanVertexRadius())
+        for _ in range(3):
+            d.calcNeighborList(cut)
+        ms = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            d.calcNeighborList(cut)
+            torch.cuda.synchronize()
+            ms.append((time.perf_counter() - t0) * 1e3)
+        print(json.dumps({"profile_build_wall_ms": min(ms), "vertices": nv,
+                          "list_size": d.getNeighborListSize()}), flush=True)
+        d.close()
+        return
     if args.profile_kernel:
         d.setPrecision(args.precision)
         ms = d.profileStepKernel(3)
