@@ -1,4 +1,5 @@
-// Context, op sequencer (CUDA graphs with conditional rebuild nodes) and the
+// Context, op sequencer (CUDA graphs of step ops, each followed by the
+// one-launch neighbour build that runs only when the op armed it) and the
 // C ABI declared in include/cudaring.h.
 #include <algorithm>
 #include <cmath>
@@ -30,7 +31,7 @@ struct Op {
   int in_buf;     // position buffer read
   int out_buf;    // position buffer written (drift/advance), or in_buf
   int advance;    // tile: 1 = write next positions, 0 = final (store v, F)
-  int check_after;  // a rebuild conditional follows this op
+  int check_after;  // the op's displacement check may arm a rebuild (the build follows it)
   int check_buf;    // buffer whose positions the rebuild would use
 };
 

@@ -59,7 +59,7 @@ template <> struct BoxSel<true> {
 };
 
 // Every CTA ends in the last-block protocol so that the op counter and the
-// conditional rebuild node see each op exactly once.
+// conditional rebuild node of a batch graph see each op exactly once.
 __device__ __forceinline__ void tile_skip(const StepArgs& s, DevStatus* st) {
   if (is_last_block(st)) {
     if (threadIdx.x == 0) {
