@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-systems FIRE / compression measurement")
     ap.add_argument("--batch-systems", type=int, default=256)
+    ap.add_argument("--no-rigid", action="store_true", help="skip the rigid-ellipse (config 2) measurement")
+    ap.add_argument("--rigid-steps", type=int, default=2000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--save-state", default=None, help="write the prepared state (npz) after preparation")
     ap.add_argument("--load-state", default=None, help="start from a state written by --save-state")
@@ -423,6 +425,10 @@ def main():
     if rank == 0 and not args.no_batch:
         batch = batched_fire_measurement(args.batch_systems)
 
+    rigid = None
+    if rank == 0 and not args.no_rigid:
+        rigid = rigid_ellipse_measurement(args.rigid_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         steps_per_rebuild = (M * args.steps / run["updates"]) if run["updates"] else None
@@ -445,6 +451,7 @@ def main():
                        "lanes_per_vertex": info["lanes"]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": run["launches"],
             "clocks": run["clocks"], "precision_comparison": comparison, "batched_systems": batch,
+            "rigid_ellipses": rigid,
         }
         print(json.dumps(line), flush=True)
     d.close()
@@ -452,6 +459,52 @@ def main():
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def rigid_ellipse_measurement(steps: int) -> dict:
+    """Rigid bumpy ellipses (4096 rings of 24 vertices, WCA, rigid phi 0.65):
+    rigid Langevin at T 0.1, gamma 1, and the same with active self-propulsion
+    (f0 = v0 gamma = 0.1, taup = 1 / Dr = 100), dt 0.001, FP64 and mixed.
+    vertex-steps/s over ``steps`` steps timed with CUDA events on the
+    context's stream after a warm-up, neighbour rebuilds included."""
+    import ctypes
+
+    import torch
+
+    from cudaring_b200 import workloads
+    from cudaring_b200.dpm2d import simControl
+
+    d, info = workloads.prepared_ellipses()
+    c = info["config"]
+    sp = ctypes.c_void_p()
+    d._call("cr_get_stream", ctypes.byref(sp))
+    stream = torch.cuda.ExternalStream(sp.value)
+    nv = d.numVertices
+    out = {"workload": f"{d.numParticles} rigid ellipses x 24 vertices ({nv} vertices), aspect U[1.2, 2.0], WCA, "
+                       f"rigid phi {info['phi']:.3f}, dt {c['dt']}", "unit": "vertex-steps/s", "steps": steps,
+           "prep_seconds": info["prep_seconds"], "lanes_per_vertex": d.getLanes()}
+    for prec in ("fp64", "mixed"):
+        d.setPrecision(prec)
+        res = {}
+        for mode in ("langevin", "active"):
+            d.setParticleType(simControl.particleEnum.active if mode == "active" else simControl.particleEnum.passive)
+            d.setSelfPropulsionParams(c["driving"] if mode == "active" else 0.0, c["taup"])
+            d.initRigidLangevin(c["T"], c["gamma"], readState=True)
+            d.rigidLangevinLoop(max(100, steps // 10))
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            u0 = d.getUpdateCount()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            d.rigidLangevinLoop(steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            res[mode] = {"value": nv * steps / (ms / 1e3), "ms_per_step": ms / steps,
+                         "rebuilds": d.getUpdateCount() - u0}
+        out[prec] = res
+    d.setParticleType(simControl.particleEnum.passive)
+    d.close()
+    return out
 
 
 def batched_fire_measurement(num_systems: int, fire_iters: int = 2000, loop_systems: int = 8) -> dict:

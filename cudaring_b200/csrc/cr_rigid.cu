@@ -24,7 +24,10 @@
 
 namespace cr {
 
-template <int POT, int MODE, int BLOCK, int L>
+// PREC_MIXED: the vertex pair terms in FP32 on FP64-formed offsets (as the
+// deformable kernel's mixed path), accumulated per vertex in FP32; torques,
+// ring sums and integration stay FP64.
+template <int POT, int MODE, int BLOCK, int L, int PREC>
 __global__ void __launch_bounds__(BLOCK) k_rigid(const __grid_constant__ SysParams p,
                                                  const __grid_constant__ SysArrays a,
                                                  const __grid_constant__ StepArgs s,
@@ -81,7 +84,8 @@ __global__ void __launch_bounds__(BLOCK) k_rigid(const __grid_constant__ SysPara
   // pair forces
   {
     const int lv = t / L, lane = t % L;
-    double2 fi = make_double2(0.0, 0.0);
+    using T = typename std::conditional<PREC == PREC_MIXED, float, double>::type;
+    typename Vec2<T>::type fi{0, 0};
     double ei = 0.0;
     if (lv < nvt) {
       const int i = v0 + lv;
@@ -90,7 +94,8 @@ __global__ void __launch_bounds__(BLOCK) k_rigid(const __grid_constant__ SysPara
       const int cnt = min(a.nbr_cnt[i], a.nbr_cap);
       for (int sl = lane; sl < cnt; sl += L) {
         const int j = __ldg(a.nbr + (size_t)sl * p.nv + i);
-        pair_own<POT>(p, pbc2(p, xi, a.pos[j]), ri + __ldg(a.rad + j), fi, ei);
+        if constexpr (PREC == PREC_MIXED) pair_own_f<POT>(p, f2(pbc2(p, xi, a.pos[j])), (float)(ri + __ldg(a.rad + j)), fi, ei);
+        else pair_own<POT>(p, pbc2(p, xi, a.pos[j]), ri + __ldg(a.rad + j), fi, ei);
       }
     }
 #pragma unroll
@@ -100,7 +105,7 @@ __global__ void __launch_bounds__(BLOCK) k_rigid(const __grid_constant__ SysPara
       ei += __shfl_xor_sync(0xffffffffu, ei, o);
     }
     if (lane == 0 && lv < nvt) {
-      s_f[lv] = fi;
+      s_f[lv] = make_double2(fi.x, fi.y);
       s_e[lv] = ei;
     }
   }
@@ -352,17 +357,25 @@ __global__ void k_rigid_inject(int np, double2* p_vel, double amp, unsigned long
   }
 }
 
+template <int POT, int MODE, int PREC>
+static void launch_rigid_p(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s,
+                           const RigidArgs& r) {
+  if (c.lanes == 1) k_rigid<POT, MODE, 128, 1, PREC><<<c.grid, 128, 0, c.stream>>>(p, a, s, r);
+  else if (c.lanes == 4) k_rigid<POT, MODE, 256, 4, PREC><<<c.grid, 256, 0, c.stream>>>(p, a, s, r);
+  else if (c.lanes == 8) k_rigid<POT, MODE, 256, 8, PREC><<<c.grid, 256, 0, c.stream>>>(p, a, s, r);
+  else k_rigid<POT, MODE, 192, 2, PREC><<<c.grid, 192, 0, c.stream>>>(p, a, s, r);  // tiles of up to 96 vertices
+}
+
 template <int POT, int MODE>
 static void launch_rigid_t(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s,
                            const RigidArgs& r) {
-  if (c.lanes == 1) k_rigid<POT, MODE, 128, 1><<<c.grid, 128, 0, c.stream>>>(p, a, s, r);
-  else if (c.lanes == 4) k_rigid<POT, MODE, 256, 4><<<c.grid, 256, 0, c.stream>>>(p, a, s, r);
-  else if (c.lanes == 8) k_rigid<POT, MODE, 256, 8><<<c.grid, 256, 0, c.stream>>>(p, a, s, r);
-  else k_rigid<POT, MODE, 192, 2><<<c.grid, 192, 0, c.stream>>>(p, a, s, r);  // tiles of up to 96 vertices
+  if (c.precision == CR_PRECISION_MIXED) launch_rigid_p<POT, MODE, PREC_MIXED>(c, p, a, s, r);
+  else launch_rigid_p<POT, MODE, PREC_FP64>(c, p, a, s, r);
 }
 
-void launch_rigid(const LaunchCfg& c, int pot, int mode, const SysParams& p, const SysArrays& a, const StepArgs& s,
-                  const RigidArgs& r) {
+void launch_rigid(const LaunchCfg& c, int pot, int mode, const SysParams& p_in, const SysArrays& a,
+                  const StepArgs& s, const RigidArgs& r) {
+  const SysParams p = with_f32_constants(p_in);  // the FP32 pair terms read them
 #define CR_RIGID_CASE(P)                                              \
   case P:                                                             \
     if (mode == MODE_FORCE) launch_rigid_t<P, MODE_FORCE>(c, p, a, s, r); \

@@ -315,6 +315,9 @@ __device__ __forceinline__ float sign_of_f(float c) {
 //     decision only for pproj within rounding of 0 or 1).
 // ----------------------------------------------------------------------------
 
+// Arithmetic of the pair terms: FP64, or FP32 on FP64-formed offsets.
+enum Prec : int { PREC_FP64 = 0, PREC_MIXED = 1 };
+
 template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };

@@ -24,7 +24,6 @@
 
 namespace cr {
 
-enum Prec : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 
 // Occupancy target in threads per SM.  One lane per vertex: 512 leaves 128
 // registers per thread, where the FP64 smooth-interaction body compiles

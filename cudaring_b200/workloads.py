@@ -130,6 +130,58 @@ def prepared_deformable(index: int = 1, rings: int | None = None, seed: int = 20
     return d, info
 
 
+def prepared_ellipses(n: int | None = None, seed: int = 20261205, phi_start: float = 0.2, dphi: float = 0.01,
+                      relax_steps: int = 200, ec_compress: float = 100.0, wca_steps: int = 3000) -> tuple[DPM2D, dict]:
+    """Rigid bumpy ellipses of config 2 (4096 rings of 24 vertices, aspect
+    ratio U[1.2, 2.0], WCA) at their target rigid packing fraction.
+
+    Rings are placed without overlap at ``phi_start`` and compressed affinely
+    (ring centres and box scaled by sqrt(phi / phi_new), shapes unchanged) in
+    steps of ``dphi`` under a stiff harmonic repulsion (bounded forces), each
+    step followed by ``relax_steps`` steps of rigid Langevin dynamics at the
+    configuration's temperature; then the WCA potential is switched on and the
+    packing relaxed with ``wca_steps`` steps at a tenth of the time step.
+    """
+    import time
+
+    c = synth.workload_config(2, n)
+    t0 = time.perf_counter()
+    pk = synth.make_ellipse_packing(c["n"], c["nv"], c["ratio_range"], phi_start, seed=seed)
+    d = DPM2D.from_packing(pk, potential="harmonic", interaction=c["interaction"], ec=ec_compress, dt=c["dt"])
+    d.setShapeType(simControl.shapeEnum.rigid)
+    cut = d.setDisplacementCutoff(0.5, 2.0 * float(pk.rad.mean()))
+    ring_of = np.repeat(np.arange(pk.num_particles), pk.nv_list)
+    d.setSeed(seed)
+    phi, steps = phi_start, 0
+    while phi < c["phi"] - 1e-12:
+        nxt = min(c["phi"], phi + dphi)
+        s = math.sqrt(phi / nxt)
+        d.calcParticlePositions()
+        cen = d.getParticlePositions().reshape(-1, 2)[ring_of]
+        x = d.getVertexPositions().reshape(-1, 2)
+        box = d.getBoxSize()
+        rel = x - cen
+        rel -= box * np.round(rel / box)
+        d.setBoxSize(box * s)
+        d.setVertexPositions((cen * s + rel).reshape(-1))
+        d.calcNeighborList(cut)
+        d.initRigidLangevin(c["T"], c["gamma"], readState=False)
+        d.rigidLangevinLoop(relax_steps)
+        phi, steps = nxt, steps + 1
+    d.setPotentialType(getattr(simControl.potentialEnum, c["potential"]))
+    d.setEnergyCosts(0.0, 0.0, 0.0, c["ec"])
+    cut = d.setDisplacementCutoff(0.5, 2.0 * float(pk.rad.mean()))
+    d.calcNeighborList(cut)
+    d.setTimeStep(0.1 * c["dt"])
+    d.initRigidLangevin(c["T"], c["gamma"], readState=False)
+    d.rigidLangevinLoop(wca_steps)
+    d.setTimeStep(c["dt"])
+    box = d.getBoxSize()
+    info = dict(config=c, phi=float(np.sum(pk.a0) / (box[0] * box[1])), compression_steps=steps,
+                prep_seconds=time.perf_counter() - t0, cut_distance=cut)
+    return d, info
+
+
 def tile_system(d: DPM2D, k: int, config: dict) -> DPM2D:
     """A k x k periodic tiling of the system held by ``d`` (positions,
     velocities, radii, rest lengths / areas / angles, box) as a new context

@@ -65,3 +65,31 @@ def test_rigid_langevin_temperature(cuda_device):
         ke.append(d.getParticleKineticEnergy())
     t_meas = 2.0 * np.mean(ke) / (2 * pk.num_particles)
     assert t_meas == pytest.approx(T, rel=0.08)
+
+
+def test_rigid_mixed_precision_forces_and_langevin(cuda_device):
+    # FP32 vertex pair terms on FP64 offsets: forces and torques within FP32
+    # rounding of the FP64 path; a Langevin run stays finite and at temperature
+    c = synth.workload_config(2, 256)
+    pk = synth.make_ellipse_packing(c["n"], c["nv"], c["ratio_range"], 0.25, seed=6)
+    d = DPM2D.from_packing(pk, potential="wca", interaction="vertexVertex", ec=1.0, dt=0.001)
+    d.setShapeType(simControl.shapeEnum.rigid)
+    d.calcNeighborList(d.setDisplacementCutoff(0.5, 2 * pk.rad.mean()))
+    d.setSeed(4)
+    d.initRigidLangevin(0.1, 1.0, readState=False)
+    d.rigidLangevinLoop(500)  # thermal contacts
+    out = {}
+    for prec in ("fp64", "mixed"):
+        d.setPrecision(prec)
+        d.calcRigidForceEnergy()
+        out[prec] = (d.getParticleForces(), d.getParticleTorques(), d.getPotentialEnergy())
+    assert rel_inf(out["mixed"][0], out["fp64"][0]) < 1e-5
+    assert rel_inf(out["mixed"][1], out["fp64"][1]) < 1e-5
+    assert out["fp64"][2] > 0.0
+    assert out["mixed"][2] == pytest.approx(out["fp64"][2], rel=1e-5)
+    d.setSeed(5)
+    d.initRigidLangevin(0.1, 1.0, readState=False)
+    d.rigidLangevinLoop(2000)
+    assert np.all(np.isfinite(d.getVertexPositions()))
+    ke = d.getParticleKineticEnergy()
+    assert 0.02 < 2.0 * ke / (2 * pk.num_particles) < 0.5
