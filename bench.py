@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--batch-systems", type=int, default=256)
     ap.add_argument("--no-rigid", action="store_true", help="skip the rigid-ellipse (config 2) measurement")
     ap.add_argument("--rigid-steps", type=int, default=2000)
+    ap.add_argument("--no-diff", action="store_true", help="skip the derivative (config 4) measurement")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--save-state", default=None, help="write the prepared state (npz) after preparation")
     ap.add_argument("--load-state", default=None, help="start from a state written by --save-state")
@@ -429,6 +430,10 @@ def main():
     if rank == 0 and not args.no_rigid:
         rigid = rigid_ellipse_measurement(args.rigid_steps)
 
+    deriv = None
+    if rank == 0 and not args.no_diff:
+        deriv = derivative_measurement()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         steps_per_rebuild = (M * args.steps / run["updates"]) if run["updates"] else None
@@ -451,7 +456,7 @@ def main():
                        "lanes_per_vertex": info["lanes"]},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": run["launches"],
             "clocks": run["clocks"], "precision_comparison": comparison, "batched_systems": batch,
-            "rigid_ellipses": rigid,
+            "rigid_ellipses": rigid, "derivatives": deriv,
         }
         print(json.dumps(line), flush=True)
     d.close()
@@ -459,6 +464,56 @@ def main():
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def derivative_measurement() -> dict:
+    """Config 4 of the benchmark list (differentiation): 256 rings of 32
+    vertices, harmonic, phi 0.88, FIRE-minimised to max |F| <= 1e-12; wall
+    times of the minimised-state gradients of U and P along (ea, el, eb, calA0)
+    (two conjugate-gradient Hessian solves to 1e-10), of Hessian-vector
+    products on device buffers, and of d(U + K)/d(x0, v0) through 200 NVE
+    steps (dt 0.002) with checkpoints every 20 steps."""
+    import torch
+
+    from cudaring_b200 import diff, workloads
+
+    t0 = time.perf_counter()
+    d, info = workloads.prepared_deformable(4)
+    c = info["config"]
+    sig = d.getMeanParticleSize()
+    d.initFIRE([0.2, 0.5, 1.1, 0.99, 1e-3 * sig, 1e-2 * sig, 0.2], 20, 0, d.numVertices)
+    fire_it, fmax = d.minimizeFIRE(1e-12, 1000000)
+    prep = time.perf_counter() - t0
+    nv = d.numVertices
+    t1 = time.perf_counter()
+    g = diff.minimized_gradients(d, float(np.mean(c["calA0"])) if np.ndim(c["calA0"]) else float(c["calA0"]),
+                                 tol=1e-10)
+    t_grad = time.perf_counter() - t1
+    v = torch.randn(2 * nv, dtype=torch.float64, device="cuda")
+    hv = torch.empty_like(v)
+    for _ in range(5):
+        d.hvpDevice(v.data_ptr(), hv.data_ptr())
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    reps = 200
+    for _ in range(reps):
+        d.hvpDevice(v.data_ptr(), hv.data_ptr())
+    torch.cuda.synchronize()
+    t_hvp = (time.perf_counter() - t2) / reps
+    x0 = d.getVertexPositions()
+    v0 = np.random.default_rng(3).normal(0.0, 0.01, size=x0.shape)
+    t3 = time.perf_counter()
+    J, gx, gv = diff.nve_gradient(d, x0, v0, 200, 0.002, checkpoint=20)
+    t_nve = time.perf_counter() - t3
+    out = {"workload": f"{d.numParticles} rings nv 32 ({nv} vertices), harmonic, phi {info['phi']:.3f}, "
+                       f"FIRE to max |F| {fmax:.1e} ({fire_it} iterations)",
+           "prep_seconds": prep,
+           "minimized_gradients": {"seconds": t_grad, "cg_iterations": {k: it_rr[0] for k, it_rr in g["cg"].items()},
+                                   "dU": g["dU"], "dP": g["dP"]},
+           "hvp": {"ms_per_product": t_hvp * 1e3, "vertex_products_per_s": nv / t_hvp},
+           "nve_gradient": {"seconds": t_nve, "steps": 200, "checkpoint": 20, "J": J}}
+    d.close()
+    return out
 
 
 def rigid_ellipse_measurement(steps: int) -> dict:
