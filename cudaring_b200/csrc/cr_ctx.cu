@@ -102,6 +102,9 @@ struct cr_ctx {
   double* diff_e = nullptr;   // [nv][4]
   double* diff_dot = nullptr; // [256] dot-product partials
   double* diff_vec = nullptr; // [5][2 nv] CG vectors
+  double* diff_area = nullptr; // [np][4] hyper-dual ring areas
+  CgState* cg_state = nullptr;
+  double* cg_part = nullptr;   // [148][4] CG reduction partials
   int partials_n = 0;
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
@@ -834,7 +837,8 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->tiles, ctx->nbr, ctx->nbr_cnt, ctx->cell_of, ctx->slot,
                   ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
                   ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
-                  ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec,
+                  ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec, ctx->diff_area, ctx->cg_state,
+                  ctx->cg_part,
                   ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum,
                   ctx->prad, ctx->plast, ctx->pid, ctx->pnbr, ctx->pnbr_cnt, ctx->pstatus, ctx->pfire, ctx->pdraws};
   for (void* p : ptrs)
@@ -1749,7 +1753,9 @@ static int diff_ready(cr_ctx* ctx) {
   if (!ctx->nbr_built && (rc = build_list(ctx, ctx->cur, ctx->cut_distance))) return rc;
   if (!ctx->diff_f) {
     if ((rc = dalloc(ctx, &ctx->diff_f, (size_t)8 * ctx->nv)) || (rc = dalloc(ctx, &ctx->diff_e, (size_t)4 * ctx->nv)) ||
-        (rc = dalloc(ctx, &ctx->diff_dot, 256)) || (rc = dalloc(ctx, &ctx->diff_vec, (size_t)10 * ctx->nv)))
+        (rc = dalloc(ctx, &ctx->diff_dot, 256)) || (rc = dalloc(ctx, &ctx->diff_vec, (size_t)10 * ctx->nv)) ||
+        (rc = dalloc(ctx, &ctx->diff_area, (size_t)4 * ctx->np)) || (rc = dalloc(ctx, &ctx->cg_state, 1)) ||
+        (rc = dalloc(ctx, &ctx->cg_part, (size_t)4 * 148)))
       return rc;
   }
   return CR_OK;
@@ -1770,12 +1776,13 @@ static DiffArgs diff_args(cr_ctx* ctx) {
   g.nbr_cap = ctx->cap;
   g.force_out = ctx->diff_f;
   g.energy_out = ctx->diff_e;
+  g.ring_area = ctx->diff_area;
   return g;
 }
 
 static int diff_launch(cr_ctx* ctx, const DiffArgs& g) {
-  launch_diff(ctx->stream, ctx->potential, inter_kind(ctx), g);
-  ctx->launches++;
+  launch_diff(ctx->stream, ctx->potential, inter_kind(ctx), g, ctx->ring_first, ctx->ring_nv);
+  ctx->launches += 2;
   CR_TRY(cudaGetLastError());
   return CR_OK;
 }
@@ -1902,35 +1909,67 @@ extern "C" int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double 
   double* pv = r + n;
   double* hp = pv + n;
   // conjugate gradients on the Hessian restricted to vectors without a
-  // uniform translation (its null space in a periodic box): b and every
-  // iterate are projected
+  // uniform translation (its null space in a periodic box): b is projected,
+  // and each H p loses its mean, so every iterate stays in that subspace
   if ((rc = upload(ctx, r, b, (size_t)n * sizeof(double)))) return rc;
   if ((rc = dev_project(ctx, r))) return rc;
   CR_TRY(cudaMemsetAsync(xd, 0, (size_t)n * sizeof(double), ctx->stream));
   CR_TRY(cudaMemcpyAsync(pv, r, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  double rr, bb;
-  if ((rc = dev_dot(ctx, r, r, n, &rr))) return rc;
-  bb = rr;
-  long it = 0;
-  while (it < maxIter && bb > 0.0 && std::sqrt(rr / bb) > tol) {
-    if ((rc = cr_hvp_device(ctx, pv, hp))) return rc;
-    if ((rc = dev_project(ctx, hp))) return rc;
-    double pHp;
-    if ((rc = dev_dot(ctx, pv, hp, n, &pHp))) return rc;
-    if (!(pHp > 0.0)) return ctx->fail(CR_ENONFINITE, "Hessian not positive along a CG direction");
-    const double alpha = rr / pHp;
-    launch_axpby(ctx->stream, n, alpha, pv, 1.0, xd);
-    launch_axpby(ctx->stream, n, -alpha, hp, 1.0, r);
-    double rr2;
-    if ((rc = dev_dot(ctx, r, r, n, &rr2))) return rc;
-    launch_axpby(ctx->stream, n, 1.0, r, rr2 / rr, pv);
-    ctx->launches += 3;
-    rr = rr2;
-    it++;
+  double bb;
+  if ((rc = dev_dot(ctx, r, r, n, &bb))) return rc;
+  CgState cs;
+  memset(&cs, 0, sizeof(cs));
+  cs.rr = bb;
+  cs.bb = bb;
+  cs.tol = tol;
+  cs.max_iters = maxIter;
+  cs.done = (maxIter == 0 || !(bb > 0.0) || !(std::sqrt(cs.rr / bb) > tol)) ? 1 : 0;
+  if ((rc = upload(ctx, ctx->cg_state, &cs, sizeof(cs)))) return rc;
+  // the iterations run in captured chunks: H p (hyper-dual forces along p),
+  // then the CG scalars and vector updates, all on the device; every kernel
+  // returns at once after the state says done, so a chunk may overrun
+  constexpr int kChunk = 32;
+  DiffArgs g = diff_args(ctx);
+  g.t1 = reinterpret_cast<const double2*>(pv);
+  g.skip = &ctx->cg_state->done;
+  CgArgs a;
+  a.nv = ctx->nv;
+  a.x = xd;
+  a.r = r;
+  a.p = pv;
+  a.hp = hp;
+  a.fhd = ctx->diff_f;
+  a.st = ctx->cg_state;
+  a.partials = ctx->cg_part;
+  a.nblk = cg_blocks(ctx->nv);
+  cudaGraphExec_t exec = nullptr;
+  if (!cs.done) {
+    cudaGraph_t graph = nullptr;
+    CR_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kChunk; k++) {
+      launch_diff(ctx->stream, ctx->potential, inter_kind(ctx), g, ctx->ring_first, ctx->ring_nv);
+      launch_cg_iteration(ctx->stream, a);
+    }
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    CR_TRY(ce);
   }
+  while (!cs.done) {
+    cudaError_t ce = cudaGraphLaunch(exec, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&cs, ctx->cg_state, sizeof(cs), cudaMemcpyDeviceToHost, ctx->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(ctx->stream);
+    if (ce != cudaSuccess) {
+      cudaGraphExecDestroy(exec);
+      CR_TRY(ce);
+    }
+    ctx->launches += (long long)kChunk * 7;
+  }
+  if (exec) cudaGraphExecDestroy(exec);
   CR_TRY(cudaGetLastError());
-  if (iters) *iters = it;
-  if (relres) *relres = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;
+  if (cs.bad) return ctx->fail(CR_ENONFINITE, "Hessian not positive along a CG direction");
+  if (iters) *iters = (long)cs.iters;
+  if (relres) *relres = bb > 0.0 ? std::sqrt(cs.rr / bb) : 0.0;
   return download(ctx, x, xd, (size_t)n * sizeof(double));
 }
 

@@ -12,9 +12,11 @@
 // The e1 part of the force is then D_t1 F = -H t1 (the Hessian-vector
 // product), the e1 part of the energy along the affine dilation t1 = x,
 // s1 = 1 is dU/dlambda = -2 A P, and the e1 e2 parts give the mixed
-// derivatives that the adjoint gradients need.  The ring's area is summed by
-// each of its threads (O(nv) per vertex): this kernel serves small systems
-// and iterative solves, not the time-stepping hot path.
+// derivatives that the adjoint gradients need.  The rings' areas are summed
+// once per ring by a first kernel.  These kernels serve small systems and
+// iterative solves, not the time-stepping hot path.
+#include <algorithm>
+
 #include "cr_hd.cuh"
 #include "cr_launch.h"
 #include "cr_tile.cuh"
@@ -167,10 +169,35 @@ __device__ __forceinline__ int prev_of(const DiffArgs& g, int j, int back) {
   return j - k + (k - back + 2 * n) % n;
 }
 
+// ring area by the shoelace sum of offsets from the ring's first vertex, one
+// thread per ring
+__global__ void __launch_bounds__(64) k_ring_area_hd(const __grid_constant__ DiffArgs g, const int* ring_first,
+                                                     const int* ring_nv) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= g.p.np || (g.skip && *g.skip)) return;
+  const SysParams& p = g.p;
+  const HBox bx{HD{p.lx, p.lx * g.s1, p.lx * g.s2, 0.0}, HD{p.ly, p.ly * g.s1, p.ly * g.s2, 0.0}};
+  const int f = ring_first[q], nvr = ring_nv[q];
+  const HD2 x0 = load_x(g, f);
+  HD sum = hd(0.0);
+  HD2 u = HD2{hd(0.0), hd(0.0)};
+  for (int k = 0; k < nvr; k++) {
+    const HD2 un = pbc2_hd(load_x(g, f + (k + 1) % nvr), x0, bx);
+    sum += cross(u, un);
+    u = un;
+  }
+  const HD area = 0.5 * habs(sum);
+  double* o = g.ring_area + (size_t)4 * q;
+  o[0] = area.a;
+  o[1] = area.b;
+  o[2] = area.c;
+  o[3] = area.d;
+}
+
 template <int POT, int INTER>
-__global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g) {
+__global__ void __launch_bounds__(64) k_diff(const __grid_constant__ DiffArgs g) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (v >= g.p.nv) return;
+  if (v >= g.p.nv || (g.skip && *g.skip)) return;
   const SysParams& p = g.p;
   const HBox bx{HD{p.lx, p.lx * g.s1, p.lx * g.s2, 0.0}, HD{p.ly, p.ly * g.s1, p.ly * g.s2, 0.0}};
   const HD ea{p.ea, g.pe1[0], g.pe2[0], 0.0}, el{p.el, g.pe1[1], g.pe2[1], 0.0}, eb{p.eb, g.pe1[2], g.pe2[2], 0.0};
@@ -180,18 +207,8 @@ __global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g
   auto at = [&](int kk) { return f + ((kk % nvr) + nvr) % nvr; };
   const int vp = at(k - 1), vn = at(k + 1), vpp = at(k - 2), vnn = at(k + 2);
 
-  // ring area by the shoelace sum of offsets from the first vertex
-  const HD2 x0 = load_x(g, f);
-  HD sum = hd(0.0);
-  {
-    HD2 u = HD2{hd(0.0), hd(0.0)};
-    for (int q = 0; q < nvr; q++) {
-      const HD2 un = pbc2_hd(load_x(g, at(q + 1)), x0, bx);
-      sum += cross(u, un);
-      u = un;
-    }
-  }
-  const HD area = 0.5 * habs(sum);
+  const double* ra = g.ring_area + (size_t)4 * ring;
+  const HD area{ra[0], ra[1], ra[2], ra[3]};
   const HD2 x = load_x(g, v), xn = load_x(g, vn), xp = load_x(g, vp);
   const HD2 ns = pbc2_hd(xn, x, bx), ps = pbc2_hd(x, xp, bx);
   const HD2 pps = pbc2_hd(xp, load_x(g, vpp), bx), nns = pbc2_hd(load_x(g, vnn), xn, bx);
@@ -281,19 +298,22 @@ __global__ void __launch_bounds__(128) k_diff(const __grid_constant__ DiffArgs g
 }  // namespace
 
 namespace {
+// small CTAs: the systems these derivatives serve hold a few thousand
+// vertices, so 32-thread CTAs spread them over every SM
 template <int INTER>
 void launch_diff_i(cudaStream_t st, int pot, const DiffArgs& g) {
-  const int nb = (g.p.nv + 127) / 128;
+  const int nb = (g.p.nv + 31) / 32;
   switch (pot) {
-    case POT_HARMONIC: k_diff<POT_HARMONIC, INTER><<<nb, 128, 0, st>>>(g); break;
-    case POT_LJ: k_diff<POT_LJ, INTER><<<nb, 128, 0, st>>>(g); break;
-    case POT_ADHESIVE: k_diff<POT_ADHESIVE, INTER><<<nb, 128, 0, st>>>(g); break;
-    default: k_diff<POT_WCA, INTER><<<nb, 128, 0, st>>>(g); break;
+    case POT_HARMONIC: k_diff<POT_HARMONIC, INTER><<<nb, 32, 0, st>>>(g); break;
+    case POT_LJ: k_diff<POT_LJ, INTER><<<nb, 32, 0, st>>>(g); break;
+    case POT_ADHESIVE: k_diff<POT_ADHESIVE, INTER><<<nb, 32, 0, st>>>(g); break;
+    default: k_diff<POT_WCA, INTER><<<nb, 32, 0, st>>>(g); break;
   }
 }
 }  // namespace
 
-void launch_diff(cudaStream_t st, int pot, int inter, const DiffArgs& g) {
+void launch_diff(cudaStream_t st, int pot, int inter, const DiffArgs& g, const int* ring_first, const int* ring_nv) {
+  k_ring_area_hd<<<(g.p.np + 63) / 64, 64, 0, st>>>(g, ring_first, ring_nv);
   if (inter == INT_VV) launch_diff_i<INT_VV>(st, pot, g);
   else launch_diff_i<INT_SMOOTH>(st, pot, g);
 }
@@ -350,6 +370,116 @@ void launch_extract_hv(cudaStream_t st, int nv, const double* fhd, double* hv) {
 }
 void launch_sub_mean(cudaStream_t st, int nv, double* x, double mx, double my) {
   k_sub_mean<<<(nv + 255) / 256, 256, 0, st>>>(nv, x, mx, my);
+}
+
+// ----------------------------------------------- device-resident CG iteration
+namespace {
+constexpr int kCgBlock = 256;
+
+__device__ __forceinline__ void cg_block_sums(double* v, int n, double* out) {
+  // fixed-order CTA sums of n values per thread; results in out[0..n) on thread 0
+  __shared__ double s[kCgBlock / 32][4];
+  for (int q = 0; q < n; q++) {
+    double x = v[q];
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5][q] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < n; q++) {
+      double t = 0.0;
+      for (int w = 0; w < kCgBlock / 32; w++) t += s[w][q];
+      out[q] = t;
+    }
+  }
+}
+
+// hp = H p (the negated e1 parts of the forces); partials: sum hp.x, sum hp.y, p.hp
+__global__ void __launch_bounds__(kCgBlock) k_cg_hp(const __grid_constant__ CgArgs a) {
+  if (((volatile CgState*)a.st)->done) return;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int v = blockIdx.x * kCgBlock + threadIdx.x; v < a.nv; v += a.nblk * kCgBlock) {
+    const double hx = -a.fhd[(size_t)v * 8 + 1], hy = -a.fhd[(size_t)v * 8 + 5];
+    a.hp[2 * v] = hx;
+    a.hp[2 * v + 1] = hy;
+    acc[0] += hx;
+    acc[1] += hy;
+    acc[2] += a.p[2 * v] * hx + a.p[2 * v + 1] * hy;
+  }
+  double out[3];
+  cg_block_sums(acc, 3, out);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 3; q++) a.partials[(size_t)4 * blockIdx.x + q] = out[q];
+}
+
+// one thread: the mean of H p and the step alpha = |r|^2 / p.Hp (p carries no
+// translation, so p.Hp is the curvature along p of the projected Hessian)
+__global__ void k_cg_alpha(const __grid_constant__ CgArgs a) {
+  CgState& st = *a.st;
+  if (st.done) return;
+  double sx = 0.0, sy = 0.0, php = 0.0;
+  for (int b = 0; b < a.nblk; b++) {
+    sx += a.partials[4 * b];
+    sy += a.partials[4 * b + 1];
+    php += a.partials[4 * b + 2];
+  }
+  st.mx = sx / a.nv;
+  st.my = sy / a.nv;
+  if (!(php > 0.0)) {
+    st.bad = 1;
+    st.done = 1;
+    return;
+  }
+  st.alpha = st.rr / php;
+}
+
+// x += alpha p; r -= alpha (H p - mean); partials: |r|^2
+__global__ void __launch_bounds__(kCgBlock) k_cg_update(const __grid_constant__ CgArgs a) {
+  const CgState st = *(const CgState*)a.st;
+  if (st.done) return;
+  double acc[1] = {0.0};
+  for (int i = blockIdx.x * kCgBlock + threadIdx.x; i < 2 * a.nv; i += a.nblk * kCgBlock) {
+    const double m = (i & 1) ? st.my : st.mx;
+    a.x[i] += st.alpha * a.p[i];
+    const double r = a.r[i] - st.alpha * (a.hp[i] - m);
+    a.r[i] = r;
+    acc[0] += r * r;
+  }
+  double out[1];
+  cg_block_sums(acc, 1, out);
+  if (threadIdx.x == 0) a.partials[(size_t)4 * blockIdx.x + 3] = out[0];
+}
+
+// one thread: the new |r|^2, beta, the iteration count and the stop tests of
+// the host loop (relative residual, iteration limit)
+__global__ void k_cg_beta(const __grid_constant__ CgArgs a) {
+  CgState& st = *a.st;
+  if (st.done) return;
+  double rr2 = 0.0;
+  for (int b = 0; b < a.nblk; b++) rr2 += a.partials[4 * b + 3];
+  st.beta = rr2 / st.rr;
+  st.rr = rr2;
+  st.iters += 1;
+  if (!(sqrt(st.rr / st.bb) > st.tol) || st.iters >= st.max_iters) st.done = 1;
+}
+
+// p = r + beta p
+__global__ void __launch_bounds__(kCgBlock) k_cg_direction(const __grid_constant__ CgArgs a) {
+  const CgState st = *(const CgState*)a.st;
+  if (st.done) return;
+  for (int i = blockIdx.x * kCgBlock + threadIdx.x; i < 2 * a.nv; i += a.nblk * kCgBlock)
+    a.p[i] = a.r[i] + st.beta * a.p[i];
+}
+}  // namespace
+
+int cg_blocks(int nv) { return std::max(1, std::min(148, (2 * nv + kCgBlock - 1) / kCgBlock)); }
+
+void launch_cg_iteration(cudaStream_t st, const CgArgs& a) {
+  k_cg_hp<<<a.nblk, kCgBlock, 0, st>>>(a);
+  k_cg_alpha<<<1, 1, 0, st>>>(a);
+  k_cg_update<<<a.nblk, kCgBlock, 0, st>>>(a);
+  k_cg_beta<<<1, 1, 0, st>>>(a);
+  k_cg_direction<<<a.nblk, kCgBlock, 0, st>>>(a);
 }
 
 }  // namespace cr

@@ -85,8 +85,34 @@ struct DiffArgs {
   int nbr_cap;
   double* force_out;   // [nv][8]: Fx (a, b, c, d), Fy (a, b, c, d)
   double* energy_out;  // [nv][4]
+  double* ring_area;   // [np][4] scratch: hyper-dual ring areas (filled by the launch)
+  const int* skip;     // nullable: nothing is evaluated while *skip != 0
 };
-void launch_diff(cudaStream_t st, int pot, int inter, const DiffArgs& g);
+void launch_diff(cudaStream_t st, int pot, int inter, const DiffArgs& g, const int* ring_first, const int* ring_nv);
+// Device-resident conjugate-gradient iterations on the projected Hessian
+// (cr_hessian_solve): every scalar stays on the device, so a run of
+// iterations is one captured graph with no host synchronisation.
+struct CgState {
+  double rr, bb, tol;     // |r|^2, |b|^2, relative tolerance
+  double alpha, beta;     // step and direction coefficients of the iteration
+  double mx, my;          // mean of H p over the vertices (removed: translations)
+  long long iters, max_iters;
+  int done;               // converged, iteration limit, or non-positive curvature
+  int bad;                // 1: a non-positive curvature p.Hp was met
+};
+struct CgArgs {
+  int nv;
+  double* x;
+  double* r;
+  double* p;
+  double* hp;
+  const double* fhd;  // hyper-dual forces of the H p launch
+  CgState* st;
+  double* partials;   // [nblk][4]
+  int nblk;
+};
+void launch_cg_iteration(cudaStream_t st, const CgArgs& a);
+int cg_blocks(int nv);
 void launch_dot_partials(cudaStream_t st, int n, const double* a, const double* b, double* out, int nblocks);
 void launch_axpby(cudaStream_t st, int n, double a, const double* x, double b, double* y);
 void launch_extract_hv(cudaStream_t st, int nv, const double* fhd, double* hv);
