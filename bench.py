@@ -54,9 +54,9 @@ def parse():
     ap.add_argument("--no-batch", action="store_true",
                     help="skip the batched-systems FIRE / compression measurement")
     ap.add_argument("--batch-systems", type=int, default=256)
-    ap.add_argument("--no-rigid", action="store_true", help="skip the rigid-ellipse (config 2) measurement")
+    ap.add_argument("--no-rigid", action="store_true", help="skip the rigid-ellipse measurement")
     ap.add_argument("--rigid-steps", type=int, default=2000)
-    ap.add_argument("--no-diff", action="store_true", help="skip the derivative (config 4) measurement")
+    ap.add_argument("--no-diff", action="store_true", help="skip the derivative measurement")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--save-state", default=None, help="write the prepared state (npz) after preparation")
     ap.add_argument("--load-state", default=None, help="start from a state written by --save-state")
@@ -80,7 +80,7 @@ def prepared_state(args, rank):
 
     if args.load_state:
         z = np.load(args.load_state)
-        c = synth.workload_config(1, len(z["nv_list"]))
+        c = synth.workload_config("smooth_lj", len(z["nv_list"]))
         pk = synth.Packing(nv_list=z["nv_list"], pos=z["pos"], vel=z["vel"], rad=z["rad"], l0=z["l0"],
                            theta0=z["theta0"], a0=z["a0"], box=z["box"], centres=np.zeros((len(z["nv_list"]), 2)))
         kw = {k: c[k] for k in ("potential", "interaction", "ea", "el", "eb", "ec", "LJcutoff", "dt")}
@@ -94,13 +94,13 @@ def prepared_state(args, rank):
         # large systems: the prepared 1024-ring packing replicated k x k times
         # (a periodic image tiling is itself a packing at the same phi); the
         # thermal velocities drawn afterwards decorrelate the copies
-        d0, info = workloads.prepared_deformable(1, 1024, seed=20261203 + rank)
+        d0, info = workloads.prepared_deformable("smooth_lj", 1024, seed=20261203 + rank)
         k = int(round((args.rings // 1024) ** 0.5))
         d = workloads.tile_system(d0, k, info["config"])
         d0.close()
         info = dict(info, tiled=f"{k}x{k} copies of the 1024-ring packing")
     else:
-        d, info = workloads.prepared_deformable(1, args.rings, seed=20261203 + rank)
+        d, info = workloads.prepared_deformable("smooth_lj", args.rings, seed=20261203 + rank)
     if args.save_state and not args.load_state:
         nvl = d.numVertexInParticleList
         np.savez(args.save_state, nv_list=nvl, pos=d.getVertexPositions(), vel=d.getVertexVelocities(),
@@ -467,7 +467,7 @@ def main():
 
 
 def derivative_measurement() -> dict:
-    """Config 4 of the benchmark list (differentiation): 256 rings of 32
+    """The differentiation workload: 256 rings of 32
     vertices, harmonic, phi 0.88, FIRE-minimised to max |F| <= 1e-12; wall
     times of the minimised-state gradients of U and P along (ea, el, eb, calA0)
     (two conjugate-gradient Hessian solves to 1e-10), of Hessian-vector
@@ -478,7 +478,7 @@ def derivative_measurement() -> dict:
     from cudaring_b200 import diff, workloads
 
     t0 = time.perf_counter()
-    d, info = workloads.prepared_deformable(4)
+    d, info = workloads.prepared_deformable("dense_harmonic")
     c = info["config"]
     sig = d.getMeanParticleSize()
     d.initFIRE([0.2, 0.5, 1.1, 0.99, 1e-3 * sig, 1e-2 * sig, 0.2], 20, 0, d.numVertices)
@@ -692,7 +692,7 @@ def run_reference_arm(args, world, rank):
     # same prepared state, built on the GPU when one is present, else on the CPU port
     from cudaring_b200 import workloads
 
-    d, info = workloads.prepared_deformable(1, args.rings, seed=20261203)
+    d, info = workloads.prepared_deformable("smooth_lj", args.rings, seed=20261203)
     c = info["config"]
     R = oracle.ref()
     nvl = d.numVertexInParticleList

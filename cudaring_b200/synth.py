@@ -216,38 +216,39 @@ def make_ellipse_packing(n: int, nv: int, ratio_range: tuple[float, float], phi:
                    centres=centres, meta={"seed": seed, "phi": phi, "ratios": ratios, "placement": placement})
 
 
-def workload_config(index: int, scale_rings: int | None = None) -> dict:
-    """Ring counts and parameters of the five benchmark configurations.
+def workload_config(name: str, scale_rings: int | None = None) -> dict:
+    """Ring counts and parameters of the benchmark workloads, by name.
 
-    index 0: 32 rings, nv 16/22 bidisperse 1:1.4, harmonic, calA0 1.0, phi 0.70.
-    index 1: 1024 rings, nv 32/45 (1:1.4), smooth LJ rc 2.5, calA0 1.05, phi 0.85;
-             the shape constants are those of the reference's NVE driver
-             (ea 1e5, el 20, eb 10; runNVE.cpp:39), stiff enough that the LJ
-             well (epsilon 1) does not crumple the rings.
-    index 2: 4096 rigid ellipses, 24 vertices, WCA, phi 0.65.
-    index 3: batched FIRE compression (see the batch module).
-    index 4: 256 rings, nv 32, harmonic, phi 0.88.
+    "bidisperse_harmonic": 32 rings, nv 16/22 bidisperse 1:1.4, harmonic,
+        calA0 1.0, phi 0.70.
+    "smooth_lj": 1024 rings, nv 32/45 (1:1.4), smooth LJ rc 2.5, calA0 1.05,
+        phi 0.85; the shape constants are those of the reference's NVE driver
+        (ea 1e5, el 20, eb 10; runNVE.cpp:39), stiff enough that the LJ well
+        (epsilon 1) does not crumple the rings.
+    "rigid_ellipses": 4096 rigid ellipses, 24 vertices, WCA, phi 0.65.
+    "dense_harmonic": 256 rings, nv 32, harmonic, phi 0.88 (derivatives).
+    The batched FIRE compression workload lives in the batch module.
     ``scale_rings`` overrides the ring count (even split small/large).
     """
-    if index == 0:
+    if name == "bidisperse_harmonic":
         n = scale_rings or 32
         nv = [16] * (n // 2) + [22] * (n - n // 2)
         a0 = [1.0] * (n // 2) + [1.4 ** 2] * (n - n // 2)
         return dict(nv=nv, a0=a0, calA0=1.0, phi=0.70, potential="harmonic", interaction="vertexVertex",
                     ea=1.0, el=1.0, eb=0.01, ec=1.0, dt=0.005, T=1e-3)
-    if index == 1:
+    if name == "smooth_lj":
         n = scale_rings or 1024
         nv = [32] * (n // 2) + [45] * (n - n // 2)
         a0 = [1.0] * (n // 2) + [1.4 ** 2] * (n - n // 2)
         return dict(nv=nv, a0=a0, calA0=1.05, phi=0.85, potential="lennardJones", interaction="vertexSmooth",
                     LJcutoff=2.5, ea=1e5, el=20.0, eb=10.0, ec=1.0, dt=0.002, T=0.01)
-    if index == 2:
+    if name == "rigid_ellipses":
         n = scale_rings or 4096
         return dict(rigid=True, n=n, nv=24, ratio_range=(1.2, 2.0), phi=0.65, potential="wca",
                     interaction="vertexVertex", ea=0.0, el=0.0, eb=0.0, ec=1.0, dt=0.001, T=0.1, gamma=1.0,
                     driving=0.1, taup=100.0)
-    if index == 4:
+    if name == "dense_harmonic":
         n = scale_rings or 256
         return dict(nv=[32] * n, a0=[1.0] * n, calA0=1.0, phi=0.88, potential="harmonic",
                     interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0, dt=0.002, T=0.0)
-    raise ValueError(f"no deformable ring config {index}")
+    raise ValueError(f"unknown workload {name!r}")

@@ -86,14 +86,16 @@ def rescale_lengths(d: DPM2D, f: float) -> None:
     d.setRestAreas(d.getRestAreas() * f * f)
 
 
-def prepared_deformable(index: int = 1, rings: int | None = None, seed: int = 20261203, phi_start: float = 0.40,
+def prepared_deformable(workload: str = "smooth_lj", rings: int | None = None, seed: int = 20261203,
+                        phi_start: float = 0.40,
                         placement: str | None = None) -> tuple[DPM2D, dict]:
-    """A relaxed packing of deformable-ring config ``index`` at its target phi.
+    """A relaxed packing of a deformable-ring workload at its target phi.
 
-    index 1: 1024 rings nv 32/45, smooth vertex-segment LJ (rc 2.5), calA0
-    1.05, phi 0.85.  ``rings`` scales the ring count (even small/large split).
+    "smooth_lj": 1024 rings nv 32/45, smooth vertex-segment LJ (rc 2.5),
+    calA0 1.05, phi 0.85.  ``rings`` scales the ring count (even small/large
+    split).
     """
-    c = synth.workload_config(index, rings)
+    c = synth.workload_config(workload, rings)
     n = len(c["nv"])
     if placement is None:
         placement = "rsa" if n <= 4096 else "lattice"
@@ -132,7 +134,7 @@ def prepared_deformable(index: int = 1, rings: int | None = None, seed: int = 20
 
 def prepared_ellipses(n: int | None = None, seed: int = 20261205, phi_start: float = 0.2, dphi: float = 0.01,
                       relax_steps: int = 200, ec_compress: float = 100.0, wca_steps: int = 3000) -> tuple[DPM2D, dict]:
-    """Rigid bumpy ellipses of config 2 (4096 rings of 24 vertices, aspect
+    """Rigid bumpy ellipses (4096 rings of 24 vertices, aspect
     ratio U[1.2, 2.0], WCA) at their target rigid packing fraction.
 
     Rings are placed without overlap at ``phi_start`` and compressed affinely
@@ -144,7 +146,7 @@ def prepared_ellipses(n: int | None = None, seed: int = 20261205, phi_start: flo
     """
     import time
 
-    c = synth.workload_config(2, n)
+    c = synth.workload_config("rigid_ellipses", n)
     t0 = time.perf_counter()
     pk = synth.make_ellipse_packing(c["n"], c["nv"], c["ratio_range"], phi_start, seed=seed)
     d = DPM2D.from_packing(pk, potential="harmonic", interaction=c["interaction"], ec=ec_compress, dt=c["dt"])

@@ -27,15 +27,15 @@ OUT = os.path.dirname(os.path.abspath(__file__))
 
 # Force/energy/neighbour cases: (name, rings, potential, interaction, placement, phi, extra)
 FORCE_CASES = [
-    ("harmonic_vv_cfg0", dict(cfg=0), "harmonic", "vertexVertex", "uniform", 0.70, {}),
-    ("harmonic_smooth", dict(cfg=1, n=48), "harmonic", "vertexSmooth", "uniform", 0.80, {}),
-    ("lj_smooth", dict(cfg=1, n=64), "lennardJones", "vertexSmooth", "rsa", 0.40, {}),
-    ("lj_vv", dict(cfg=1, n=64), "lennardJones", "vertexVertex", "rsa", 0.40, {}),
+    ("harmonic_vv_bidisperse", dict(workload="bidisperse_harmonic"), "harmonic", "vertexVertex", "uniform", 0.70, {}),
+    ("harmonic_smooth", dict(workload="smooth_lj", n=48), "harmonic", "vertexSmooth", "uniform", 0.80, {}),
+    ("lj_smooth", dict(workload="smooth_lj", n=64), "lennardJones", "vertexSmooth", "rsa", 0.40, {}),
+    ("lj_vv", dict(workload="smooth_lj", n=64), "lennardJones", "vertexVertex", "rsa", 0.40, {}),
     ("wca_vv", dict(nv=24, n=64), "wca", "vertexVertex", "rsa", 0.40, {}),
     ("wca_smooth", dict(nv=24, n=64), "wca", "vertexSmooth", "rsa", 0.40, {}),
-    ("adhesive_vv", dict(cfg=0), "adhesive", "vertexVertex", "uniform", 0.70, dict(l1=0.1, l2=0.3)),
-    ("adhesive_smooth", dict(cfg=0), "adhesive", "vertexSmooth", "uniform", 0.70, dict(l1=0.1, l2=0.3)),
-    ("fene_vv", dict(cfg=0), "harmonic", "vertexVertex", "uniform", 0.70, dict(monomer=1, stiff=1.0, ext=1.5)),
+    ("adhesive_vv", dict(workload="bidisperse_harmonic"), "adhesive", "vertexVertex", "uniform", 0.70, dict(l1=0.1, l2=0.3)),
+    ("adhesive_smooth", dict(workload="bidisperse_harmonic"), "adhesive", "vertexSmooth", "uniform", 0.70, dict(l1=0.1, l2=0.3)),
+    ("fene_vv", dict(workload="bidisperse_harmonic"), "harmonic", "vertexVertex", "uniform", 0.70, dict(monomer=1, stiff=1.0, ext=1.5)),
 ]
 
 FIELDS = {"pos": 0, "vel": 1, "force": 2, "energy": 3, "p_energy": 4, "area": 5, "perimeter": 6,
@@ -43,8 +43,8 @@ FIELDS = {"pos": 0, "vel": 1, "force": 2, "energy": 3, "p_energy": 4, "area": 5,
 
 
 def packing_for(spec, phi, placement, seed):
-    if "cfg" in spec:
-        c = synth.workload_config(spec["cfg"], spec.get("n"))
+    if "workload" in spec:
+        c = synth.workload_config(spec["workload"], spec.get("n"))
         nv, a0, calA0 = c["nv"], c["a0"], c["calA0"]
     else:
         n = spec["n"]
@@ -113,8 +113,8 @@ def force_cases():
 
 
 def traj_cases():
-    # NVE on config-0 geometry with ring-rigid velocities large enough to trigger rebuilds.
-    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 200)
+    # NVE on the 32-ring bidisperse harmonic geometry with ring-rigid velocities large enough to trigger rebuilds.
+    pk = packing_for(dict(workload="bidisperse_harmonic"), 0.70, "uniform", seed=20261203 + 200)
     rng = np.random.default_rng(7)
     pk.vel = np.repeat(rng.normal(0.0, 0.3, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
     dt, nsteps = 0.005, 200
@@ -134,7 +134,7 @@ def traj_cases():
     print(f"traj_nve_harmonic_vv: updates={int(d['out_update_count'])}")
 
     # NVE, smooth LJ, 64 rings.
-    pk = packing_for(dict(cfg=1, n=64), 0.40, "rsa", seed=20261203 + 201)
+    pk = packing_for(dict(workload="smooth_lj", n=64), 0.40, "rsa", seed=20261203 + 201)
     pk.vel = np.repeat(rng.normal(0.0, 0.3, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
     dt, nsteps = 0.002, 150
     R, cut = setup_ref(pk, "lennardJones", "vertexSmooth")
@@ -151,8 +151,8 @@ def traj_cases():
     np.savez_compressed(os.path.join(OUT, "traj_nve_lj_smooth.npz"), **d)
     print(f"traj_nve_lj_smooth: updates={int(d['out_update_count'])}")
 
-    # FIRE on config-0 geometry.
-    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 202)
+    # FIRE on the 32-ring bidisperse harmonic geometry.
+    pk = packing_for(dict(workload="bidisperse_harmonic"), 0.70, "uniform", seed=20261203 + 202)
     R, cut = setup_ref(pk, "harmonic", "vertexVertex")
     dt = 0.01
     params = np.array([0.2, 0.5, 1.1, 0.99, dt, 10 * dt, 0.2])
@@ -174,7 +174,7 @@ def traj_cases():
     print(f"traj_fire_harmonic_vv: maxF={float(d['out_max_unbalanced_force']):.3e} state={st}")
 
     # Langevin with the library's Philox noise (seed, streams 2s) injected.
-    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 203)
+    pk = packing_for(dict(workload="bidisperse_harmonic"), 0.70, "uniform", seed=20261203 + 203)
     pk.vel = np.repeat(rng.normal(0.0, 0.1, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
     dt, nsteps, T, gamma, seed = 0.005, 60, 0.01, 1.0, 12345
     R, cut = setup_ref(pk, "harmonic", "vertexVertex")
@@ -201,7 +201,7 @@ def stochastic_cases():
     # Philox draws (seed, stream 2s for the thermostat of step s, 2s+1 for the
     # self-propulsion angle) injected into the reference kernels.
     seed = 4242
-    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 204)
+    pk = packing_for(dict(workload="bidisperse_harmonic"), 0.70, "uniform", seed=20261203 + 204)
     rng = np.random.default_rng(5)
     vel = np.repeat(rng.normal(0.0, 0.1, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
     npart = pk.num_particles
@@ -303,7 +303,7 @@ def rigid_cases():
 
 def rescale_cases():
     # NVE with velocity rescaling to Tinject before every step (NVERescale).
-    pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 205)
+    pk = packing_for(dict(workload="bidisperse_harmonic"), 0.70, "uniform", seed=20261203 + 205)
     rng = np.random.default_rng(9)
     pk.vel = np.repeat(rng.normal(0.0, 0.1, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
     dt, nsteps, Tinject = 0.005, 120, 0.02
@@ -328,7 +328,7 @@ def soft_cases():
     cases = [("harmonic", 0, 1.0, 0.8, dict(), True), ("wca", 3, 1.0, 0.35, dict(), False),
              ("lj", 1, 3.0, 0.35, dict(lj=2.5), False)]
     for name, pot, cut, phi0, extra, full in cases:
-        pk = packing_for(dict(cfg=0), 0.70, "uniform", seed=20261203 + 301)
+        pk = packing_for(dict(workload="bidisperse_harmonic"), 0.70, "uniform", seed=20261203 + 301)
         extra_rad, seed = 1.1, 4242
         R = oracle.ref()
         R.ref_create(pk.num_particles, pk.nv_list)

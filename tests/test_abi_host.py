@@ -66,7 +66,7 @@ def test_ring_rest_shape_matches_reference_formula():
 
 
 def test_packing_phi_and_orientation():
-    c = synth.workload_config(1)
+    c = synth.workload_config("smooth_lj")
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], c["phi"], seed=1)
     assert pk.num_vertices == 512 * 32 + 512 * 45 == 39424
     assert synth.preferred_phi(pk.nv_list, pk.a0, pk.rad, pk.box) == pytest.approx(0.85, rel=1e-12)

@@ -10,7 +10,7 @@ from oracle.integrators import OracleState, nve_adjoint_reference
 
 
 def test_verlet_adjoint_matches_trajectory_differences():
-    c = synth.workload_config(0, 4)
+    c = synth.workload_config("bidisperse_harmonic", 4)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.6, seed=3, placement="uniform")
     pk.rad = pk.rad * 1.2
     pk.vel = np.repeat(np.random.default_rng(1).normal(0, 0.05, size=(4, 2)), pk.nv_list, axis=0).reshape(-1)

@@ -21,10 +21,10 @@ from conftest import rel_inf
 pytestmark = pytest.mark.gpu
 
 
-def _systems(cfg, sizes, phi, seed, placement="rsa", rad_scale=1.0):
+def _systems(workload, sizes, phi, seed, placement="rsa", rad_scale=1.0):
     out = []
     for k, n in enumerate(sizes):
-        c = synth.workload_config(cfg, n)
+        c = synth.workload_config(workload, n)
         pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=seed + k, placement=placement)
         pk.rad = pk.rad * rad_scale
         out.append(pk)
@@ -39,11 +39,12 @@ def _single(pk, **kw):
     return d
 
 
-@pytest.mark.parametrize("potential,interaction,cfg,rad_scale", [
-    ("harmonic", "vertexVertex", 0, 1.5), ("lennardJones", "vertexSmooth", 1, 1.0), ("wca", "vertexSmooth", 1, 1.3)])
+@pytest.mark.parametrize("potential,interaction,workload,rad_scale", [
+    ("harmonic", "vertexVertex", "bidisperse_harmonic", 1.5), ("lennardJones", "vertexSmooth", "smooth_lj", 1.0),
+    ("wca", "vertexSmooth", "smooth_lj", 1.3)])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_batch_forces_match_single(cuda_device, potential, interaction, cfg, rad_scale, precision):
-    pks = _systems(cfg, [8, 24, 40, 16, 64], 0.40, seed=101, rad_scale=rad_scale)
+def test_batch_forces_match_single(cuda_device, potential, interaction, workload, rad_scale, precision):
+    pks = _systems(workload, [8, 24, 40, 16, 64], 0.40, seed=101, rad_scale=rad_scale)
     kw = dict(potential=potential, interaction=interaction, ea=1.0, el=1.0, eb=0.01, ec=1.0, LJcutoff=2.5)
     b = Batch.from_packings(pks, **kw)
     b.setPrecision(precision)
@@ -72,7 +73,7 @@ def test_batch_forces_match_single(cuda_device, potential, interaction, cfg, rad
 
 
 def test_batch_fire_matches_single(cuda_device):
-    pks = _systems(0, [16, 32, 20], 0.70, seed=7, placement="uniform")
+    pks = _systems("bidisperse_harmonic", [16, 32, 20], 0.70, seed=7, placement="uniform")
     kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
     b = Batch.from_packings(pks, **kw)
     b.setDisplacementCutoff(0.5)
@@ -94,7 +95,7 @@ def test_batch_fire_matches_single(cuda_device):
 
 
 def test_batch_scale_matches_single(cuda_device):
-    pks = _systems(0, [16, 24], 0.40, seed=3)
+    pks = _systems("bidisperse_harmonic", [16, 24], 0.40, seed=3)
     kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
     b = Batch.from_packings(pks, **kw)
     b.setDisplacementCutoff(0.5)
@@ -132,7 +133,7 @@ def test_batch_compress_matches_per_system_loop(cuda_device):
 
 
 def test_batch_autotune_and_lanes(cuda_device):
-    pks = _systems(1, [16, 32], 0.40, seed=9)
+    pks = _systems("smooth_lj", [16, 32], 0.40, seed=9)
     kw = dict(potential="lennardJones", interaction="vertexSmooth", ea=1.0, el=1.0, eb=0.01, ec=1.0, LJcutoff=2.5)
     b = Batch.from_packings(pks, **kw)
     b.setDisplacementCutoff(0.5)

@@ -20,7 +20,7 @@ KW = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0
 
 
 def _system(n=16, phi=0.70, seed=4, rad_scale=1.3, placement="uniform", **kw):
-    c = synth.workload_config(0, n)
+    c = synth.workload_config("bidisperse_harmonic", n)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=seed, placement=placement)
     pk.rad = pk.rad * rad_scale  # overlapping rings: every term of U acts
     args = dict(KW, **kw)
@@ -228,7 +228,7 @@ def _minimised(pk, theta, want_grad=False):
 @pytest.fixture(scope="module")
 def jammed_packing(cuda_device):
     # rings nv 32, harmonic, above jamming (phi 0.88), relaxed; calA0 = 1 at the reference point
-    d, info = workloads.prepared_deformable(4, 16, seed=21)
+    d, info = workloads.prepared_deformable("dense_harmonic", 16, seed=21)
     pk = synth.Packing(nv_list=d.numVertexInParticleList, pos=d.getVertexPositions(),
                        vel=np.zeros(2 * d.numVertices), rad=d.getVertexRadii(), l0=d.getRestLengths(),
                        theta0=d.getRestAngles(), a0=d.getRestAreas(), box=d.getBoxSize(),

@@ -40,7 +40,7 @@ def test_list_overflow_inside_a_step_sequence_resumes_exactly(cuda_device):
     # capacity: the chunk aborts, the host grows the list and resumes from the
     # failed build.  Context B starts with a large capacity.  The two runs must
     # be identical.
-    c = synth.workload_config(0, 64)
+    c = synth.workload_config("bidisperse_harmonic", 64)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.85, seed=17, placement="uniform")
     out = []
     for grow_first in (False, True):

@@ -42,7 +42,7 @@ def _forces(d, precision):
 def thermal_state(cuda_device):
     # 256 rings of the smooth-LJ deformable workload, relaxed by FIRE at
     # phi 0.85 and thermalised by 300 NVE steps at T = 0.01
-    d, info = workloads.prepared_deformable(1, 256, seed=77)
+    d, info = workloads.prepared_deformable("smooth_lj", 256, seed=77)
     d.initNVE(0.01)
     d.NVELoop(300)
     z = dict(nv_list=d.numVertexInParticleList, pos=d.getVertexPositions(), vel=d.getVertexVelocities(),
@@ -84,7 +84,7 @@ def test_thermal_state_force_error(thermal_state, lanes, interaction, bar):
     ("lennardJones", "vertexSmooth"), ("wca", "vertexVertex"), ("wca", "vertexSmooth"),
     ("adhesive", "vertexVertex"), ("adhesive", "vertexSmooth")])
 def test_pair_only_force_error(cuda_device, potential, interaction):
-    c = synth.workload_config(1, 64)
+    c = synth.workload_config("smooth_lj", 64)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.40, seed=3, placement="rsa")
     # radii enlarged so that rings of every potential overlap their neighbours
     pk.rad = pk.rad * 1.8

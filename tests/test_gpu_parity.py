@@ -172,7 +172,7 @@ def test_stochastic_integrators_match_reference(cuda_device, kind):
 
 
 def _lj_smooth_packing(n, phi=0.40, seed=5, placement="rsa"):
-    c = synth.workload_config(1, n)
+    c = synth.workload_config("smooth_lj", n)
     return c, synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=seed, placement=placement)
 
 
@@ -217,7 +217,7 @@ def test_stiff_area_constant_within_reference_conditioning(cuda_device):
 
 def test_full_size_config_neighbor_sets_and_forces(cuda_device):
     # 1024 rings, nv 32/45 (39,424 vertices), smooth LJ rc 2.5, phi 0.85
-    c = synth.workload_config(1)
+    c = synth.workload_config("smooth_lj")
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], c["phi"], seed=20261204)
     d = DPM2D.from_packing(pk, **{k: c[k] for k in ("potential", "interaction", "ea", "el", "eb", "ec", "LJcutoff")})
     cut = d.setDisplacementCutoff(0.5, 2 * pk.rad.mean())

@@ -38,7 +38,7 @@ def _run_reference(dirname, npart, steps, dt, ea, el, eb, pot, inter, out):
 @pytest.mark.skipif(not os.path.exists(BIN), reason="reference CUDA build not present")
 @pytest.mark.parametrize("pot,inter", [("lj", "smooth"), ("harmonic", "vertex")])
 def test_nve_matches_reference_cuda_build(cuda_device, tmp_path, pot, inter):
-    c = synth.workload_config(1, 64)
+    c = synth.workload_config("smooth_lj", 64)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.40, seed=31, placement="rsa")
     rng = np.random.default_rng(2)
     pk.vel = np.repeat(rng.normal(0.0, 0.3, size=(pk.num_particles, 2)), pk.nv_list, axis=0).reshape(-1)
@@ -71,7 +71,7 @@ def test_nve_matches_reference_cuda_build(cuda_device, tmp_path, pot, inter):
 
 
 def test_save_packing_from_context_round_trip(cuda_device, tmp_path):
-    c = synth.workload_config(1, 8)
+    c = synth.workload_config("smooth_lj", 8)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.40, seed=5, placement="rsa")
     m = DPM2D.from_packing(pk, potential="lennardJones", interaction="vertexSmooth", ea=1.0, el=1.0, eb=0.01)
     m.calcNeighborList(m.setDisplacementCutoff(0.5, 2.0 * m.getMeanVertexRadius()))

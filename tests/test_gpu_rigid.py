@@ -49,7 +49,7 @@ def test_rigid_nve_trajectory(cuda_device, chunks):
 
 def test_rigid_langevin_temperature(cuda_device):
     # corrected thermostat: ring kinetic energy per translational degree of freedom -> T/2
-    c = synth.workload_config(2, 256)
+    c = synth.workload_config("rigid_ellipses", 256)
     pk = synth.make_ellipse_packing(c["n"], c["nv"], c["ratio_range"], 0.2, seed=5)
     d = DPM2D.from_packing(pk, potential="wca", interaction="vertexVertex", ec=1.0, dt=0.002)
     d.setShapeType(simControl.shapeEnum.rigid)
@@ -70,7 +70,7 @@ def test_rigid_langevin_temperature(cuda_device):
 def test_rigid_mixed_precision_forces_and_langevin(cuda_device):
     # FP32 vertex pair terms on FP64 offsets: forces and torques within FP32
     # rounding of the FP64 path; a Langevin run stays finite and at temperature
-    c = synth.workload_config(2, 256)
+    c = synth.workload_config("rigid_ellipses", 256)
     pk = synth.make_ellipse_packing(c["n"], c["nv"], c["ratio_range"], 0.25, seed=6)
     d = DPM2D.from_packing(pk, potential="wca", interaction="vertexVertex", ec=1.0, dt=0.001)
     d.setShapeType(simControl.shapeEnum.rigid)

@@ -106,7 +106,7 @@ def test_vertices_on_particles_match_reference(cuda_device):
 def test_cell_list_build_and_forces_match_oracle(cuda_device, phi0):
     # 1024 rings: the particle cells are many per side, so the cell-list path
     # (not the brute-force one of the 32-ring fixtures) builds the list
-    c = synth.workload_config(1)
+    c = synth.workload_config("smooth_lj")
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.85, seed=11, placement="uniform")
     pk.box = np.array([1.0, 1.0])
     with DPM2D.from_packing(pk) as d:
@@ -125,7 +125,7 @@ def test_cell_list_build_and_forces_match_oracle(cuda_device, phi0):
 
 def test_soft_prepack_driver_end_to_end(cuda_device):
     # compressFIRE.cpp:53-86 in one call on 1024 rings, then the vertex model
-    c = synth.workload_config(1)
+    c = synth.workload_config("smooth_lj")
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.85, seed=12, placement="uniform")
     pk.box = np.array([1.0, 1.0])
     with DPM2D.from_packing(pk) as d:

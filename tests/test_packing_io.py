@@ -7,7 +7,7 @@ from cudaring_b200 import packing_io, synth
 
 
 def _packing():
-    c = synth.workload_config(0, 8)
+    c = synth.workload_config("bidisperse_harmonic", 8)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.5, seed=3, placement="rsa")
     pk.vel = np.random.default_rng(0).normal(size=pk.pos.shape)
     return pk

@@ -33,7 +33,7 @@ def _rows(nbr_slot_major, cnt, nv, width):
 def test_noalloc_matches_context_build_twice(cuda_device, rings, phi):
     import torch
 
-    c = synth.workload_config(1, rings)
+    c = synth.workload_config("smooth_lj", rings)
     pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], phi, seed=31, placement="rsa")
     d = DPM2D.from_packing(pk, **{k: c[k] for k in ("potential", "interaction", "ea", "el", "eb", "ec", "LJcutoff")})
     cut = d.setDisplacementCutoff(0.5, 2 * pk.rad.mean())
