@@ -21,6 +21,35 @@
 
 namespace cr {
 
+// Programmatic dependent launch.  A kernel launched with launch_k(pdl = true)
+// may be scheduled while the kernel before it in the stream is finishing;
+// pdl_wait() blocks until that kernel has completed and its writes are
+// visible (a no-op for an ordinary launch), so it comes before any read of
+// data the previous kernel writes.  pdl_trigger() lets the next kernel be
+// scheduled early; without it the next kernel starts when this one exits.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(bool pdl, void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                            Args&&... args) {
+  if (!pdl) {
+    kernel<<<grid, block, 0, st>>>(static_cast<KArgs>(args)...);
+    return cudaSuccess;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 constexpr double kPi = 3.141592653589793238462643383279502884197;
 constexpr double kWCAcut = 1.122462048;  // include/defs.h:17 of the reference
 

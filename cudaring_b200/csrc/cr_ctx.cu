@@ -493,6 +493,7 @@ void enqueue_op(cr_ctx* ctx, cudaStream_t st, const Op& op, int kind, bool use_c
     case OP_TILE: {
       LaunchCfg c = tile_cfg(ctx);
       c.stream = st;
+      c.pdl = true;
       if (ctx->shape == CR_SHAPE_RIGID) launch_rigid(c, ctx->potential, MODE_STEP, ctx->p, a, s, rigid_args(ctx));
       else launch_tile(c, ctx->potential, inter_kind(ctx), MODE_STEP, ctx->p, a, s);
       break;
@@ -521,7 +522,7 @@ int capture_graph(cr_ctx* ctx, const std::vector<Op>& ops, int kind, GraphEntry&
     if (op.check_after) {
       NbrArgs nb = nbr_args(ctx, op.check_buf, ctx->cut_distance);
       nb.count_update = 1;
-      launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nb, fb, 0);
+      launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nb, fb, 0, ctx->shape != CR_SHAPE_RIGID);
       ge.launches++;
     }
   }

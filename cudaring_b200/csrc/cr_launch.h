@@ -13,6 +13,7 @@ struct LaunchCfg {
   int grid;    // number of tiles / CTAs
   int lanes;   // lanes per vertex in the pair phase (1, 2, 4, 8)
   int precision = CR_PRECISION_FP64;  // CR_PRECISION_* (deformable tile kernel)
+  bool pdl = false;   // programmatic dependent launch (inside step graphs)
 };
 
 // cr_tile.cu
@@ -160,8 +161,9 @@ void launch_nbr_build(cudaStream_t st, const SysParams& p, const CellGrid& g, co
 // The whole build in one launch of `blocks` CTAs (at most nbr_fused_max_blocks()).
 // force = 0: return at once unless the status block armed a rebuild (and no
 // abort or convergence is pending), so it can follow every step op in a graph.
+// pdl: programmatic dependent launch after the step kernel (inside graphs).
 void launch_nbr_fused(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n, int blocks,
-                      int force);
+                      int force, bool pdl = false);
 // CTAs of the one-launch build that the current device holds at once.
 int nbr_fused_max_blocks();
 // Grid of the one-launch build for nv vertices.

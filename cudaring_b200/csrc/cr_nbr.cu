@@ -563,6 +563,10 @@ __device__ __forceinline__ int block_scan(int x, int* total) {
 
 __global__ void __launch_bounds__(kFusedBlock, kFusedMinBlocks)
     k_nbr_fused(const __grid_constant__ SysParams p, int ncx, int ncy, const __grid_constant__ NbrArgs n, int force) {
+  // the status block and positions come from the step kernel before this
+  // launch; the next kernel starts when this one exits (no early trigger, so
+  // no later grid can take the SMs that the grid barriers need)
+  pdl_wait();
   DevStatus* st = n.status;
   if (!force) {
     const volatile DevStatus* vs = st;
@@ -658,8 +662,8 @@ int nbr_fused_blocks(int nv, int max_blocks) {
 }
 
 void launch_nbr_fused(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n, int blocks,
-                      int force) {
-  k_nbr_fused<<<blocks, kFusedBlock, 0, st>>>(p, g.ncx, g.ncy, n, force);
+                      int force, bool pdl) {
+  launch_k(pdl, k_nbr_fused, dim3(blocks), dim3(kFusedBlock), st, p, g.ncx, g.ncy, n, force);
 }
 
 }  // namespace cr

@@ -7,10 +7,10 @@ namespace cr {
 
 template <int POT, int INTER, int MODE>
 static void launch_tile_t(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s) {
-  if (c.lanes == 1) k_tile<POT, INTER, MODE, 128, 1, PREC_FP64><<<c.grid, 128, 0, c.stream>>>(p, a, s);
-  else if (c.lanes == 4) k_tile<POT, INTER, MODE, 256, 4, PREC_FP64><<<c.grid, 256, 0, c.stream>>>(p, a, s);
-  else if (c.lanes == 8) k_tile<POT, INTER, MODE, 256, 8, PREC_FP64><<<c.grid, 256, 0, c.stream>>>(p, a, s);
-  else k_tile<POT, INTER, MODE, 192, 2, PREC_FP64><<<c.grid, 192, 0, c.stream>>>(p, a, s);
+  if (c.lanes == 1) launch_k(c.pdl, k_tile<POT, INTER, MODE, 128, 1, PREC_FP64>, dim3(c.grid), dim3(128), c.stream, p, a, s);
+  else if (c.lanes == 4) launch_k(c.pdl, k_tile<POT, INTER, MODE, 256, 4, PREC_FP64>, dim3(c.grid), dim3(256), c.stream, p, a, s);
+  else if (c.lanes == 8) launch_k(c.pdl, k_tile<POT, INTER, MODE, 256, 8, PREC_FP64>, dim3(c.grid), dim3(256), c.stream, p, a, s);
+  else launch_k(c.pdl, k_tile<POT, INTER, MODE, 192, 2, PREC_FP64>, dim3(c.grid), dim3(192), c.stream, p, a, s);
 }
 
 void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p_in, const SysArrays& a,

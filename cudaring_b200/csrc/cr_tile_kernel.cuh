@@ -97,6 +97,11 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
   __shared__ Box s_box;
   __shared__ bool s_syslast;
 
+  // every input may come from the kernel before this one (positions, lists,
+  // status); the next kernel (the rebuild check) may be scheduled at once and
+  // waits for this one's completion itself
+  pdl_wait();
+  pdl_trigger();
   DevStatus* st = s.status;
   if (MODE == MODE_STEP && (st->abort | st->converged)) {
     // keep the last-block protocol intact so later ops see a consistent counter
