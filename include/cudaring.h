@@ -319,11 +319,12 @@ int cr_profile_step_kernel(cr_ctx* ctx, long reps, double* ms_per_launch);
 
 /* ---- tuning (no reference counterpart: launch shape of the fused kernel) -- */
 /* Lanes per vertex in the pair phase of the fused kernel (1, 2, 4 or 8);
- * tiles hold 128, 64, 64 or 32 vertices of whole rings respectively. */
+ * tiles hold 128, 96, 64 or 32 vertices of whole rings respectively. */
 int cr_set_lanes(cr_ctx* ctx, int lanes);
 int cr_get_lanes(const cr_ctx* ctx, int* lanes);
-/* 1: step sequences run as captured CUDA graphs with conditional rebuild
- * nodes (default); 0: direct launches with a host check after each op. */
+/* 1: step sequences run as captured CUDA graphs (default), every op that
+ * moved positions followed by the one-launch rebuild check; 0: direct
+ * launches with a host check after each op. */
 int cr_set_use_graphs(cr_ctx* ctx, int on);
 /* Times the fused step kernel for every lane count whose tile holds the
  * largest ring (cr_profile_step_kernel, `reps` launches each) and keeps the
