@@ -207,6 +207,13 @@ struct DevStatus {
   double sums[8];     // final reductions written by the last block
   unsigned int bar_count;  // grid barrier of the one-launch build: arrivals
   int stalled;        // a grid-barrier wait gave up (the build did not finish)
+  // multi-step kernel (k_tile_steps): barrier arrivals, the rotation base of
+  // its three per-step flag slots (bit 1: a rebuild is due, bit 2: a
+  // non-finite force), and the middle steps of the sequence still to run
+  unsigned int pbar;
+  int pflag[3];
+  long long pbase;
+  long long steps_left;
 };
 
 }  // namespace cr

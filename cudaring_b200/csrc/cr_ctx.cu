@@ -135,6 +135,7 @@ struct cr_ctx {
   bool fire_ready = false;
   FireParams fp{};
   bool use_graphs = true;
+  bool multistep = true;  // middle steps of NVE / Langevin / BAOAB runs in k_tile_steps
 
   std::map<std::tuple<int, long, int, int, unsigned long long>, GraphEntry> graphs;
 
@@ -333,6 +334,9 @@ int clear_flags(cr_ctx* ctx) {
   s.done_ctr = 0;
   s.bar_count = 0;
   s.stalled = 0;
+  s.pbar = 0;
+  s.pflag[0] = s.pflag[1] = s.pflag[2] = 0;
+  s.pbase = 0;
   *ctx->status_h = s;
   CR_TRY(cudaMemcpyAsync(ctx->status, ctx->status_h, sizeof(DevStatus), cudaMemcpyHostToDevice, ctx->stream));
   CR_TRY(cudaStreamSynchronize(ctx->stream));
@@ -578,6 +582,114 @@ int launch_chunk(cr_ctx* ctx, const std::vector<Op>& ops, int kind, long n) {
   return run_direct(ctx, ops, 0, kind);
 }
 
+// ---------------------------------------------------- multi-step sequences
+// NVE, Langevin and BAOAB runs of deformable rings: the drift op, then the
+// middle steps in k_tile_steps launches (each runs until its step budget, a
+// due rebuild or the end of the sequence; the one-launch build follows
+// every launch), then the final op.  Graphs of kStepsLaunches such pairs
+// are launched until the device counter of middle steps reaches zero; the
+// step arithmetic is the per-op path's, so results are identical to it.
+constexpr int kStepsPerLaunch = 64;
+constexpr int kStepsLaunches = 16;
+
+bool steps_eligible(cr_ctx* ctx, int kind, long nsteps) {
+  if (!ctx->multistep || !ctx->use_graphs || nsteps < 2) return false;
+  if (ctx->shape == CR_SHAPE_RIGID) return false;
+  if (kind != KIND_NVE && kind != KIND_LANGEVIN && kind != KIND_BAOAB) return false;
+  if (ctx->lanes != 1 && ctx->lanes != 2) return false;
+  const int maxb = tile_steps_max_blocks(ctx->potential, inter_kind(ctx), ctx->lanes, ctx->precision);
+  return maxb >= (int)ctx->tiles_h.size();
+}
+
+int capture_steps_graph(cr_ctx* ctx, int kind, int b, GraphEntry& ge) {
+  StepArgs s = base_args(ctx);
+  s.kind = kind;
+  s.pos_out = ctx->pos[b ^ 1];
+  s.advance = 1;
+  s.accumulate = 0;
+  s.write_out = 0;
+  s.persist_max = kStepsPerLaunch;
+  const SysArrays a = arrays(ctx, b);
+  LaunchCfg c = tile_cfg(ctx);
+  c.stream = ctx->stream;
+  c.pdl = true;
+  NbrArgs nb = nbr_args(ctx, b, ctx->cut_distance);
+  nb.count_update = 1;
+  const int fb = nbr_fused_blocks(ctx->nv, ctx->fused_max);
+  CR_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaSuccess;
+  for (int r = 0; r < kStepsLaunches && e == cudaSuccess; r++) {
+    e = launch_tile_steps(c, ctx->potential, inter_kind(ctx), ctx->p, a, s);
+    launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nb, fb, 0, true);
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &out);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&ge.exec, out, 0);
+  if (e != cudaSuccess) {
+    if (out) cudaGraphDestroy(out);
+    return ctx->fail(CR_ECUDA, std::string("multi-step graph: ") + cudaGetErrorString(e));
+  }
+  ge.graph = out;
+  ge.launches = 2 * kStepsLaunches;
+  return CR_OK;
+}
+
+int run_steps(cr_ctx* ctx, int kind, long nsteps) {
+  int rc;
+  int b = ctx->cur;
+  // drift (first half kick + drift) and its displacement check
+  enqueue_op(ctx, ctx->stream, Op{OP_DRIFT, b, b ^ 1, 0, 1, b ^ 1}, kind, false, 0);
+  {
+    NbrArgs nb = nbr_args(ctx, b ^ 1, ctx->cut_distance);
+    nb.count_update = 1;
+    launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nb, nbr_fused_blocks(ctx->nv, ctx->fused_max), 0);
+    ctx->launches++;
+  }
+  b ^= 1;
+  const long long middle = nsteps - 1;
+  CR_TRY(cudaMemcpyAsync(&ctx->status->steps_left, &middle, sizeof(middle), cudaMemcpyHostToDevice, ctx->stream));
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  for (;;) {
+    auto key = std::make_tuple(kind, -1L, b, ctx->cap, 1ULL);
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+      GraphEntry ge;
+      if ((rc = capture_steps_graph(ctx, kind, b, ge))) return rc;
+      it = ctx->graphs.emplace(key, ge).first;
+    }
+    CR_TRY(cudaGraphLaunch(it->second.exec, ctx->stream));
+    ctx->launches += it->second.launches;
+    if ((rc = read_status(ctx))) return rc;
+    const DevStatus& st = *ctx->status_h;
+    if (st.abort) {
+      if (st.stalled) return ctx->fail(CR_ECUDA, "a grid barrier timed out");
+      if (st.nonfinite) return ctx->fail(CR_ENONFINITE, "non-finite force during the step sequence");
+      if (!st.overflow) return ctx->fail(CR_ECUDA, "step sequence aborted");
+      // a rebuild found more neighbours than capacity: grow the list, rebuild
+      // from the positions the failed build read (pos[b]), count the update
+      // as the in-graph build would have, and carry on
+      if ((rc = clear_flags(ctx))) return rc;
+      ctx->cap = 0;
+      if ((rc = build_list(ctx, b, ctx->cut_distance))) return rc;
+      if ((rc = clear_flags(ctx))) return rc;
+      ctx->status_h->update_count += 1;
+      if ((rc = upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus)))) return rc;
+      continue;
+    }
+    if (st.steps_left <= 0) break;
+  }
+  // final op: forces at the last positions and the second half kick
+  enqueue_op(ctx, ctx->stream, Op{OP_TILE, b, b, 0, 0, b}, kind, false, 0);
+  CR_TRY(cudaGetLastError());
+  if ((rc = read_status(ctx))) return rc;
+  if (ctx->status_h->nonfinite) return ctx->fail(CR_ENONFINITE, "non-finite force during the step sequence");
+  ctx->cur = b;
+  if (ctx->status_h->max_ever > 0)
+    ctx->list_size_ref = std::max<long long>(ctx->list_size_ref, pow2ceil(ctx->status_h->max_ever));
+  return CR_OK;
+}
+
 // Runs nsteps integrator steps (or FIRE iterations) as chunks of captured
 // graphs.  Non-FIRE chunks are launched back to back with one status read at
 // the end; FIRE reads the status after every chunk to stop at convergence.
@@ -601,6 +713,7 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
     CR_TRY(cudaGetLastError());
   }
   if ((rc = clear_flags(ctx))) return rc;
+  if (steps_eligible(ctx, kind, nsteps)) return run_steps(ctx, kind, nsteps);
   const long chunk = 128;
   std::vector<std::vector<Op>> plan;
   std::vector<long> sizes;
@@ -1736,6 +1849,12 @@ int cr_set_precision(cr_ctx* ctx, int precision) {
 int cr_get_precision(const cr_ctx* ctx, int* precision) {
   if (!ctx || !precision) return CR_EINVAL;
   *precision = ctx->precision;
+  return CR_OK;
+}
+
+int cr_set_multistep(cr_ctx* ctx, int on) {
+  if (!ctx) return CR_EINVAL;
+  ctx->multistep = on != 0;
   return CR_OK;
 }
 

@@ -24,6 +24,15 @@ int tile_vertices(int lanes);
 // system, s.bsys the per-system table); lanes 1, 2 or 4
 void launch_tile_batch(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
                        const StepArgs& s);
+// Multi-step kernel (k_tile_steps): up to s.persist_max middle steps per
+// launch with grid barriers between them; one or two lanes per vertex.  The
+// grid must be resident at once: tile_steps_max_blocks() CTAs at most.
+using TileStepsFn = void (*)(SysParams, SysArrays, StepArgs);
+TileStepsFn tile_steps_fn_fp64(int pot, int inter, int lanes);
+TileStepsFn tile_steps_fn_mixed(int pot, int inter, int lanes);
+int tile_steps_max_blocks(int pot, int inter, int lanes, int precision);
+cudaError_t launch_tile_steps(const LaunchCfg& c, int pot, int inter, const SysParams& p, const SysArrays& a,
+                              const StepArgs& s);
 // cr_tile_mixed.cu (expects p with its FP32 constants filled)
 void launch_tile_mixed(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
                        const StepArgs& s);

@@ -74,6 +74,7 @@ struct StepArgs {
   BatchSys* bsys;          // batch mode: per-system table (tile.x is the system)
   const double* bfire_state;  // batch mode: [S][2][4] FIRE scalars per system
   unsigned long long seed;
+  int persist_max;          // multi-step kernel: most steps per launch
 };
 
 // ------------------------------------------------------------------ helpers

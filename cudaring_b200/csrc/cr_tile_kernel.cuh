@@ -71,10 +71,25 @@ __device__ __forceinline__ void tile_skip(const StepArgs& s, DevStatus* st) {
 // BATCH: the grid covers the tiles of many independent systems; tile.x is
 // the system, whose box, displacement cutoff, FIRE scalars and flags come
 // from s.bsys, and whose last tile reduces the system's partial sums.
-template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH = false>
-__global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK) k_tile(const __grid_constant__ SysParams p,
-                                                const __grid_constant__ SysArrays a,
-                                                const __grid_constant__ StepArgs s) {
+// Positions: the read-only path for a single-step launch; plain loads in the
+// multi-step kernel, where other CTAs rewrite them between steps (the grid
+// barrier's acquire makes their writes visible to plain loads, not to the
+// non-coherent read-only path).
+template <bool PERSIST>
+__device__ __forceinline__ double2 ld_pos(const double2* p) {
+  if constexpr (PERSIST) return *p;
+  else return __ldg(p);
+}
+
+// One step (or force evaluation) of one tile.  pin / pout: positions read
+// and written; step: the integrator step index (Philox stream of the noise).
+// PERSIST (the multi-step kernel): a rebuild due or a non-finite force is
+// reported in *pflag instead of the status block, and the last-block
+// protocol is left to the caller.
+template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH, bool PERSIST>
+__device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a, const StepArgs& s,
+                                          const double2* __restrict__ pin, double2* __restrict__ pout,
+                                          unsigned long long step, int* pflag) {
   constexpr int TV = BLOCK / L;
   constexpr int TS = (MODE == MODE_STEP) ? TV : 1;
   __shared__ double2 s_pos[TV];
@@ -97,23 +112,7 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
   __shared__ Box s_box;
   __shared__ bool s_syslast;
 
-  // every input may come from the kernel before this one (positions, lists,
-  // status); the next kernel (the rebuild check) may be scheduled at once and
-  // waits for this one's completion itself
-  pdl_wait();
-  pdl_trigger();
   DevStatus* st = s.status;
-  if (MODE == MODE_STEP && (st->abort | st->converged)) {
-    // keep the last-block protocol intact so later ops see a consistent counter
-    if (is_last_block(st)) {
-      if (threadIdx.x == 0) {
-        st->done_ctr = 0;
-        if (s.use_cond) cudaGraphSetConditional(s.cond, 0u);
-      }
-    }
-    return;
-  }
-
   const int4 tile = a.tiles[blockIdx.x];
   const int v0 = tile.z, nvt = tile.w - tile.z;
   const int t = threadIdx.x;
@@ -139,7 +138,7 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
       cp_async_commit();
     }
     const int2 tp = __ldg(a.vtopo + v);
-    s_pos[t] = __ldg(a.pos + v);
+    s_pos[t] = ld_pos<PERSIST>(pin + v);
     s_l0[t] = __ldg(a.l0 + v);
     s_th0[t] = __ldg(a.theta0 + v);
     ring = tp.x;
@@ -259,7 +258,7 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
         double2 nxj = make_double2(0.0, 0.0);
         double nr = 0.0;
         if (sl < cnt) {
-          nxj = __ldg(a.pos + jn);
+          nxj = ld_pos<PERSIST>(pin + jn);
           nr = __ldg(a.rad + jn);
         }
         while (sl < cnt) {
@@ -267,7 +266,7 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
           const double rj = nr;
           sl += L;
           if (sl < cnt) {
-            nxj = __ldg(a.pos + j2);
+            nxj = ld_pos<PERSIST>(pin + j2);
             nr = __ldg(a.rad + j2);
             if (sl + L < cnt) j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
           }
@@ -292,9 +291,9 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
         double2 nxj = make_double2(0.0, 0.0), nxjq = nxj, nxjqq = nxj;
         double nr = 0.0;
         if (sl < cnt) {
-          nxj = __ldg(a.pos + jn);
-          nxjq = __ldg(a.pos + jn + pq_first(pkn));
-          nxjqq = __ldg(a.pos + jn + pq_second(pkn));
+          nxj = ld_pos<PERSIST>(pin + jn);
+          nxjq = ld_pos<PERSIST>(pin + jn + pq_first(pkn));
+          nxjqq = ld_pos<PERSIST>(pin + jn + pq_second(pkn));
           nr = __ldg(a.rad + jn);
         }
         while (sl < cnt) {
@@ -302,9 +301,9 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
           const double rsum64 = ri + nr;
           sl += L;
           if (sl < cnt) {
-            nxj = __ldg(a.pos + j2);
-            nxjq = __ldg(a.pos + j2 + pq_first(pk2));
-            nxjqq = __ldg(a.pos + j2 + pq_second(pk2));
+            nxj = ld_pos<PERSIST>(pin + j2);
+            nxjq = ld_pos<PERSIST>(pin + j2 + pq_first(pk2));
+            nxjqq = ld_pos<PERSIST>(pin + j2 + pq_second(pk2));
             nr = __ldg(a.rad + j2);
             if (sl + L < cnt) {
               j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
@@ -432,7 +431,6 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
     // ---- MODE_STEP: integrator tail (src/Simulator.cu, src/FIRE.cu) ----------
     double sums[NSUM] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     int nonfinite = 0;
-    const unsigned long long step = (unsigned long long)st->rng_step;
     if (s.active) {
       // addSelfPropulsion (src/DPM2D.cu:1995-2035): the ring's angle takes a
       // N(0, sqrt(2 dt / taup)) increment and is wrapped to [-pi, pi); the
@@ -484,12 +482,13 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
           vn = make_double2(F.x / s.gamma, F.y / s.gamma);
         }
         const double2 xn = make_double2(x.x + s.dt * vn.x, x.y + s.dt * vn.y);
-        s.pos_out[v] = xn;
+        pout[v] = xn;
         s.vel[v] = vn;
         s.force[v] = F;
         if (s.write_out) s.energy[v] = evtx;
         if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
           st->rebuild = 1;
+          if constexpr (PERSIST) atomicOr(pflag, 1);
           if constexpr (BATCH) s.bsys[sysid].rebuild = 1;
         }
       } else {
@@ -508,10 +507,11 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
             vh2 = make_double2(vn.x + s.hdt * F.x, vn.y + s.hdt * F.y);
             xn = make_double2(x.x + s.dt * vh2.x, x.y + s.dt * vh2.y);
           }
-          s.pos_out[v] = xn;
+          pout[v] = xn;
           s.vel[v] = vh2;
           if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
             st->rebuild = 1;
+            if constexpr (PERSIST) atomicOr(pflag, 1);
             if constexpr (BATCH) s.bsys[sysid].rebuild = 1;
           }
         } else {
@@ -561,9 +561,14 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
         s.partials[(size_t)blockIdx.x * NSUM + t] = x;
       }
     } else if (__syncthreads_or(nonfinite) && t == 0) {
-      st->nonfinite = 1;
-      st->abort = 1;
+      if constexpr (PERSIST) {
+        atomicOr(pflag, 2);
+      } else {
+        st->nonfinite = 1;
+        st->abort = 1;
+      }
     }
+    if constexpr (PERSIST) return;
     if constexpr (BATCH) {
       if (s.accumulate) {
         // the system's last tile reduces the system's partials
@@ -612,6 +617,145 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
         if (s.use_cond) cudaGraphSetConditional(s.cond, st->rebuild ? 1u : 0u);
       }
     }
+  }
+}
+
+template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH = false>
+__global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK) k_tile(const __grid_constant__ SysParams p,
+                                                const __grid_constant__ SysArrays a,
+                                                const __grid_constant__ StepArgs s) {
+  // every input may come from the kernel before this one (positions, lists,
+  // status); the next kernel (the rebuild check) may be scheduled at once and
+  // waits for this one's completion itself
+  pdl_wait();
+  pdl_trigger();
+  DevStatus* st = s.status;
+  if (MODE == MODE_STEP && (st->abort | st->converged)) {
+    // keep the last-block protocol intact so later ops see a consistent counter
+    if (is_last_block(st)) {
+      if (threadIdx.x == 0) {
+        st->done_ctr = 0;
+        if (s.use_cond) cudaGraphSetConditional(s.cond, 0u);
+      }
+    }
+    return;
+  }
+  tile_body<POT, INTER, MODE, BLOCK, L, PREC, BATCH, false>(p, a, s, a.pos, s.pos_out,
+                                                           (unsigned long long)st->rng_step, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Multi-step kernel: up to s.persist_max middle steps of an NVE / Langevin /
+// BAOAB sequence in one launch, with a grid barrier between steps in place
+// of a kernel boundary.  Every tile is one resident CTA (the host launches it
+// only when occupancy x SMs holds the grid).  Positions ping-pong between
+// pos0 (read by step 0) and pos1; a launch that ends after an odd number of
+// steps copies its tiles' positions back, so the result is always in pos0.
+// The launch stops after the first step whose displacement check fired (the
+// one-launch build that follows it rebuilds the list) or that met a
+// non-finite force.
+//
+// Those stop decisions must be the same in every CTA, so they travel in three
+// flag words used in rotation: step j writes slot (base + j) % 3, every CTA
+// reads it after barrier j, and CTA 0 clears slot (base + j + 1) % 3 during
+// step j (its last reader passed barrier j - 1, its next writer waits for
+// barrier j).  base advances by the steps run, so every launch starts on a
+// clean slot.  The step counters (rng_step, ops_done, steps_left, base) are
+// read by every CTA before barrier 0 and updated by CTA 0 after the loop.
+// Every barrier wait is bounded: a CTA that gives up sets stalled and abort
+// and leaves; the others see stalled and leave too.
+
+__device__ __forceinline__ unsigned int pst_ld_acquire(const unsigned int* a) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ unsigned int pst_atom_add_release(unsigned int* a, unsigned int x) {
+  unsigned int old;
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(a), "r"(x) : "memory");
+  return old;
+}
+
+// Barrier over the grid on status.pbar (a multiple of gridDim.x at launch).
+__device__ __forceinline__ bool steps_barrier(DevStatus* st) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned int prev = pst_atom_add_release(&st->pbar, 1u);
+    const unsigned int target = (prev / gridDim.x + 1u) * gridDim.x;
+    long it = 0;
+    while (pst_ld_acquire(&st->pbar) < target) {
+      if (++it > (1L << 20) || *(volatile int*)&st->stalled) {
+        ok = 0;
+        break;
+      }
+      __nanosleep(64);
+    }
+    if (!ok) {
+      atomicExch(&st->stalled, 1);
+      atomicExch(&st->abort, 1);
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+template <int POT, int INTER, int BLOCK, int L, int PREC>
+__global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
+    k_tile_steps(const __grid_constant__ SysParams p, const __grid_constant__ SysArrays a,
+                 const __grid_constant__ StepArgs s) {
+  pdl_wait();
+  pdl_trigger();
+  DevStatus* st = s.status;
+  const volatile DevStatus* vs = st;
+  __shared__ int s_flag;
+  if (vs->abort | vs->converged) return;
+  const long long left = vs->steps_left;
+  const int n = (int)(left < (long long)s.persist_max ? left : (long long)s.persist_max);
+  const unsigned long long step0 = (unsigned long long)vs->rng_step;
+  const long long base = vs->pbase;
+  double2* pos0 = const_cast<double2*>(a.pos);
+  double2* pos1 = s.pos_out;
+  int done = 0;
+  bool stalled = false;
+  for (int j = 0; j < n; j++) {
+    int* slot = &st->pflag[(base + j) % 3];
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->pflag[(base + j + 1) % 3] = 0;
+    const double2* pin = (j & 1) ? pos1 : pos0;
+    double2* pout = (j & 1) ? pos0 : pos1;
+    tile_body<POT, INTER, MODE_STEP, BLOCK, L, PREC, false, true>(p, a, s, pin, pout, step0 + (unsigned long long)j,
+                                                                 slot);
+    done = j + 1;
+    if (!steps_barrier(st)) {
+      stalled = true;
+      break;
+    }
+    if (threadIdx.x == 0) s_flag = *(volatile int*)slot;
+    __syncthreads();
+    const int f = s_flag;
+    __syncthreads();
+    if (f) break;
+  }
+  if (stalled) return;
+  if (done & 1) {
+    // the last step wrote pos1: this tile's vertices back to pos0 (every read
+    // of pos0 by the last step finished before the last barrier)
+    const int4 tile = a.tiles[blockIdx.x];
+    for (int v = tile.z + threadIdx.x; v < tile.w; v += BLOCK) pos0[v] = pos1[v];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0 && done > 0) {
+    const int f = *(volatile int*)&st->pflag[(base + done - 1) % 3];
+    if (f & 2) {
+      st->nonfinite = 1;
+      st->abort = 1;
+    }
+    st->rng_step += done;
+    st->ops_done += done;
+    st->steps_left -= done;
+    st->pbase = base + done;
   }
 }
 

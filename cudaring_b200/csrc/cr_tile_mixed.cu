@@ -36,4 +36,25 @@ void launch_tile_mixed(const LaunchCfg& c, int pot, int inter, int mode, const S
 #undef CR_MIXED_CASE
 }
 
+
+// Multi-step kernel (k_tile_steps) for one or two lanes per vertex; nullptr
+// for other lane counts.
+template <int POT, int INTER>
+static TileStepsFn steps_fn_l(int lanes) {
+  if (lanes == 1) return k_tile_steps<POT, INTER, 128, 1, PREC_MIXED>;
+  if (lanes == 2) return k_tile_steps<POT, INTER, 192, 2, PREC_MIXED>;
+  return nullptr;
+}
+
+TileStepsFn tile_steps_fn_mixed(int pot, int inter, int lanes) {
+  const bool vv = inter == INT_VV;
+  switch (pot) {
+    case POT_HARMONIC: return vv ? steps_fn_l<POT_HARMONIC, INT_VV>(lanes) : steps_fn_l<POT_HARMONIC, INT_SMOOTH>(lanes);
+    case POT_LJ: return vv ? steps_fn_l<POT_LJ, INT_VV>(lanes) : steps_fn_l<POT_LJ, INT_SMOOTH>(lanes);
+    case POT_ADHESIVE: return vv ? steps_fn_l<POT_ADHESIVE, INT_VV>(lanes) : steps_fn_l<POT_ADHESIVE, INT_SMOOTH>(lanes);
+    case POT_WCA: return vv ? steps_fn_l<POT_WCA, INT_VV>(lanes) : steps_fn_l<POT_WCA, INT_SMOOTH>(lanes);
+    default: return nullptr;
+  }
+}
+
 }  // namespace cr

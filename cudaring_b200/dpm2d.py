@@ -358,6 +358,8 @@ class DPM2D:
 
     def setUseGraphs(self, on): self._call("cr_set_use_graphs", int(bool(on)))
 
+    def setMultistep(self, on): self._call("cr_set_multistep", int(bool(on)))
+
     def setPrecision(self, precision):
         """"fp64" (default, the reference's arithmetic) or "mixed" (FP32 pair
         terms on FP64-formed offsets; everything else FP64)."""

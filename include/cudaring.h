@@ -326,6 +326,12 @@ int cr_get_lanes(const cr_ctx* ctx, int* lanes);
  * moved positions followed by the one-launch rebuild check; 0: direct
  * launches with a host check after each op. */
 int cr_set_use_graphs(cr_ctx* ctx, int on);
+/* 1 (default): the middle steps of NVE, Langevin and BAOAB runs of
+ * deformable rings run in a multi-step kernel (up to 64 steps per launch,
+ * grid barriers between steps) when the GPU holds all of its CTAs at once
+ * and one or two lanes per vertex are in use; 0: one launch per step.  The
+ * results are identical. */
+int cr_set_multistep(cr_ctx* ctx, int on);
 /* Times the fused step kernel for every lane count whose tile holds the
  * largest ring (cr_profile_step_kernel, `reps` launches each) and keeps the
  * fastest; reports the choice.  Needs a neighbour list. */
