@@ -586,9 +586,10 @@ int launch_chunk(cr_ctx* ctx, const std::vector<Op>& ops, int kind, long n) {
 // NVE, Langevin and BAOAB runs of deformable rings: the drift op, then the
 // middle steps in k_tile_steps launches (each runs until its step budget, a
 // due rebuild or the end of the sequence; the one-launch build follows
-// every launch), then the final op.  Graphs of kStepsLaunches such pairs
-// are launched until the device counter of middle steps reaches zero; the
-// step arithmetic is the per-op path's, so results are identical to it.
+// every launch), then the final op.  Graphs of up to kStepsLaunches such
+// pairs (sized to the steps left, one spare launch for a rebuild) are
+// launched until the device counter of middle steps reaches zero; the step
+// arithmetic is the per-op path's, so FP64 results are identical to it.
 constexpr int kStepsPerLaunch = 64;
 constexpr int kStepsLaunches = 16;
 
@@ -601,7 +602,7 @@ bool steps_eligible(cr_ctx* ctx, int kind, long nsteps) {
   return maxb >= (int)ctx->tiles_h.size();
 }
 
-int capture_steps_graph(cr_ctx* ctx, int kind, int b, GraphEntry& ge) {
+int capture_steps_graph(cr_ctx* ctx, int kind, int b, int launches, GraphEntry& ge) {
   StepArgs s = base_args(ctx);
   s.kind = kind;
   s.pos_out = ctx->pos[b ^ 1];
@@ -618,7 +619,7 @@ int capture_steps_graph(cr_ctx* ctx, int kind, int b, GraphEntry& ge) {
   const int fb = nbr_fused_blocks(ctx->nv, ctx->fused_max);
   CR_TRY(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaSuccess;
-  for (int r = 0; r < kStepsLaunches && e == cudaSuccess; r++) {
+  for (int r = 0; r < launches && e == cudaSuccess; r++) {
     e = launch_tile_steps(c, ctx->potential, inter_kind(ctx), ctx->p, a, s);
     launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nb, fb, 0, true);
   }
@@ -631,7 +632,7 @@ int capture_steps_graph(cr_ctx* ctx, int kind, int b, GraphEntry& ge) {
     return ctx->fail(CR_ECUDA, std::string("multi-step graph: ") + cudaGetErrorString(e));
   }
   ge.graph = out;
-  ge.launches = 2 * kStepsLaunches;
+  ge.launches = 2 * launches;
   return CR_OK;
 }
 
@@ -650,12 +651,15 @@ int run_steps(cr_ctx* ctx, int kind, long nsteps) {
   const long long middle = nsteps - 1;
   CR_TRY(cudaMemcpyAsync(&ctx->status->steps_left, &middle, sizeof(middle), cudaMemcpyHostToDevice, ctx->stream));
   CR_TRY(cudaStreamSynchronize(ctx->stream));
+  long long left = middle;
   for (;;) {
-    auto key = std::make_tuple(kind, -1L, b, ctx->cap, 1ULL);
+    const int launches =
+        (int)std::min<long long>(kStepsLaunches, std::max<long long>(2, (left + kStepsPerLaunch - 1) / kStepsPerLaunch + 1));
+    auto key = std::make_tuple(kind, -(long)launches, b, ctx->cap, 1ULL);
     auto it = ctx->graphs.find(key);
     if (it == ctx->graphs.end()) {
       GraphEntry ge;
-      if ((rc = capture_steps_graph(ctx, kind, b, ge))) return rc;
+      if ((rc = capture_steps_graph(ctx, kind, b, launches, ge))) return rc;
       it = ctx->graphs.emplace(key, ge).first;
     }
     CR_TRY(cudaGraphLaunch(it->second.exec, ctx->stream));
@@ -678,6 +682,7 @@ int run_steps(cr_ctx* ctx, int kind, long nsteps) {
       continue;
     }
     if (st.steps_left <= 0) break;
+    left = st.steps_left;
   }
   // final op: forces at the last positions and the second half kick
   enqueue_op(ctx, ctx->stream, Op{OP_TILE, b, b, 0, 0, b}, kind, false, 0);
