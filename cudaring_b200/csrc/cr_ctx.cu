@@ -275,6 +275,25 @@ int setup_grid(cr_ctx* ctx, double cut) {
     ctx->grid = CellGrid{0, 0, 0.0, 0.0};
     return CR_OK;
   }
+  // The build's stencil phase deals home cells to its warps in rounds; a last
+  // round that only a few warps take costs a whole round.  When the build
+  // fills the GPU and there are more cells than warps, coarsen the grid
+  // (larger cells hold every pair the smaller ones did) to a whole number of
+  // rounds: the lists hold the same neighbours, in the order of the coarser
+  // cells.  Smaller systems keep the finest grid.
+  {
+    const int blocks = nbr_fused_blocks(ctx->nv, ctx->fused_max);
+    const long warps = (long)blocks * 32;
+    const long cells = (long)ncx * ncy;
+    if (ctx->fused_max > 0 && blocks >= ctx->fused_max && cells > warps && cells % warps != 0) {
+      const double f = std::sqrt((double)((cells / warps) * warps) / (double)cells);
+      const int nx = std::max(3, (int)std::floor(ncx * f)), ny = std::max(3, (int)std::floor(ncy * f));
+      if ((long)nx * ny <= (cells / warps) * warps) {
+        ncx = nx;
+        ncy = ny;
+      }
+    }
+  }
   ctx->grid = CellGrid{ncx, ncy, ctx->p.lx / ncx, ctx->p.ly / ncy};
   const int ncells = ncx * ncy;
   if (ncells > ctx->ncells_alloc) {
