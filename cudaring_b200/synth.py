@@ -121,8 +121,8 @@ def make_packing(nv_list, a0_list, calA0, phi: float, seed: int, jitter: float =
     """Build a seeded packing.
 
     ``calA0`` may be a scalar or one value per ring.  ``placement`` is
-    ``"uniform"`` (ring centres uniform in the box, as the survey's conventions
-    state; rings may overlap) or ``"rsa"`` (non-overlapping discs of radius
+    ``"uniform"`` (ring centres uniform in the box, the benchmark workloads'
+    convention; rings may overlap) or ``"rsa"`` (non-overlapping discs of radius
     ``disc_scale * (R + rad)``).
     """
     nv_list = np.asarray(nv_list, dtype=np.int64)
