@@ -329,8 +329,12 @@ int cr_set_use_graphs(cr_ctx* ctx, int on);
 /* 1 (default): the middle steps of NVE, Langevin and BAOAB runs of
  * deformable rings run in a multi-step kernel (up to 64 steps per launch,
  * grid barriers between steps) when the GPU holds all of its CTAs at once
- * and one or two lanes per vertex are in use; 0: one launch per step.  The
- * results are identical. */
+ * and one or two lanes per vertex are in use; 0: one launch per step.  FP64
+ * results are identical; mixed-precision results agree to FP32 rounding.
+ * The kernel's grid barriers need all of its CTAs resident: with other work
+ * running on the same GPU at the same time, a barrier may give up after
+ * about a second and the call returns CR_ECUDA; such contexts should set 0
+ * (the one-launch neighbour-list build has the same requirement). */
 int cr_set_multistep(cr_ctx* ctx, int on);
 /* Times the fused step kernel for every lane count whose tile holds the
  * largest ring (cr_profile_step_kernel, `reps` launches each) and keeps the
