@@ -89,3 +89,22 @@ def test_rsa_centres_do_not_overlap():
     d -= L * np.round(d / L)
     dist = np.sqrt((d ** 2).sum(-1)) + np.eye(200) * 1e9
     assert (dist >= r[:, None] + r[None, :] - 1e-12).all()
+
+
+def test_tuning_entry_points_reject_a_null_context(libcr):
+    # the step-structure switches validate their context before any device call
+    assert libcr.cr_set_multistep(None, 1) == 1
+    assert libcr.cr_set_use_graphs(None, 1) == 1
+    assert libcr.cr_set_lanes(None, 2) == 1
+    assert libcr.cr_hessian_solve(None, None, None, 1e-10, 10, None, None) == 1
+
+
+def test_benchmark_workloads_are_named():
+    for name, rings in (("bidisperse_harmonic", 32), ("smooth_lj", 1024), ("rigid_ellipses", 4096),
+                        ("dense_harmonic", 256)):
+        c = synth.workload_config(name)
+        n = c["n"] if c.get("rigid") else len(c["nv"])
+        assert n == rings
+    assert len(synth.workload_config("smooth_lj", 64)["nv"]) == 64
+    with pytest.raises(ValueError):
+        synth.workload_config("cfg2")
