@@ -3,23 +3,29 @@
 // Some callers cannot allocate device memory from inside their own code: a
 // host framework that owns a fixed device memory budget and hands out only
 // pre-sized buffers, or code that must not call cudaMalloc/cudaFree because
-// those calls synchronise the device (and are not allowed at all while a
-// stream is being captured into a CUDA graph).  cr_neighbor_list_noalloc
-// serves them: it runs the same cell-list kernels as cr_calc_neighbor_list on
-// device buffers the caller passes, and keeps every temporary in one static
-// device array of this file, so it never calls cudaMalloc, cudaFree or any
-// allocating library routine.
+// those calls synchronise the whole device and stall every other stream.
+// cr_neighbor_list_noalloc serves them: it runs the same cell-list kernels as
+// cr_calc_neighbor_list on device buffers the caller passes, and keeps every
+// temporary in one static device array of this file, so it never calls
+// cudaMalloc, cudaFree or any allocating library routine.
 //
 // Limits and rules of use:
-//   * at most CR_NOALLOC_MAX_VERTICES vertices and CR_NOALLOC_MAX_CELLS cells
-//     (the scratch array is sized for these; every GPU that loads the library
-//     keeps it, about 4.2 MB, until the process exits); larger inputs return
-//     CR_EINVAL before touching any buffer;
+//   * at most CR_NOALLOC_MAX_VERTICES vertices (the scratch array is sized
+//     for these; every GPU that loads the library keeps it, about 4.2 MB,
+//     until the process exits); larger inputs return CR_EINVAL before any
+//     buffer is touched.  The cell grid is coarsened to at most
+//     CR_NOALLOC_MAX_CELLS cells (larger cells hold every pair the finer grid
+//     did, so the list is the same);
 //   * the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (once per device); make that first call before any
-//     stream capture starts;
+//     cudaGetSymbolAddress (once per device) and keeps it for the life of the
+//     process; make that first call before any stream capture.  After
+//     cudaDeviceReset on that device the kept address is stale: do not call
+//     this entry point on a device that was reset;
+//   * the call waits for its stream (it reads the largest count back);
 //   * all calls share the one array, so calls that overlap on the GPU (other
 //     streams, other host threads) race; serialise them.
+#include <algorithm>
+#include <cmath>
 #include <mutex>
 
 #include "cr_launch.h"
@@ -87,10 +93,19 @@ extern "C" int cr_neighbor_list_noalloc(const double* pos, const double* rad, co
   // the same cell rule as the context's build: cells no smaller than the
   // largest neighbour distance, brute force below three cells per side
   const double cmin = (1.0 + cutDistance) * 2.0 * maxRad * (1.0 + 1e-9);
-  long ncx = (long)(p.lx / cmin), ncy = (long)(p.ly / cmin);
+  long ncx = (long)std::min(p.lx / cmin, 1048576.0), ncy = (long)std::min(p.ly / cmin, 1048576.0);
   cr::CellGrid g{0, 0, 0.0, 0.0};
   if (ncx >= 3 && ncy >= 3) {
-    if (ncx * ncy > kMaxCells) return CR_EINVAL;
+    if (ncx * ncy > kMaxCells) {
+      // coarsen to the scratch array's cell budget, at least three cells a side
+      const double f = std::sqrt((double)kMaxCells / (double)(ncx * ncy));
+      ncx = std::max(3L, (long)std::floor((double)ncx * f));
+      ncy = std::max(3L, (long)std::floor((double)ncy * f));
+      if (ncx * ncy > kMaxCells) {
+        if (ncx > ncy) ncx = std::max(3L, kMaxCells / ncy);
+        else ncy = std::max(3L, kMaxCells / ncx);
+      }
+    }
     g = cr::CellGrid{(int)ncx, (int)ncy, p.lx / ncx, p.ly / ncy};
   }
   void* base = nullptr;
