@@ -40,11 +40,16 @@ class OcSys(C.Structure):
                 ("potential", C.c_int), ("interaction", C.c_int), ("monomer", C.c_int)]
 
 
+def reference_dir() -> str:
+    """The reference checkout: $CUDARING_REFERENCE, else /root/reference."""
+    return os.environ.get("CUDARING_REFERENCE", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
     """Build liboracle.so (and _ref when the reference checkout exists)."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.run(["make", "-C", HERE, "liboracle.so"], check=True, stdout=out)
-    ref_src = "/root/reference"
+    ref_src = reference_dir()
     if os.path.isdir(ref_src):
         subprocess.run([os.path.join(HERE, "build_ref.sh"), ref_src], check=True, stdout=out)
 
@@ -110,7 +115,7 @@ def ref():
         R.ref_get.argtypes = [C.c_int, _dp]
         R.ref_set_particle_state.argtypes = [C.c_void_p] * 4
         for fn in ("ref_potential_energy", "ref_kinetic_energy", "ref_max_unbalanced_force",
-                   "ref_total_force_magnitude", "ref_phi"):
+                   "ref_total_force_magnitude", "ref_phi", "ref_preferred_phi"):
             getattr(R, fn).restype = C.c_double
         R.ref_nve_loop.argtypes = [C.c_long]
         R.ref_nve_rescale_loop.argtypes = [C.c_long, C.c_double]
@@ -215,6 +220,23 @@ class System:
                                 out["force"], out["torque"], out["energy"], out["moi"], out["p_force"],
                                 out["p_torque"], out["p_energy"])
         return out
+
+
+def packing_fraction(nv_list, rad, ring_area, box) -> float:
+    """DPM2D::getPhi / getPreferredPhi for the periodic box (src/DPM2D.cu:1202-1238):
+    ring areas (current or rest) plus pi * r_first^2 * (nv / 2 - 1) per ring
+    (kernelCalcVertexArea, include/cudaKernel.cuh:1636-1642), over the box area.
+    Ring terms are summed in ring order, as the reference's reduce does on the host."""
+    nv_list = np.asarray(nv_list, dtype=np.int64)
+    first = np.concatenate([[0], np.cumsum(nv_list)[:-1]])
+    r = np.asarray(rad, dtype=np.float64)[first]
+    s = 0.0
+    for a in np.asarray(ring_area, dtype=np.float64):
+        s += float(a)
+    v = 0.0
+    for rr, n in zip(r, nv_list):
+        v += float(rr * rr * (0.5 * n - 1))
+    return (s + np.pi * v) / (float(box[0]) * float(box[1]))
 
 
 def normal2(seed: int, stream: int, index: int) -> np.ndarray:

@@ -5,10 +5,10 @@
 # oracle/ref_shim/shim.h, plus the host driver oracle/ref_shim/ref_driver.cpp.
 # Test infrastructure only (golden fixtures, oracle pinning, CPU baseline).
 #
-# usage: oracle/build_ref.sh [REFERENCE_DIR]   (default /root/reference)
+# usage: oracle/build_ref.sh [REFERENCE_DIR]   (default $CUDARING_REFERENCE, else /root/reference)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${CUDARING_REFERENCE:-/root/reference}}"
 if [ ! -f "$REF/include/cudaKernel.cuh" ]; then
   echo "build_ref: reference sources not found under $REF; skipping" >&2
   exit 0

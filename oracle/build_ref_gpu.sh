@@ -7,10 +7,10 @@
 # (-O3 --expt-extended-lambda --expt-relaxed-constexpr, -lstdc++fs).
 # Measurement infrastructure only.
 #
-# usage: oracle/build_ref_gpu.sh [REFERENCE_DIR]   (default /root/reference)
+# usage: oracle/build_ref_gpu.sh [REFERENCE_DIR]   (default $CUDARING_REFERENCE, else /root/reference)
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${1:-/root/reference}"
+REF="${1:-${CUDARING_REFERENCE:-/root/reference}}"
 if [ ! -f "$REF/src/DPM2D.cu" ]; then
   echo "build_ref_gpu: reference sources not found under $REF; skipping" >&2
   exit 0
