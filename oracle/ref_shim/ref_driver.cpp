@@ -722,6 +722,9 @@ static double preferred_phi(void) {
   return phi / (M.boxSize[0] * M.boxSize[1]);
 }
 
+// DPM2D::getPreferredPhi (DPM2D.cu:1222-1238), exported.
+double ref_preferred_phi(void) { return preferred_phi(); }
+
 // DPM2D::setRandomParticles (DPM2D.cu:1601-1629) with the drand48() stream
 // of srand48(seed): erand48 on the state srand48 would set.
 void ref_set_random_particles(double phi0, double extraRad, long seed) {

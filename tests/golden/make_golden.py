@@ -401,10 +401,39 @@ def soft_cases():
               + (f" iters={int(d['out_min_iters'])}" if full else ""))
 
 
+def phi_cases():
+    """DPM2D::getPhi (src/DPM2D.cu:1202-1220, current ring areas plus the vertex
+    caps) and getPreferredPhi (:1222-1238, rest areas) on packings of three
+    workloads, the first two deformed away from their rest shapes."""
+    specs = [("smooth_lj", dict(workload="smooth_lj", n=64), "rsa", 0.40, 1.00),
+             ("bidisperse", dict(workload="bidisperse_harmonic"), "uniform", 0.70, 0.97),
+             ("monodisperse", dict(nv=24, n=64), "uniform", 0.55, 1.00)]
+    d = {}
+    for idx, (name, spec, placement, phi, squeeze) in enumerate(specs):
+        pk = packing_for(spec, phi, placement, seed=20261203 + 500 + idx)
+        if squeeze != 1.0:
+            # ring areas away from a0: squeeze every ring along x about its centroid
+            pos = pk.pos.reshape(-1, 2).copy()
+            first = np.concatenate([[0], np.cumsum(pk.nv_list)[:-1]])
+            for f, n in zip(first, pk.nv_list):
+                c = pos[f:f + n].mean(axis=0)
+                pos[f:f + n, 0] = c[0] + squeeze * (pos[f:f + n, 0] - c[0])
+            pk.pos = pos.reshape(-1)
+        R, _ = setup_ref(pk, "harmonic", "vertexVertex")
+        R.ref_calc_force_energy()
+        for k, v in inputs(pk).items():
+            d[f"{name}_{k}"] = v
+        d[f"{name}_out_phi"] = np.asarray(R.ref_phi())
+        d[f"{name}_out_preferred_phi"] = np.asarray(R.ref_preferred_phi())
+        print(f"phi_{name}: phi={float(d[name + '_out_phi']):.15f} preferred={float(d[name + '_out_preferred_phi']):.15f}")
+    d["names"] = np.array([s[0] for s in specs])
+    np.savez_compressed(os.path.join(OUT, "phi_cases.npz"), **d)
+
+
 if __name__ == "__main__":
     if not oracle.ref_available():
         oracle.build()
-    which = sys.argv[1:] or ["force", "traj", "stochastic", "rigid", "rescale", "soft"]
+    which = sys.argv[1:] or ["force", "traj", "stochastic", "rigid", "rescale", "soft", "phi"]
     if "force" in which:
         force_cases()
     if "traj" in which:
@@ -417,3 +446,5 @@ if __name__ == "__main__":
         rescale_cases()
     if "soft" in which:
         soft_cases()
+    if "phi" in which:
+        phi_cases()

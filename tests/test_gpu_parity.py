@@ -59,6 +59,21 @@ def test_force_energy_and_neighbors_match_reference(cuda_device, path):
     d.close()
 
 
+@pytest.mark.parametrize("name", ["smooth_lj", "bidisperse", "monodisperse"])
+def test_packing_fraction_matches_reference(cuda_device, name):
+    """cr_get_phi / cr_get_preferred_phi against DPM2D::getPhi / getPreferredPhi
+    (src/DPM2D.cu:1202-1238) on rings deformed away from their rest areas."""
+    g = load_golden(golden_files("phi_cases")[0])
+    c = {k[len(name) + 1:]: v for k, v in g.items() if k.startswith(name + "_")}
+    d = DPM2D.from_packing(packing_of(c), potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01,
+                           ec=1.0)
+    d.calcNeighborList(d.setDisplacementCutoff(0.5, 2 * c["rad"].mean()))
+    d.calcForceEnergy()
+    assert d.getPhi() == pytest.approx(float(c["out_phi"]), rel=1e-14)
+    assert d.getPreferredPhi() == pytest.approx(float(c["out_preferred_phi"]), rel=1e-14)
+    d.close()
+
+
 def _prepared(g):
     d, cut = dpm_of(g)
     d.calcNeighborList(cut)

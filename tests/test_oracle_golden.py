@@ -186,3 +186,18 @@ def test_philox_normals_are_standard():
     z = np.stack([oracle.normal2(99, 3, i) for i in range(4000)]).reshape(-1)
     assert abs(z.mean()) < 0.05
     assert abs(z.std() - 1.0) < 0.05
+
+
+def _phi_case(g, name):
+    return {k[len(name) + 1:]: v for k, v in g.items() if k.startswith(name + "_")}
+
+
+@pytest.mark.parametrize("name", ["smooth_lj", "bidisperse", "monodisperse"])
+def test_packing_fraction_matches_reference(name):
+    c = _phi_case(load_golden(golden_files("phi_cases")[0]), name)
+    S = oracle.System(c["nv_list"], c["box"], "harmonic", "vertexVertex", 1.0, 1.0, 0.01, 1.0)
+    area = S.force_energy(c["pos"], c["rad"], c["a0"], c["l0"], c["theta0"])["area"]
+    assert oracle.packing_fraction(c["nv_list"], c["rad"], area, c["box"]) == pytest.approx(float(c["out_phi"]),
+                                                                                           rel=1e-14)
+    assert oracle.packing_fraction(c["nv_list"], c["rad"], c["a0"], c["box"]) == pytest.approx(
+        float(c["out_preferred_phi"]), rel=1e-14)
