@@ -353,7 +353,7 @@ int cr_get_precision(const cr_ctx* ctx, int* precision);
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory themselves (a host framework that hands out only fixed, pre-sized
  * buffers; code that must not call cudaMalloc/cudaFree because they
- * synchronise the device and are refused during stream capture): builds the
+ * synchronise the whole device and stall its other streams): builds the
  * same neighbour list as cr_calc_neighbor_list from caller-owned device
  * arrays, keeping every temporary in one static device array of the library,
  * so it calls no cudaMalloc, cudaFree or allocating library routine.
@@ -363,11 +363,13 @@ int cr_get_precision(const cr_ctx* ctx, int* precision);
  *   (slot-major: neighbour s of vertex v at neighbors[s * Nv + v]); counts:
  *   device int32 [Nv]; *maxCount: host, largest count; stream: cudaStream_t
  *   (NULL = legacy default stream); the call synchronises that stream.
- * Limits: Nv <= CR_NOALLOC_MAX_VERTICES and at most CR_NOALLOC_MAX_CELLS
- * cells, else CR_EINVAL before any buffer is touched; CR_ENBR_OVERFLOW when a
- * count exceeds capacity (counts are still complete).  The first call on a
- * device looks up the scratch array's address (once per device): make it
- * before any stream capture.  All calls share that array: calls that
+ * Limits: Nv <= CR_NOALLOC_MAX_VERTICES, else CR_EINVAL before any buffer
+ * is touched; the cell grid is coarsened to at most CR_NOALLOC_MAX_CELLS
+ * cells (same list); CR_ENBR_OVERFLOW when a count exceeds capacity (counts
+ * and *maxCount are still complete).  The first call on a device looks up the
+ * scratch array's address (once per device) and keeps it for the process:
+ * make that call before any stream capture, and do not use the entry point on
+ * a device after cudaDeviceReset.  All calls share that array: calls that
  * overlap on the GPU race and must be serialised. */
 #define CR_NOALLOC_MAX_VERTICES 65536
 #define CR_NOALLOC_MAX_CELLS 65536
