@@ -351,23 +351,7 @@ __global__ void __launch_bounds__(BLOCK) k_btile_reduce(const int4* tiles, const
   }
   __shared__ double s_red[BLOCK / 32][NSUM];
   __shared__ bool s_last;
-  const int warp = threadIdx.x / 32, wl = threadIdx.x % 32;
-#pragma unroll
-  for (int q = 0; q < NSUM; q++) {
-    double x = acc[q];
-    for (int o = 16; o > 0; o >>= 1) {
-      const double y = __shfl_xor_sync(0xffffffffu, x, o);
-      x = (q == S_FMAX2) ? fmax(x, y) : x + y;
-    }
-    if (wl == 0) s_red[warp][q] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < NSUM) {
-    const int q = threadIdx.x;
-    double x = 0.0;
-    for (int w = 0; w < BLOCK / 32; w++) x = (q == S_FMAX2) ? fmax(x, s_red[w][q]) : x + s_red[w][q];
-    partials[(size_t)blockIdx.x * NSUM + q] = x;
-  }
+  block_partials<BLOCK>(acc, s_red, partials + (size_t)blockIdx.x * NSUM);
   BatchSys& bs = bsys[tile.x];
   __syncthreads();
   if (threadIdx.x == 0) {

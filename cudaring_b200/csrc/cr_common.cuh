@@ -69,6 +69,9 @@ struct SysParams {
   // FP32 copies of the pair constants for the mixed-precision pair terms,
   // filled from the FP64 values when a mixed-precision kernel is launched
   float f_ec, f_l1, f_l2, f_lj_cutoff, f_lj_ecut, f_lj_fshift;
+  // mixed precision: a smooth unit whose vertex lies within f_near * radSum
+  // of its segment is evaluated in FP64 (0: none)
+  float f_near;
 };
 
 inline SysParams with_f32_constants(SysParams p) {
@@ -78,6 +81,14 @@ inline SysParams with_f32_constants(SysParams p) {
   p.f_lj_cutoff = (float)p.lj_cutoff;
   p.f_lj_ecut = (float)p.lj_ecut;
   p.f_lj_fshift = (float)p.lj_fshift;
+  // Near-contact units of the steep potentials carry the FP32 error: around
+  // the Lennard-Jones minimum (radSum * 2^(1/6)) the force falls by ~57
+  // epsilon/sigma per sigma and 2 r^12 - r^6 cancels, so one FP32 rounding of
+  // the distance or of r^6 moves a unit force by ~1e-6 of the net force.
+  // Units closer than 1.2 radSum are therefore evaluated in FP64 (every WCA
+  // unit: its whole range is that steep); harmonic and adhesive forces are
+  // linear in the overlap and stay FP32.
+  p.f_near = p.potential == 1 ? 1.2f : (p.potential == 3 ? 1.2f : 0.0f);
   return p;
 }
 

@@ -1936,9 +1936,17 @@ static int diff_energy(cr_ctx* ctx, double out[4]) {
   std::vector<double> e((size_t)4 * ctx->nv);
   int rc = download(ctx, e.data(), ctx->diff_e, e.size() * sizeof(double));
   if (rc) return rc;
+  // compensated (TwoSum) sums in vertex order: the energy and pressure
+  // tangents are differences of large terms of both signs
+  double c[4] = {0.0, 0.0, 0.0, 0.0};
   for (int q = 0; q < 4; q++) out[q] = 0.0;
   for (int v = 0; v < ctx->nv; v++)
-    for (int q = 0; q < 4; q++) out[q] += e[(size_t)4 * v + q];
+    for (int q = 0; q < 4; q++) {
+      const double x = e[(size_t)4 * v + q], t = out[q] + x, bp = t - out[q];
+      c[q] += (out[q] - (t - bp)) + (x - bp);
+      out[q] = t;
+    }
+  for (int q = 0; q < 4; q++) out[q] += c[q];
   return CR_OK;
 }
 

@@ -133,36 +133,24 @@ __global__ void __launch_bounds__(256) k_fire_pre(const __grid_constant__ SysPar
 __global__ void __launch_bounds__(256) k_reduce(int nv, int np, const double2* vel, const double2* force,
                                                 const double* energy, const double* p_energy, int use_p_energy,
                                                 double* partials, DevStatus* st) {
-  double acc[NSUM] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // compensated per-thread sums (two_sum_add), then the compensated CTA tree
+  double acc[NSUM] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, cmp[4] = {0.0, 0.0, 0.0, 0.0};
   for (int v = blockIdx.x * blockDim.x + threadIdx.x; v < nv; v += gridDim.x * blockDim.x) {
     const double2 u = vel[v], f = force[v];
-    acc[S_PE] += energy[v];
-    acc[S_VV] += u.x * u.x + u.y * u.y;
-    acc[S_VF] += u.x * f.x + u.y * f.y;
-    acc[S_FF] += f.x * f.x + f.y * f.y;
+    two_sum_add(acc[S_PE], cmp[S_PE], energy[v]);
+    two_sum_add(acc[S_VV], cmp[S_VV], u.x * u.x + u.y * u.y);
+    two_sum_add(acc[S_VF], cmp[S_VF], u.x * f.x + u.y * f.y);
+    two_sum_add(acc[S_FF], cmp[S_FF], f.x * f.x + f.y * f.y);
     acc[S_FMAX2] = fmax(acc[S_FMAX2], fmax(f.x * f.x, f.y * f.y));
     if (!(isfinite(f.x) && isfinite(f.y))) acc[S_NONFINITE] = 1.0;
   }
   if (use_p_energy)
-    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x) acc[S_PE] += p_energy[q];
-  __shared__ double s_red[8][NSUM];
-  const int warp = threadIdx.x / 32, wl = threadIdx.x % 32;
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < np; q += gridDim.x * blockDim.x)
+      two_sum_add(acc[S_PE], cmp[S_PE], p_energy[q]);
 #pragma unroll
-  for (int q = 0; q < NSUM; q++) {
-    double x = acc[q];
-    for (int o = 16; o > 0; o >>= 1) {
-      double y = __shfl_xor_sync(0xffffffffu, x, o);
-      x = (q == S_FMAX2) ? fmax(x, y) : x + y;
-    }
-    if (wl == 0) s_red[warp][q] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < NSUM) {
-    const int q = threadIdx.x;
-    double x = 0.0;
-    for (int w = 0; w < (int)(blockDim.x / 32); w++) x = (q == S_FMAX2) ? fmax(x, s_red[w][q]) : x + s_red[w][q];
-    partials[(size_t)blockIdx.x * NSUM + q] = x;
-  }
+  for (int q = 0; q < 4; q++) acc[q] += cmp[q];
+  __shared__ double s_red[8][NSUM];
+  block_partials<256>(acc, s_red, partials + (size_t)blockIdx.x * NSUM);
   if (is_last_block(st)) {
     reduce_partials(partials, gridDim.x, st->sums);
     __syncthreads();

@@ -227,24 +227,7 @@ __global__ void __launch_bounds__(BLOCK) k_rigid(const __grid_constant__ SysPara
         r.v_torque[v] = tau;
       }
     }
-    {
-      const int warp = t / 32, wl = t % 32;
-#pragma unroll
-      for (int q = 0; q < NSUM; q++) {
-        double x = sums[q];
-        for (int o = 16; o > 0; o >>= 1) {
-          double y = __shfl_xor_sync(0xffffffffu, x, o);
-          x = (q == S_FMAX2) ? fmax(x, y) : x + y;
-        }
-        if (wl == 0) s_red[warp][q] = x;
-      }
-      __syncthreads();
-      if (t < NSUM) {
-        double x = 0.0;
-        for (int w = 0; w < BLOCK / 32; w++) x = (t == S_FMAX2) ? fmax(x, s_red[w][t]) : x + s_red[w][t];
-        s.partials[(size_t)blockIdx.x * NSUM + t] = x;
-      }
-    }
+    block_partials<BLOCK>(sums, s_red, s.partials + (size_t)blockIdx.x * NSUM);
     if (is_last_block(st)) {
       reduce_partials(s.partials, gridDim.x, st->sums);
       __syncthreads();

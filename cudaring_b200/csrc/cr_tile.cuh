@@ -436,25 +436,80 @@ __device__ __forceinline__ bool is_last_block(DevStatus* st) {
   return s_last;
 }
 
+// Compensated summation for the energy, kinetic-energy and power sums:
+// TwoSum (Knuth, TAOCP vol. 2, 4.2.2) gives the exact rounding error of each
+// addition, which is carried in c, so s + c holds the sum to about one
+// rounding of the result whatever the number of terms and their
+// cancellation (Neumaier 1974).
+__device__ __forceinline__ void two_sum_add(double& s, double& c, double x) {
+  const double t = s + x;
+  const double bp = t - s;
+  c += (s - (t - bp)) + (x - bp);
+  s = t;
+}
+
+// Warp tree of a compensated pair; the total on lane 0.
+__device__ __forceinline__ void warp_csum(double& s, double& c) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ys = __shfl_xor_sync(0xffffffffu, s, o), yc = __shfl_xor_sync(0xffffffffu, c, o);
+    two_sum_add(s, c, ys);
+    c += yc;
+  }
+}
+
+// Per-CTA partials of the NSUM quantities in a fixed order (every thread
+// calls it with its own values): the additive ones summed with
+// compensation, the largest force component and the non-finite flag by
+// max.  s_red: shared [BLOCK / 32][NSUM]; out: this CTA's NSUM partials.
+template <int BLOCK>
+__device__ __forceinline__ void block_partials(const double (&v)[NSUM], double (*s_red)[NSUM], double* out) {
+  const int warp = threadIdx.x / 32, wl = threadIdx.x % 32;
+#pragma unroll
+  for (int q = 0; q < NSUM; q++) {
+    double s = v[q], c = 0.0;
+    if (q == S_FMAX2 || q == S_NONFINITE) {
+      for (int o = 16; o > 0; o >>= 1) s = fmax(s, __shfl_xor_sync(0xffffffffu, s, o));
+    } else {
+      warp_csum(s, c);
+      s += c;
+    }
+    if (wl == 0) s_red[warp][q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NSUM) {
+    const int q = threadIdx.x;
+    double s = 0.0, c = 0.0;
+    for (int w = 0; w < BLOCK / 32; w++) {
+      if (q == S_FMAX2 || q == S_NONFINITE) s = fmax(s, s_red[w][q]);
+      else two_sum_add(s, c, s_red[w][q]);
+    }
+    out[q] = s + c;
+  }
+}
+
 __device__ __forceinline__ void reduce_partials(const double* partials, int nblocks, double* out) {
-  // one warp, fixed order: lane l sums blocks l, l+32, ... then a fixed tree
+  // one warp, fixed order: lane l sums blocks l, l+32, ... then a fixed tree,
+  // the additive sums with compensation
   int lane = threadIdx.x;
   if (lane < 32) {
-    double acc[NSUM];
+    double acc[NSUM], cmp[NSUM];
 #pragma unroll
-    for (int k = 0; k < NSUM; k++) acc[k] = 0.0;
+    for (int k = 0; k < NSUM; k++) acc[k] = cmp[k] = 0.0;
     for (int b = lane; b < nblocks; b += 32) {
 #pragma unroll
       for (int k = 0; k < NSUM; k++) {
-        double x = __ldcg(partials + (size_t)b * NSUM + k);
-        acc[k] = (k == S_FMAX2) ? fmax(acc[k], x) : acc[k] + x;
+        const double x = __ldcg(partials + (size_t)b * NSUM + k);
+        if (k == S_FMAX2 || k == S_NONFINITE) acc[k] = fmax(acc[k], x);
+        else two_sum_add(acc[k], cmp[k], x);
       }
     }
 #pragma unroll
     for (int k = 0; k < NSUM; k++) {
-      for (int o = 16; o > 0; o >>= 1) {
-        double y = __shfl_xor_sync(0xffffffffu, acc[k], o);
-        acc[k] = (k == S_FMAX2) ? fmax(acc[k], y) : acc[k] + y;
+      if (k == S_FMAX2 || k == S_NONFINITE) {
+        for (int o = 16; o > 0; o >>= 1) acc[k] = fmax(acc[k], __shfl_xor_sync(0xffffffffu, acc[k], o));
+      } else {
+        warp_csum(acc[k], cmp[k]);
+        acc[k] += cmp[k];
       }
       if (lane == 0) out[k] = acc[k];
     }

@@ -27,14 +27,16 @@ namespace cr {
 
 // Occupancy target in threads per SM.  One lane per vertex: 512 leaves 128
 // registers per thread, where the FP64 smooth-interaction body compiles
-// without spills, and the mixed body fits 96 (640 threads).  Two lanes per
-// vertex (192-thread CTAs, tiles of up to 96 vertices): 576 threads (three
-// CTAs, 112 registers) for FP64 and 768 (four CTAs, 80 registers) for mixed,
-// so that the grid of a 39,424-vertex system (about 430 tiles) runs as one
-// wave; four or more lanes: 768 for mixed.
+// without spills.  Two lanes per vertex (192-thread CTAs, tiles of up to 96
+// vertices): 576 threads (three CTAs, 96 registers), so that the grid of a
+// 39,424-vertex system (about 430 tiles) runs as one wave.  The mixed path
+// takes the same budgets: it holds an FP64 unit body for its near-contact
+// slots beside the FP32 one, and at 80 registers (four CTAs) its spills cost
+// more than the fourth CTA gains (27.5 against 25.5 us per step measured at
+// 39,424 vertices).
 template <int PREC, int L = 1>
 constexpr int tile_threads_per_sm() {
-  return PREC == PREC_MIXED ? (L >= 2 ? 768 : 640) : (L == 2 ? 576 : 512);
+  return L >= 2 ? 576 : 512;
 }
 
 template <typename T2> __device__ __forceinline__ T2 cvt2(double2 d);
@@ -79,6 +81,111 @@ template <bool PERSIST>
 __device__ __forceinline__ double2 ld_pos(const double2* p) {
   if constexpr (PERSIST) return *p;
   else return __ldg(p);
+}
+
+// ---------------------------------------------------------------------------
+// Mixed-precision smooth units.
+//
+// Near contact the FP32 evaluation of a steep potential cannot meet a 1e-6
+// force error: one rounding of the distance or of (radSum/d)^6 moves a unit
+// force by ~1e-6 of the net force, which is a small residual of pair and
+// shape forces several times larger.  So each list slot (vertex i against
+// neighbour j: role 1, i against the segment prev(j) -> j; role 2, j against
+// i's segment prev(i) -> i) first takes a near test in FP32: whether a live
+// unit's vertex lies within f_near * radSum of its segment.  Far slots are
+// evaluated in FP32 (every term of such a unit is at least that far away);
+// near slots are evaluated afterwards exactly as the FP64 path evaluates
+// them (same differences, same arithmetic, FP64 accumulators).  Each lane
+// first walks its slots in FP32, deferring near ones to a bit mask, then
+// runs the deferred ones in FP64: each loop carries one precision, and a
+// vertex's force is the same whatever happened at earlier evaluations.
+// ---------------------------------------------------------------------------
+
+// Whether t lies within Rn of the segment q -> o (tq = t - q, w = t - o,
+// seg = o - q, len2 = |seg|^2, squared lengths precomputed), without a
+// division: an end point within Rn, or the foot of the perpendicular on the
+// segment and |tq x seg|^2 < Rn^2 |seg|^2.
+__device__ __forceinline__ bool seg_near(float2 tq, float tq2, float w2, float2 seg, float len2, float Rn2) {
+  if (tq2 < Rn2 || w2 < Rn2) return true;
+  const float dot = tq.x * seg.x + tq.y * seg.y;
+  const float cr = tq.x * seg.y - tq.y * seg.x;
+  return dot > 0.0f && dot < len2 && cr * cr < Rn2 * len2;
+}
+
+// FP32 body of one slot; returns true (and evaluates nothing) when the slot
+// is near and belongs to the FP64 pass.  The slot's FP32 sums enter the FP64
+// accumulators.  seg_i64 = x_i - x_q (q = prev(i)).
+template <int POT, class B>
+__device__ __forceinline__ bool mixed_slot_f32(const SysParams& p, const B& bx, double2 xi, double2 seg_i64,
+                                               float2 seg_i, float2 pseg_i, float len2_i, float len_i, double ri,
+                                               double rj, double2 xj, double2 xjq, double2 xjqq, double2& fi64,
+                                               double2& fq64, double& ei) {
+  const double rsum64 = ri + rj;
+  const float rsum = (float)rsum64;
+  const float R = pot_range_f<POT>(p) * rsum;
+  const double2 w64 = pbc2(bx, xi, xj);    // x_i - x_j
+  const double2 tq64 = pbc2(bx, xi, xjq);  // x_i - x_jq
+  const float2 w1 = f2(w64), tq1 = f2(tq64);
+  const float2 seg1 = f2(make_double2(tq64.x - w64.x, tq64.y - w64.y));      // x_j - x_jq
+  const float2 tq2 = f2(make_double2(seg_i64.x - w64.x, seg_i64.y - w64.y));  // x_j - x_q
+  const float w2 = fmaf(w1.y, w1.y, w1.x * w1.x);
+  const float tq1_2 = fmaf(tq1.y, tq1.y, tq1.x * tq1.x);
+  const float len1 = fmaf(seg1.y, seg1.y, seg1.x * seg1.x);
+  const float tq2_2 = fmaf(tq2.y, tq2.y, tq2.x * tq2.x);
+  const bool in1 = !smooth_out_of_range(R, tq1_2, w2, sqrtf(len1));
+  const bool in2 = !smooth_out_of_range(R, tq2_2, w2, len_i);
+  if (!(in1 | in2)) return false;
+  const float Rn = p.f_near * rsum, Rn2 = Rn * Rn;
+  if ((in1 && seg_near(tq1, tq1_2, w2, seg1, len1, Rn2)) || (in2 && seg_near(tq2, tq2_2, w2, seg_i, len2_i, Rn2)))
+    return true;
+  const float inv_rsum = 1.0f / rsum;
+  float2 fs{0.0f, 0.0f}, fqs{0.0f, 0.0f}, dummy{0.0f, 0.0f};
+  if (in1) {
+    const float2 pseg1 = f2(pbc2(bx, xjq, xjqq));  // x_jq - x_jqq
+    smooth_core<POT, true, float>(p, bx, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fs, dummy, dummy,
+                                  ei);
+  }
+  if (in2) {
+    const float2 mw1{-w1.x, -w1.y};  // x_j - x_i
+    smooth_core<POT, false, float>(p, bx, tq2, tq2_2, mw1, seg_i, len2_i, pseg_i, rsum, inv_rsum, xj, xj, dummy, fs,
+                                   fqs, ei);  // (box coordinates are read by the FP64 body only)
+  }
+  fi64.x += (double)fs.x;
+  fi64.y += (double)fs.y;
+  fq64.x += (double)fqs.x;
+  fq64.y += (double)fqs.y;
+  return false;
+}
+
+// FP64 body of one slot: the FP64 path's own arithmetic (its differences of
+// box coordinates and its skip tests).
+template <int POT, class B>
+__device__ __forceinline__ void smooth_slot_f64(const SysParams& p, const B& bx, double2 xi, double2 xq,
+                                                double2 seg_i, double2 pseg_i, double len2_i, float len_i, double ri,
+                                                double rj, double2 xj, double2 xjq, double2 xjqq, double2& fi,
+                                                double2& fq, double& ei) {
+  const double rsum = ri + rj;
+  const double inv_rsum = 1.0 / rsum;
+  const float R = pot_range_f<POT>(p) * (float)rsum;
+  const double2 w1 = pbc2(bx, xi, xj);    // x_i - x_j
+  const double2 tq1 = pbc2(bx, xi, xjq);  // x_i - x_jq
+  const double2 seg1 = pbc2(bx, xj, xjq);  // x_j - x_jq
+  const double2 tq2 = pbc2(bx, xj, xq);    // x_j - x_q
+  const double w2 = fma(w1.y, w1.y, w1.x * w1.x);
+  const double tq1_2 = fma(tq1.y, tq1.y, tq1.x * tq1.x);
+  const double len1 = fma(seg1.y, seg1.y, seg1.x * seg1.x);
+  const double tq2_2 = fma(tq2.y, tq2.y, tq2.x * tq2.x);
+  double2 dummy{0.0, 0.0};
+  if (!smooth_out_of_range(R, (float)tq1_2, (float)w2, sqrtf((float)len1))) {
+    const double2 pseg1 = pbc2(bx, xjq, xjqq);  // x_jq - x_jqq
+    smooth_core<POT, true, double>(p, bx, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fi, dummy, dummy,
+                                   ei);
+  }
+  if (!smooth_out_of_range(R, (float)tq2_2, (float)w2, len_i)) {
+    const double2 mw1{-w1.x, -w1.y};  // x_j - x_i
+    smooth_core<POT, false, double>(p, bx, tq2, tq2_2, mw1, seg_i, len2_i, pseg_i, rsum, inv_rsum, xj, xq, dummy, fi,
+                                    fq, ei);
+  }
 }
 
 // One step (or force evaluation) of one tile.  pin / pout: positions read
@@ -234,6 +341,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
     const int lv = t / L, lane = t % L;
     using T = typename std::conditional<PREC == PREC_MIXED, float, double>::type;
     typename Vec2<T>::type fi{0, 0}, fq{0, 0};
+    double2 fi64{0.0, 0.0}, fq64{0.0, 0.0};  // mixed smooth path: FP64 accumulators
     double ei = 0.0;
     if (lv < nvt) {
       const int i = v0 + lv;
@@ -273,11 +381,70 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
           if constexpr (PREC == PREC_MIXED) pair_own_f<POT>(p, f2(pbc2(bx, xi, xj)), (float)(ri + rj), fi, ei);
           else pair_own<POT>(p, pbc2(bx, xi, xj), ri + rj, fi, ei);
         }
+      } else if constexpr (PREC == PREC_MIXED) {
+        // Smooth units, mixed precision: the lane's slots in FP32, near ones
+        // deferred (64 lane slots at a time), then the deferred ones in FP64
+        const int lq = s_lp[lv], lqq = s_lp[lq];
+        const double2 seg_i64 = s_seg[lq];  // x_i - x_q
+        const float2 seg_i = f2(seg_i64), pseg_i = f2(s_seg[lqq]);  // x_q - x_qq
+        const float len2_i = fmaf(seg_i.y, seg_i.y, seg_i.x * seg_i.x);
+        const float len_i = sqrtf(len2_i);
+        for (int base = lane; base < cnt; base += 64 * L) {
+          const int end = min(cnt, base + 64 * L);
+          unsigned long long late = 0ull;
+          int s0 = base;
+          int j1 = 0, pk1 = 0;
+          const int j0 = __ldg(a.nbr + (size_t)s0 * stride + i), pk0 = __ldg(a.nbr_pq + (size_t)s0 * stride + i);
+          if (s0 + L < end) {
+            j1 = __ldg(a.nbr + (size_t)(s0 + L) * stride + i);
+            pk1 = __ldg(a.nbr_pq + (size_t)(s0 + L) * stride + i);
+          }
+          double2 xj = ld_pos<PERSIST>(pin + j0), xjq = ld_pos<PERSIST>(pin + j0 + pq_first(pk0)),
+                  xjqq = ld_pos<PERSIST>(pin + j0 + pq_second(pk0));
+          double rj = __ldg(a.rad + j0);
+          while (true) {
+            const int s1 = s0 + L;
+            int j2 = 0, pk2 = 0;
+            double2 nxj = xj, nxjq = xjq, nxjqq = xjqq;
+            double nr = rj;
+            if (s1 < end) {
+              if (s1 + L < end) {
+                j2 = __ldg(a.nbr + (size_t)(s1 + L) * stride + i);
+                pk2 = __ldg(a.nbr_pq + (size_t)(s1 + L) * stride + i);
+              }
+              nxj = ld_pos<PERSIST>(pin + j1);
+              nxjq = ld_pos<PERSIST>(pin + j1 + pq_first(pk1));
+              nxjqq = ld_pos<PERSIST>(pin + j1 + pq_second(pk1));
+              nr = __ldg(a.rad + j1);
+            }
+            if (mixed_slot_f32<POT>(p, bx, xi, seg_i64, seg_i, pseg_i, len2_i, len_i, ri, rj, xj, xjq, xjqq, fi64,
+                                    fq64, ei))
+              late |= 1ull << ((s0 - base) / L);
+            if (s1 >= end) break;
+            s0 = s1;
+            xj = nxj;
+            xjq = nxjq;
+            xjqq = nxjqq;
+            rj = nr;
+            j1 = j2;
+            pk1 = pk2;
+          }
+          if (late) {
+            const double2 xq = s_pos[lq], pseg_i64 = s_seg[lqq];
+            const double len2_i64 = fma(seg_i64.y, seg_i64.y, seg_i64.x * seg_i64.x);
+            const float len_i64 = sqrtf((float)len2_i64);
+            for (; late; late &= late - 1ull) {
+              const int s = base + (__ffsll((long long)late) - 1) * L;
+              const int j = __ldg(a.nbr + (size_t)s * stride + i), pk = __ldg(a.nbr_pq + (size_t)s * stride + i);
+              smooth_slot_f64<POT>(p, bx, xi, xq, seg_i64, pseg_i64, len2_i64, len_i64, ri, __ldg(a.rad + j),
+                                   ld_pos<PERSIST>(pin + j), ld_pos<PERSIST>(pin + j + pq_first(pk)),
+                                   ld_pos<PERSIST>(pin + j + pq_second(pk)), fi64, fq64, ei);
+            }
+          }
+        }
       } else {
         // Smooth units of vertex i: role 1 (i against the segment prev(j) -> j)
-        // and role 2 (j against i's own segment prev(i) -> i).  Offsets are
-        // formed in FP64 from the positions and, on the mixed path, rounded
-        // once to FP32 for the unit arithmetic.
+        // and role 2 (j against i's own segment prev(i) -> i), in FP64.
         using T2 = typename Vec2<T>::type;
         const int lq = s_lp[lv];
         const double2 xq = s_pos[lq];
@@ -355,11 +522,22 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         fq.x += __shfl_xor_sync(0xffffffffu, fq.x, o);
         fq.y += __shfl_xor_sync(0xffffffffu, fq.y, o);
       }
+      if constexpr (INTER == INT_SMOOTH && PREC == PREC_MIXED) {
+        fi64.x += __shfl_xor_sync(0xffffffffu, fi64.x, o);
+        fi64.y += __shfl_xor_sync(0xffffffffu, fi64.y, o);
+        fq64.x += __shfl_xor_sync(0xffffffffu, fq64.x, o);
+        fq64.y += __shfl_xor_sync(0xffffffffu, fq64.y, o);
+      }
     }
     if (lane == 0 && lv < nvt) {
-      s_fpair[lv] = make_double2(fi.x, fi.y);
+      if constexpr (INTER == INT_SMOOTH && PREC == PREC_MIXED) {
+        s_fpair[lv] = fi64;
+        s_fprev[lv] = fq64;
+      } else {
+        s_fpair[lv] = make_double2(fi.x, fi.y);
+        s_fprev[lv] = make_double2(fq.x, fq.y);
+      }
       s_epair[lv] = ei;
-      s_fprev[lv] = make_double2(fq.x, fq.y);
     }
   }
   __syncthreads();
@@ -543,23 +721,8 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
       if (t < nvt && k == 0) s.p_energy[ring] = s_r1[t];
     }
     if (s.accumulate) {
-      // per-CTA partials in a fixed order
-      const int warp = t / 32, wl = t % 32;
-#pragma unroll
-      for (int q = 0; q < NSUM; q++) {
-        double x = sums[q];
-        for (int o = 16; o > 0; o >>= 1) {
-          double y = __shfl_xor_sync(0xffffffffu, x, o);
-          x = (q == S_FMAX2) ? fmax(x, y) : x + y;
-        }
-        if (wl == 0) s_red[warp][q] = x;
-      }
-      __syncthreads();
-      if (t < NSUM) {
-        double x = 0.0;
-        for (int w = 0; w < BLOCK / 32; w++) x = (t == S_FMAX2) ? fmax(x, s_red[w][t]) : x + s_red[w][t];
-        s.partials[(size_t)blockIdx.x * NSUM + t] = x;
-      }
+      // per-CTA partials in a fixed order, compensated
+      block_partials<BLOCK>(sums, s_red, s.partials + (size_t)blockIdx.x * NSUM);
     } else if (__syncthreads_or(nonfinite) && t == 0) {
       if constexpr (PERSIST) {
         atomicOr(pflag, 2);
