@@ -120,11 +120,12 @@ __device__ __forceinline__ int pq_first(int pk) { return (int)(short)(pk & 0xfff
 __device__ __forceinline__ int pq_second(int pk) { return pk >> 16; }
 
 // Minimum-image difference, reference pbcDistance (include/cudaKernel.cuh:70-74)
-// with delta/size replaced by delta*(1/size); the two agree except when
+// with delta/size replaced by delta*(1/size) and round-half-away by
+// round-half-even (one rounding instruction); the two agree except when
 // delta/size lies within one ulp of a half-integer, i.e. |delta| ~ L/2, far
 // outside every interaction and list range.
 __device__ __forceinline__ double pbc1(double d, double size, double inv) {
-  return d - size * round(d * inv);
+  return d - size * rint(d * inv);
 }
 // B: anything with lx, ly, inv_lx, inv_ly (SysParams, or Box for one system
 // of a batch)

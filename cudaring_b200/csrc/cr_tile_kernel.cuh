@@ -126,7 +126,12 @@ __device__ __forceinline__ bool mixed_slot_f32(const SysParams& p, const B& bx, 
   const double2 w64 = pbc2(bx, xi, xj);    // x_i - x_j
   const double2 tq64 = pbc2(bx, xi, xjq);  // x_i - x_jq
   const float2 w1 = f2(w64), tq1 = f2(tq64);
-  const float2 seg1 = f2(make_double2(tq64.x - w64.x, tq64.y - w64.y));      // x_j - x_jq
+  // x_j - x_jq as the difference of the two offsets from x_i: the same image
+  // of ring j unless x_j and x_jq have their nearest images on different
+  // sides (a box under about twice the interaction range); then directly
+  double2 seg1_64 = make_double2(tq64.x - w64.x, tq64.y - w64.y);
+  if (fabs(seg1_64.x) > 0.25 * bx.lx || fabs(seg1_64.y) > 0.25 * bx.ly) seg1_64 = pbc2(bx, xj, xjq);
+  const float2 seg1 = f2(seg1_64);
   const float2 tq2 = f2(make_double2(seg_i64.x - w64.x, seg_i64.y - w64.y));  // x_j - x_q
   const float w2 = fmaf(w1.y, w1.y, w1.x * w1.x);
   const float tq1_2 = fmaf(tq1.y, tq1.y, tq1.x * tq1.x);
@@ -157,8 +162,10 @@ __device__ __forceinline__ bool mixed_slot_f32(const SysParams& p, const B& bx, 
   return false;
 }
 
-// FP64 body of one slot: the FP64 path's own arithmetic (its differences of
-// box coordinates and its skip tests).
+// FP64 body of one slot, shared by the FP64 path and the mixed path's
+// near-contact slots: the reference's own differences of box coordinates
+// (pbcDistance of each pair of vertices) and the FP64 skip tests.
+// seg_i = x_i - x_q, pseg_i = x_q - x_qq: vertex i's segments (q = prev(i)).
 template <int POT, class B>
 __device__ __forceinline__ void smooth_slot_f64(const SysParams& p, const B& bx, double2 xi, double2 xq,
                                                 double2 seg_i, double2 pseg_i, double len2_i, float len_i, double ri,
@@ -167,8 +174,8 @@ __device__ __forceinline__ void smooth_slot_f64(const SysParams& p, const B& bx,
   const double rsum = ri + rj;
   const double inv_rsum = 1.0 / rsum;
   const float R = pot_range_f<POT>(p) * (float)rsum;
-  const double2 w1 = pbc2(bx, xi, xj);    // x_i - x_j
-  const double2 tq1 = pbc2(bx, xi, xjq);  // x_i - x_jq
+  const double2 w1 = pbc2(bx, xi, xj);     // x_i - x_j
+  const double2 tq1 = pbc2(bx, xi, xjq);   // x_i - x_jq
   const double2 seg1 = pbc2(bx, xj, xjq);  // x_j - x_jq
   const double2 tq2 = pbc2(bx, xj, xq);    // x_j - x_q
   const double w2 = fma(w1.y, w1.y, w1.x * w1.x);
@@ -178,8 +185,8 @@ __device__ __forceinline__ void smooth_slot_f64(const SysParams& p, const B& bx,
   double2 dummy{0.0, 0.0};
   if (!smooth_out_of_range(R, (float)tq1_2, (float)w2, sqrtf((float)len1))) {
     const double2 pseg1 = pbc2(bx, xjq, xjqq);  // x_jq - x_jqq
-    smooth_core<POT, true, double>(p, bx, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fi, dummy, dummy,
-                                   ei);
+    smooth_core<POT, true, double>(p, bx, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fi, dummy,
+                                   dummy, ei);
   }
   if (!smooth_out_of_range(R, (float)tq2_2, (float)w2, len_i)) {
     const double2 mw1{-w1.x, -w1.y};  // x_j - x_i
@@ -381,7 +388,40 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
           if constexpr (PREC == PREC_MIXED) pair_own_f<POT>(p, f2(pbc2(bx, xi, xj)), (float)(ri + rj), fi, ei);
           else pair_own<POT>(p, pbc2(bx, xi, xj), ri + rj, fi, ei);
         }
-      } else if constexpr (PREC == PREC_MIXED) {
+      } else if constexpr (PREC == PREC_FP64) {
+        // Smooth units of vertex i: role 1 (i against the segment prev(j) -> j)
+        // and role 2 (j against i's own segment prev(i) -> i), in FP64.
+        const int lq = s_lp[lv];
+        const double2 xq = s_pos[lq];
+        const double2 seg_i64 = s_seg[lq];         // x_i - x_q
+        const double2 pseg_i64 = s_seg[s_lp[lq]];  // x_q - x_qq
+        const double len2_i = fma(seg_i64.y, seg_i64.y, seg_i64.x * seg_i64.x);
+        const float len_i = sqrtf((float)len2_i);
+        double2 nxj = make_double2(0.0, 0.0), nxjq = nxj, nxjqq = nxj;
+        double nr = 0.0;
+        if (sl < cnt) {
+          nxj = ld_pos<PERSIST>(pin + jn);
+          nxjq = ld_pos<PERSIST>(pin + jn + pq_first(pkn));
+          nxjqq = ld_pos<PERSIST>(pin + jn + pq_second(pkn));
+          nr = __ldg(a.rad + jn);
+        }
+        while (sl < cnt) {
+          const double2 xj = nxj, xjq = nxjq, xjqq = nxjqq;
+          const double rj = nr;
+          sl += L;
+          if (sl < cnt) {
+            nxj = ld_pos<PERSIST>(pin + j2);
+            nxjq = ld_pos<PERSIST>(pin + j2 + pq_first(pk2));
+            nxjqq = ld_pos<PERSIST>(pin + j2 + pq_second(pk2));
+            nr = __ldg(a.rad + j2);
+            if (sl + L < cnt) {
+              j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
+              pk2 = __ldg(a.nbr_pq + (size_t)(sl + L) * stride + i);
+            }
+          }
+          smooth_slot_f64<POT>(p, bx, xi, xq, seg_i64, pseg_i64, len2_i, len_i, ri, rj, xj, xjq, xjqq, fi, fq, ei);
+        }
+      } else {
         // Smooth units, mixed precision: the lane's slots in FP32, near ones
         // deferred (64 lane slots at a time), then the deferred ones in FP64
         const int lq = s_lp[lv], lqq = s_lp[lq];
@@ -440,74 +480,6 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
                                    ld_pos<PERSIST>(pin + j), ld_pos<PERSIST>(pin + j + pq_first(pk)),
                                    ld_pos<PERSIST>(pin + j + pq_second(pk)), fi64, fq64, ei);
             }
-          }
-        }
-      } else {
-        // Smooth units of vertex i: role 1 (i against the segment prev(j) -> j)
-        // and role 2 (j against i's own segment prev(i) -> i), in FP64.
-        using T2 = typename Vec2<T>::type;
-        const int lq = s_lp[lv];
-        const double2 xq = s_pos[lq];
-        const double2 seg_i64 = s_seg[lq];                // x_i - x_q
-        const T2 seg_i = cvt2<T2>(seg_i64);
-        const T2 pseg_i = cvt2<T2>(s_seg[s_lp[lq]]);      // x_q - x_qq
-        const T len2_i = fma(seg_i.y, seg_i.y, seg_i.x * seg_i.x);
-        const float len_i = sqrtf((float)len2_i);
-        const float range = pot_range_f<POT>(p);
-        T2 dummy{0, 0};
-        double2 nxj = make_double2(0.0, 0.0), nxjq = nxj, nxjqq = nxj;
-        double nr = 0.0;
-        if (sl < cnt) {
-          nxj = ld_pos<PERSIST>(pin + jn);
-          nxjq = ld_pos<PERSIST>(pin + jn + pq_first(pkn));
-          nxjqq = ld_pos<PERSIST>(pin + jn + pq_second(pkn));
-          nr = __ldg(a.rad + jn);
-        }
-        while (sl < cnt) {
-          const double2 xj = nxj, xjq = nxjq, xjqq = nxjqq;
-          const double rsum64 = ri + nr;
-          sl += L;
-          if (sl < cnt) {
-            nxj = ld_pos<PERSIST>(pin + j2);
-            nxjq = ld_pos<PERSIST>(pin + j2 + pq_first(pk2));
-            nxjqq = ld_pos<PERSIST>(pin + j2 + pq_second(pk2));
-            nr = __ldg(a.rad + j2);
-            if (sl + L < cnt) {
-              j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
-              pk2 = __ldg(a.nbr_pq + (size_t)(sl + L) * stride + i);
-            }
-          }
-          const T rsum = (T)rsum64;
-          const T inv_rsum = T(1) / rsum;
-          const float R = range * (float)rsum64;
-          const double2 w64 = pbc2(bx, xi, xj);    // x_i - x_j
-          const double2 tq64 = pbc2(bx, xi, xjq);  // x_i - x_jq
-          double2 seg1_64, tq2_64;
-          if constexpr (PREC == PREC_FP64) {
-            // the reference's own differences of box coordinates
-            seg1_64 = pbc2(bx, xj, xjq);
-            tq2_64 = pbc2(bx, xj, xq);
-          } else {
-            seg1_64 = make_double2(tq64.x - w64.x, tq64.y - w64.y);
-            tq2_64 = make_double2(seg_i64.x - w64.x, seg_i64.y - w64.y);
-          }
-          const T2 w1 = cvt2<T2>(w64);
-          const T2 tq1 = cvt2<T2>(tq64);
-          const T2 seg1 = cvt2<T2>(seg1_64);  // x_j - x_jq
-          const T2 tq2 = cvt2<T2>(tq2_64);    // x_j - x_q
-          const T w2 = fma(w1.y, w1.y, w1.x * w1.x);
-          const T tq1_2 = fma(tq1.y, tq1.y, tq1.x * tq1.x);
-          const T len1 = fma(seg1.y, seg1.y, seg1.x * seg1.x);
-          const T tq2_2 = fma(tq2.y, tq2.y, tq2.x * tq2.x);
-          if (!smooth_out_of_range(R, (float)tq1_2, (float)w2, sqrtf((float)len1))) {
-            const T2 pseg1 = cvt2<T2>(pbc2(bx, xjq, xjqq));  // x_jq - x_jqq
-            smooth_core<POT, true, T>(p, bx, tq1, tq1_2, w1, seg1, len1, pseg1, rsum, inv_rsum, xi, xjq, fi, dummy,
-                                      dummy, ei);
-          }
-          if (!smooth_out_of_range(R, (float)tq2_2, (float)w2, len_i)) {
-            const T2 mw1{-w1.x, -w1.y};  // x_j - x_i
-            smooth_core<POT, false, T>(p, bx, tq2, tq2_2, mw1, seg_i, len2_i, pseg_i, rsum, inv_rsum, xj, xq, dummy, fi,
-                                       fq, ei);
           }
         }
       }

@@ -228,3 +228,64 @@ def nve_adjoint_reference(sys_: System, pk, nsteps: int, dt: float, eps: float =
         vb = vb + dt * xb
         xb = xb - 0.5 * dt * hvp(xs[n], vb)
     return J, xb, vb
+
+
+def compress_search_step(R, sigma: float, phi: float, prev_phi: float, dphi: float, current: tuple, saved: tuple,
+                         fire_dt: float = 1e-2, tol0: float = 1e-10, max_iter: int = 100000,
+                         min_dphi: float = 0.0, cut_distance: float | None = None) -> dict:
+    """One search step of the quasi-static compression of compressFIRE.cpp:101-205
+    on the reference's own kernels (oracle/_ref ``R`` holding the system), without
+    the driver's file output and its Langevin thermalisation:
+
+    * FIRE (vertexFIREparams {0.2, 0.5, 1.1, 0.99, dt, 10 dt, 0.2}, minStep 20,
+      dt = fire_dt * sigma, :102-106) from a fresh list and fresh forces
+      (:107-109), iterated while max |F| > tol0 / sigma (:115-125);
+    * jammed: tol < F < 2 tol (:138) -> state 1;
+    * under-jammed: F < tol -> this state becomes the saved one and phi grows
+      by dphi, scale sqrt((phi + dphi) / phi) (:152-160);
+    * over-jammed: F > 2 tol -> dphi halves, the saved state comes back and
+      its phi grows by the halved step (:161-171);
+    * scaleVertices about the ring centroids of the last force evaluation,
+      then getPhi (:196-197).
+    ``current`` = (rad, l0, a0) of the system as it is (the reference library
+    does not return them), ``saved`` = (pos, rad, l0, a0) of the last
+    under-jammed state.  A halved step below ``min_dphi`` ends the search
+    (state 3).  Returns the new state, phi, saved phi, dphi, current and saved
+    arrays, the FIRE iterations and the final max |F|."""
+    dt = fire_dt * sigma
+    R.ref_fire_init(np.array([0.2, 0.5, 1.1, 0.99, dt, 10 * dt, 0.2]), 20, 0)
+    if cut_distance is None:
+        cut_distance = R.ref_set_displacement_cutoff(0.5, 2 * float(np.mean(current[0])))
+    R.ref_calc_neighbor_list(cut_distance)
+    R.ref_calc_force_energy()
+    R.ref_reset_last_positions()
+    tol = tol0 / sigma
+    it, fmax = 0, R.ref_max_unbalanced_force()
+    while fmax > tol and it != max_iter:
+        R.ref_fire_loop(1)
+        fmax = R.ref_max_unbalanced_force()
+        it += 1
+    state, scale = 0, 1.0
+    if tol < fmax < 2 * tol:
+        state = 1
+    elif fmax < tol:
+        scale = math.sqrt((phi + dphi) / phi)
+        prev_phi = phi
+        pos = np.zeros(2 * len(current[0]))
+        R.ref_get(0, pos)
+        saved = (pos, *current)
+    elif fmax > 2 * tol:
+        dphi *= 0.5
+        scale = math.sqrt((prev_phi + dphi) / prev_phi)
+        spos, srad, sl0, sa0 = (np.ascontiguousarray(a, dtype=np.float64) for a in saved)
+        R.ref_set_state(spos.ctypes.data, None, srad.ctypes.data, sl0.ctypes.data, None, sa0.ctypes.data)
+        R.ref_calc_force_energy()  # ring centroids of the restored state
+        current = saved[1:]
+    if state == 0 and dphi < min_dphi:
+        state = 3
+    if state == 0:
+        R.ref_scale_vertices(scale)
+        phi = R.ref_phi()
+        current = (current[0] * scale, current[1] * scale, current[2] * scale * scale)
+    return {"state": state, "phi": phi, "prev_phi": prev_phi, "dphi": dphi, "current": current, "saved": saved,
+            "iterations": it, "fmax": fmax, "scale": scale}
