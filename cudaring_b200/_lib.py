@@ -21,6 +21,7 @@ _TYPES = {
     "int": C.c_int,
     "long": C.c_long,
     "double": C.c_double,
+    "long long": C.c_longlong,
     "unsigned long long": C.c_ulonglong,
 }
 

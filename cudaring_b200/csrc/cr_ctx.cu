@@ -136,6 +136,14 @@ struct cr_ctx {
   FireParams fp{};
   bool use_graphs = true;
   bool multistep = true;  // middle steps of NVE / Langevin / BAOAB runs in k_tile_steps
+  // A grid-barrier wait gave up (the GPU did not hold every CTA of a
+  // one-launch build or multi-step kernel at once, e.g. because other work
+  // shared it): from then on one launch per op, no graphs, and the list built
+  // by the multi-kernel path, whose kernels never wait for one another.
+  bool degraded = false;
+  // state at the start of a multi-step sequence, restored if a barrier gives up
+  double2 *snap_pos = nullptr, *snap_vel = nullptr, *snap_force = nullptr, *snap_last = nullptr;
+  double* snap_angle = nullptr;
 
   std::map<std::tuple<int, long, int, int, unsigned long long>, GraphEntry> graphs;
 
@@ -172,6 +180,14 @@ void drop_graphs(cr_ctx* ctx) {
     if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
   }
   ctx->soft_graphs.clear();
+}
+
+// After a grid-barrier wait gave up: one launch per op from now on.
+void enter_degraded(cr_ctx* ctx) {
+  ctx->degraded = true;
+  ctx->multistep = false;
+  ctx->use_graphs = false;
+  drop_graphs(ctx);
 }
 
 void refresh_params(cr_ctx* ctx) {
@@ -377,12 +393,28 @@ int build_list(cr_ctx* ctx, int buf, double cut) {
   int rc;
   if ((rc = setup_grid(ctx, cut))) return rc;
   for (int pass = 0; pass < 3; pass++) {
-    launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nbr_args(ctx, buf, cut), nbr_fused_blocks(ctx->nv, ctx->fused_max),
-                     1);
-    ctx->launches += 1;
+    if (ctx->degraded) {
+      // the multi-kernel build: per-cell counters start at zero
+      if (ctx->grid.ncx)
+        CR_TRY(cudaMemsetAsync(ctx->cell_cnt, 0, (size_t)ctx->grid.ncx * ctx->grid.ncy * sizeof(int), ctx->stream));
+      launch_nbr_build(ctx->stream, ctx->p, ctx->grid, nbr_args(ctx, buf, cut));
+      ctx->launches += 6;
+    } else {
+      launch_nbr_fused(ctx->stream, ctx->p, ctx->grid, nbr_args(ctx, buf, cut),
+                       nbr_fused_blocks(ctx->nv, ctx->fused_max), 1);
+      ctx->launches += 1;
+    }
     CR_TRY(cudaGetLastError());
     if ((rc = read_status(ctx))) return rc;
-    if (ctx->status_h->stalled) return ctx->fail(CR_ECUDA, "neighbour-list build: a grid barrier timed out");
+    if (ctx->status_h->stalled) {
+      if (ctx->degraded) return ctx->fail(CR_ECUDA, "neighbour-list build: a grid barrier timed out");
+      // the one-launch build's CTAs were not all resident: build again with
+      // the multi-kernel path (positions are untouched by a build)
+      enter_degraded(ctx);
+      if ((rc = clear_flags(ctx))) return rc;
+      pass = -1;
+      continue;
+    }
     const int mc = ctx->status_h->max_count;
     if (!ctx->status_h->overflow) {
       ctx->list_size_ref = std::max<long long>(ctx->list_size_ref, mc > 0 ? pow2ceil(mc) : 0);
@@ -655,9 +687,56 @@ int capture_steps_graph(cr_ctx* ctx, int kind, int b, int launches, GraphEntry& 
   return CR_OK;
 }
 
+int run_ops(cr_ctx* ctx, int kind, long nsteps);
+
+// The state a multi-step sequence starts from (positions, velocities,
+// forces, last-build positions, self-propulsion angles), saved or restored.
+int sequence_state(cr_ctx* ctx, int b, bool restore) {
+  int rc;
+  if (!ctx->snap_pos) {
+    if ((rc = dalloc(ctx, &ctx->snap_pos, ctx->nv)) || (rc = dalloc(ctx, &ctx->snap_vel, ctx->nv)) ||
+        (rc = dalloc(ctx, &ctx->snap_force, ctx->nv)) || (rc = dalloc(ctx, &ctx->snap_last, ctx->nv)) ||
+        (rc = dalloc(ctx, &ctx->snap_angle, ctx->np)))
+      return rc;
+  }
+  const size_t v2 = (size_t)ctx->nv * sizeof(double2), pa = (size_t)ctx->np * sizeof(double);
+  double2* live[4] = {ctx->pos[b], ctx->vel, ctx->force, ctx->last_pos};
+  double2* saved[4] = {ctx->snap_pos, ctx->snap_vel, ctx->snap_force, ctx->snap_last};
+  for (int k = 0; k < 4; k++)
+    CR_TRY(cudaMemcpyAsync(restore ? live[k] : saved[k], restore ? saved[k] : live[k], v2, cudaMemcpyDeviceToDevice,
+                           ctx->stream));
+  CR_TRY(cudaMemcpyAsync(restore ? ctx->p_angle : ctx->snap_angle, restore ? ctx->snap_angle : ctx->p_angle, pa,
+                         cudaMemcpyDeviceToDevice, ctx->stream));
+  return CR_OK;
+}
+
+// A grid barrier of the multi-step kernel or of its builds gave up, leaving
+// the sequence's positions partly advanced: go back to the state it started
+// from (counters included), rebuild the list there with the multi-kernel
+// build and run the whole sequence again one launch per op.
+int rerun_degraded(cr_ctx* ctx, int b0, const DevStatus& start, int kind, long nsteps) {
+  int rc;
+  CR_TRY(cudaStreamSynchronize(ctx->stream));
+  if ((rc = sequence_state(ctx, b0, true))) return rc;
+  ctx->cur = b0;
+  DevStatus s = start;
+  s.abort = s.overflow = s.rebuild = s.converged = s.nonfinite = s.stalled = 0;
+  s.done_ctr = s.bar_count = s.pbar = 0;
+  s.pflag[0] = s.pflag[1] = s.pflag[2] = 0;
+  s.pbase = s.steps_left = 0;
+  *ctx->status_h = s;
+  if ((rc = upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus)))) return rc;
+  enter_degraded(ctx);
+  if ((rc = build_list(ctx, b0, ctx->cut_distance))) return rc;
+  return run_ops(ctx, kind, nsteps);
+}
+
 int run_steps(cr_ctx* ctx, int kind, long nsteps) {
   int rc;
   int b = ctx->cur;
+  const int b0 = b;
+  const DevStatus start = *ctx->status_h;  // read by the caller's clear_flags
+  if ((rc = sequence_state(ctx, b0, false))) return rc;
   // drift (first half kick + drift) and its displacement check
   enqueue_op(ctx, ctx->stream, Op{OP_DRIFT, b, b ^ 1, 0, 1, b ^ 1}, kind, false, 0);
   {
@@ -686,7 +765,7 @@ int run_steps(cr_ctx* ctx, int kind, long nsteps) {
     if ((rc = read_status(ctx))) return rc;
     const DevStatus& st = *ctx->status_h;
     if (st.abort) {
-      if (st.stalled) return ctx->fail(CR_ECUDA, "a grid barrier timed out");
+      if (st.stalled) return rerun_degraded(ctx, b0, start, kind, nsteps);
       if (st.nonfinite) return ctx->fail(CR_ENONFINITE, "non-finite force during the step sequence");
       if (!st.overflow) return ctx->fail(CR_ECUDA, "step sequence aborted");
       // a rebuild found more neighbours than capacity: grow the list, rebuild
@@ -767,16 +846,19 @@ int run_ops(cr_ctx* ctx, int kind, long nsteps) {
     }
     if ((rc = read_status(ctx))) return rc;
     if (ctx->status_h->abort) {
-      if (ctx->status_h->stalled) return ctx->fail(CR_ECUDA, "neighbour-list build: a grid barrier timed out");
-      if (ctx->status_h->nonfinite) return ctx->fail(CR_ENONFINITE, "non-finite force during the step sequence");
-      if (!ctx->status_h->overflow) return ctx->fail(CR_ECUDA, "step sequence aborted");
+      // a stalled one-launch build (its CTAs were not all resident) is
+      // resumed like an overflowed one, one launch per op from here on
+      const bool stall = ctx->status_h->stalled != 0;
+      if (stall) enter_degraded(ctx);
+      else if (ctx->status_h->nonfinite) return ctx->fail(CR_ENONFINITE, "non-finite force during the step sequence");
+      else if (!ctx->status_h->overflow) return ctx->fail(CR_ECUDA, "step sequence aborted");
       // locate the op after which the failed build ran (builds are not ops)
       long long k = ctx->status_h->ops_done - ops0;
       size_t j = c;
       while (j < c_end && k >= (long long)plan[j].size()) k -= (long long)plan[j++].size();
       if (j >= c_end || k == 0) return ctx->fail(CR_ECUDA, "inconsistent op counter after abort");
       if ((rc = clear_flags(ctx))) return rc;
-      ctx->cap = 0;  // build_list grows from the measured count
+      if (!stall) ctx->cap = 0;  // build_list grows from the measured count
       if ((rc = build_list(ctx, plan[j][(size_t)k - 1].check_buf, ctx->cut_distance))) return rc;
       if ((rc = clear_flags(ctx))) return rc;
       // the failed build was a displacement-triggered rebuild: count it, as the
@@ -978,7 +1060,8 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec, ctx->diff_area, ctx->cg_state,
                   ctx->cg_part,
                   ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum,
-                  ctx->prad, ctx->plast, ctx->pid, ctx->pnbr, ctx->pnbr_cnt, ctx->pstatus, ctx->pfire, ctx->pdraws};
+                  ctx->prad, ctx->plast, ctx->pid, ctx->pnbr, ctx->pnbr_cnt, ctx->pstatus, ctx->pfire, ctx->pdraws,
+                  ctx->snap_pos, ctx->snap_vel, ctx->snap_force, ctx->snap_last, ctx->snap_angle};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (ctx->status_h) cudaFreeHost(ctx->status_h);
@@ -1879,6 +1962,20 @@ int cr_get_precision(const cr_ctx* ctx, int* precision) {
 int cr_set_multistep(cr_ctx* ctx, int on) {
   if (!ctx) return CR_EINVAL;
   ctx->multistep = on != 0;
+  return CR_OK;
+}
+
+int cr_set_spin_limit(cr_ctx* ctx, long long polls) {
+  if (!ctx || polls < 0) return CR_EINVAL;
+  int rc = read_status(ctx);
+  if (rc) return rc;
+  ctx->status_h->spin_limit = polls;
+  return upload(ctx, ctx->status, ctx->status_h, sizeof(DevStatus));
+}
+
+int cr_get_degraded(const cr_ctx* ctx, int* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  *out = ctx->degraded ? 1 : 0;
   return CR_OK;
 }
 

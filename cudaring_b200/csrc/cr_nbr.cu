@@ -485,12 +485,12 @@ void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g
 // so both paths produce the same list.  The grid never exceeds the CTAs the
 // GPU holds at once (occupancy x SMs, nbr_fused_max_blocks), so every CTA is
 // resident while the others wait.  Every wait is bounded: a barrier that does
-// not complete within about a second (2^20 polls) sets status.stalled and
-// abort, and the CTAs return without finishing the build.
+// not complete within status.spin_limit polls (default 2^20, about a second)
+// sets status.stalled and abort, and the CTAs return without finishing the
+// build.
 
 constexpr int kFusedBlock = 1024;
 constexpr int kFusedMinBlocks = 1;
-constexpr long kBarrierSpins = 1L << 20;
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* a) {
   unsigned int v;
@@ -517,9 +517,10 @@ __device__ bool grid_barrier(DevStatus* st) {
     int ok = 1;
     const unsigned int prev = atom_add_release_u32(&st->bar_count, 1u);
     const unsigned int target = (prev / gridDim.x + 1u) * gridDim.x;
-    long it = 0;
+    const long long lim = barrier_poll_limit(st);
+    long long it = 0;
     while (ld_acquire_u32(&st->bar_count) < target) {
-      if (++it > kBarrierSpins || *(volatile int*)&st->stalled) {
+      if (++it > lim || *(volatile int*)&st->stalled) {
         ok = 0;
         break;
       }

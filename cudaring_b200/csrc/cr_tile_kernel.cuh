@@ -820,9 +820,10 @@ __device__ __forceinline__ bool steps_barrier(DevStatus* st) {
     int ok = 1;
     const unsigned int prev = pst_atom_add_release(&st->pbar, 1u);
     const unsigned int target = (prev / gridDim.x + 1u) * gridDim.x;
-    long it = 0;
+    const long long lim = barrier_poll_limit(st);
+    long long it = 0;
     while (pst_ld_acquire(&st->pbar) < target) {
-      if (++it > (1L << 20) || *(volatile int*)&st->stalled) {
+      if (++it > lim || *(volatile int*)&st->stalled) {
         ok = 0;
         break;
       }

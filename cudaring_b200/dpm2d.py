@@ -360,6 +360,16 @@ class DPM2D:
 
     def setMultistep(self, on): self._call("cr_set_multistep", int(bool(on)))
 
+    def setSpinLimit(self, polls):
+        """Polls a grid-barrier wait makes before giving up (0: the default 2^20)."""
+        self._call("cr_set_spin_limit", C.c_longlong(int(polls)))
+
+    def getDegraded(self):
+        """True once a grid-barrier wait gave up and the context runs one launch per op."""
+        out = C.c_int()
+        self._call("cr_get_degraded", C.byref(out))
+        return bool(out.value)
+
     def setPrecision(self, precision):
         """"fp64" (default, the reference's arithmetic) or "mixed" (FP32 pair
         terms on FP64-formed offsets; everything else FP64)."""

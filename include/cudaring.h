@@ -331,11 +331,20 @@ int cr_set_use_graphs(cr_ctx* ctx, int on);
  * grid barriers between steps) when the GPU holds all of its CTAs at once
  * and one or two lanes per vertex are in use; 0: one launch per step.  FP64
  * results are identical; mixed-precision results agree to FP32 rounding.
- * The kernel's grid barriers need all of its CTAs resident: with other work
- * running on the same GPU at the same time, a barrier may give up after
- * about a second and the call returns CR_ECUDA; such contexts should set 0
- * (the one-launch neighbour-list build has the same requirement). */
+ * The kernel's grid barriers need all of its CTAs resident (so does the
+ * one-launch neighbour-list build).  With other work running on the same
+ * GPU a barrier may give up (cr_set_spin_limit); the context then goes back
+ * to the state the call started from, switches to one launch per op with the
+ * multi-kernel list build for the rest of its life, and runs the call again
+ * (cr_get_degraded reports it). */
 int cr_set_multistep(cr_ctx* ctx, int on);
+/* No reference counterpart.  Polls a grid-barrier wait makes before giving
+ * up (default 2^20, about a second; 0 restores the default).  For GPUs shared
+ * with other work and for tests of the fallback above. */
+int cr_set_spin_limit(cr_ctx* ctx, long long polls);
+/* No reference counterpart.  *out = 1 once a grid-barrier wait of this
+ * context gave up and it runs one launch per op. */
+int cr_get_degraded(const cr_ctx* ctx, int* out);
 /* Times the fused step kernel for every lane count whose tile holds the
  * largest ring (cr_profile_step_kernel, `reps` launches each) and keeps the
  * fastest; reports the choice.  Needs a neighbour list. */
