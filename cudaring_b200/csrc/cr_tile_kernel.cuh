@@ -210,6 +210,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
   __shared__ double2 s_seg[TV];     // pbc(pos[next] - pos[v])
   __shared__ double s_theta[TV];
   __shared__ double s_l0[TV];       // rest length of segment v -> next(v)
+  __shared__ double s_il0[TV];      // its reciprocal
   __shared__ double s_th0[TV];      // rest angle at v
   __shared__ double s_r0[TV];       // shoelace terms -> ring area
   __shared__ double s_r1[TV];       // segment lengths -> perimeter
@@ -253,7 +254,9 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
     }
     const int2 tp = __ldg(a.vtopo + v);
     s_pos[t] = ld_pos<PERSIST>(pin + v);
-    s_l0[t] = __ldg(a.l0 + v);
+    const double l0v = __ldg(a.l0 + v);
+    s_l0[t] = l0v;
+    s_il0[t] = 1.0 / l0v;
     s_th0[t] = __ldg(a.theta0 + v);
     ring = tp.x;
     k = tp.y & 0xffff;
@@ -302,9 +305,13 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
   double2 fsh = make_double2(0.0, 0.0);
   double esh = 0.0;
   if (t < nvt) {
+    // The reference's divisions are taken as products with a few
+    // reciprocals (1/A0, 1/l0 and the segments' 1/l from one rsqrt each),
+    // a rounding-level difference
     const double area = fabs(s_r0[lf]) * 0.5;
-    const double dA = (area / a0r) - 1.0;
-    const double gmA = p.ea * dA / a0r;
+    const double inv_a0 = 1.0 / a0r;
+    const double dA = area * inv_a0 - 1.0;
+    const double gmA = p.ea * dA * inv_a0;
     const double2 ns = s_seg[t];
     const double2 ps = s_seg[lp];
     // nRel - pRel = pos[next] - pos[prev]
@@ -312,13 +319,17 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
     fsh.x += 0.5 * gmA * (-npd.y);
     fsh.y += 0.5 * gmA * (npd.x);
     esh += (0.5 * p.ea * dA * dA) / nvr;
-    const double plen = dist_of(ps), nlen = dist_of(ns);
+    const double ps2 = fma(ps.y, ps.y, ps.x * ps.x), ns2 = fma(ns.y, ns.y, ns.x * ns.x);
+    const double r_pl = rsqrt(ps2), r_nl = rsqrt(ns2);  // 1 / |segment|
+    const double plen = ps2 * r_pl, nlen = ns2 * r_nl;
     const double tl0 = s_l0[t], pl0 = s_l0[lp];
     if (p.monomer == 0) {
-      const double pd = (plen / pl0) - 1.0;
-      const double nd = (nlen / tl0) - 1.0;
-      fsh.x += p.el * ((nd * ns.x / (tl0 * nlen)) - (pd * ps.x / (pl0 * plen)));
-      fsh.y += p.el * ((nd * ns.y / (tl0 * nlen)) - (pd * ps.y / (pl0 * plen)));
+      const double inv_tl0 = s_il0[t], inv_pl0 = s_il0[lp];
+      const double pd = plen * inv_pl0 - 1.0;
+      const double nd = nlen * inv_tl0 - 1.0;
+      const double cn = nd * inv_tl0 * r_nl, cp = pd * inv_pl0 * r_pl;
+      fsh.x += p.el * (cn * ns.x - cp * ps.x);
+      fsh.y += p.el * (cn * ns.y - cp * ps.y);
       esh += 0.5 * p.el * pd * pd;
     } else {
       const double c = 2.0 * p.el * p.stiff * p.ext_sq;
@@ -331,8 +342,8 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
     const double prevAD = s_theta[lp] - s_th0[lp];
     const double thisAD = s_theta[t] - s_th0[t];
     const double nextAD = s_theta[ln] - s_th0[ln];
-    const double pvar = (thisAD - prevAD) / (ps.x * ps.x + ps.y * ps.y);
-    const double nvar = (thisAD - nextAD) / (ns.x * ns.x + ns.y * ns.y);
+    const double pvar = (thisAD - prevAD) * (r_pl * r_pl);
+    const double nvar = (thisAD - nextAD) * (r_nl * r_nl);
     fsh.x += p.eb * (pvar * ps.y + nvar * ns.y);
     fsh.y += p.eb * (pvar * (-ps.x) + nvar * (-ns.x));
     esh += 0.5 * p.eb * thisAD * thisAD;
