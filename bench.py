@@ -51,6 +51,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "vertex-steps/s at 1 B200: mixed vs plain FP64 at <=1e-6 force err; HBM GB/s frac"
+FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (vector), nominal
 UNIT = "vertex-steps/s"
 STATE = os.path.join(ROOT, "bench_state", "smooth_lj_1024.npz")
 
@@ -80,6 +81,8 @@ def parse(argv=None):
                     help="only time the fused step kernel (few launches; for ncu captures)")
     ap.add_argument("--profile-build", action="store_true",
                     help="only run full neighbour-list builds of the prepared state (for ncu captures)")
+    ap.add_argument("--profile-tiles", type=int, default=1,
+                    help="with --profile-kernel: profile k x k periodic copies of the packing")
     ap.add_argument("--lanes", type=int, default=0, help="lanes per vertex of the fused kernel (0: library default)")
     ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
                     help="arithmetic of the headline run (the other one is timed for comparison)")
@@ -403,6 +406,14 @@ def main():
         close_group(world)
         return 0
     if args.profile_kernel:
+        if args.profile_tiles > 1:
+            big = workloads.tile_system(d, args.profile_tiles, c)
+            d.close()
+            d = big
+            nv = d.numVertices
+            if args.lanes:
+                d.setLanes(args.lanes)
+            lanes = d.getLanes()
         d.setPrecision(args.precision)
         ms = d.profileStepKernel(3)
         print(json.dumps({"profile_kernel_ms": ms, "vertices": nv, "lanes": lanes,
@@ -515,6 +526,13 @@ def main():
     achieved = bytes_per_step / step_s / 1e9
     traffic = committed_traffic(prim)
     iso = bytes_per_step / (ms_launch * 1e-3) / 1e9
+    # secondary roof: the FP64 pipe.  Flop model of one step: ~120 flops per
+    # vertex for the shape terms and ~35 per listed pair and role (two smooth
+    # units per list entry), over B200's nominal FP64 rate
+    d.setVertexPositions(x0)
+    d.calcNeighborList(cut)
+    pairs = float(d.getMaxNeighborList().sum())
+    flops_per_step = 120.0 * nv + 2 * 35.0 * pairs
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                 "traffic": traffic.get("bytes_per_launch") if traffic else None,
@@ -522,7 +540,13 @@ def main():
                 "us_per_step": step_s * 1e6, "algorithmic_bytes_per_step": bytes_per_step,
                 "traffic_note": "DRAM bytes of one single-step launch of the same step body (ncu, cold L2)",
                 "single_step_kernel": {"kernel": f"k_tile<LJ, smooth, step, {prim}>", "ms_per_launch": ms_launch,
-                                       "achieved": iso, "frac": iso / peaks["hbm_gbs"]}}
+                                       "achieved": iso, "frac": iso / peaks["hbm_gbs"]},
+                "secondary": {"bound": "fp64 pipe", "unit": "TFLOP/s",
+                              "flops_per_step_model": flops_per_step,
+                              "achieved": flops_per_step / step_s / 1e12, "peak": FP64_NOMINAL_TFLOPS,
+                              "peak_source": "nominal (B200 FP64, not measured on this pool)",
+                              "frac": flops_per_step / step_s / 1e12 / FP64_NOMINAL_TFLOPS,
+                              "ncu_fp64_pipe_active_pct": traffic.get("fp64_pipe_active_pct") if traffic else None}}
 
     comparison = None
     if not args.no_compare:
