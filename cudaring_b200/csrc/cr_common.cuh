@@ -226,13 +226,15 @@ struct DevStatus {
   int pflag[3];
   long long pbase;
   long long steps_left;
-  // polls a grid-barrier wait makes before it gives up (0: 2^20, about a second)
+  // polls a grid-barrier wait makes before it gives up (0: 2^20, about a
+  // second; negative: none, the first poll that finds the barrier incomplete
+  // gives up)
   long long spin_limit;
 };
 
 __device__ __forceinline__ long long barrier_poll_limit(const DevStatus* st) {
   const long long lim = *(const volatile long long*)&st->spin_limit;
-  return lim > 0 ? lim : (1LL << 20);
+  return lim > 0 ? lim : (lim == 0 ? (1LL << 20) : 0);
 }
 
 }  // namespace cr

@@ -93,6 +93,12 @@ struct cr_ctx {
   int *cell_of = nullptr, *slot = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cell_vid = nullptr,
       *cell_ring = nullptr, *cell_pq = nullptr;
   int* block_sum = nullptr;  // per-CTA totals of the one-launch build
+  // cell buckets of the one-launch build, kCellBucket members per cell (ids,
+  // positions, radii, rings, packed offsets); cell_cnt then holds two count
+  // arrays of ncells_alloc entries and two control words
+  int *cell_bucket = nullptr, *bucket_ring = nullptr, *bucket_pq = nullptr;
+  double2* bucket_pos = nullptr;
+  double* bucket_rad = nullptr;
   int fused_max = 0;         // CTAs of the one-launch build resident at once
   double2* cell_pos = nullptr;
   double* cell_rad = nullptr;
@@ -188,6 +194,11 @@ void enter_degraded(cr_ctx* ctx) {
   ctx->multistep = false;
   ctx->use_graphs = false;
   drop_graphs(ctx);
+  // the build that gave up left its cell counts part-done: every count back
+  // to zero, the first array current (the particle-list build still uses
+  // the bucket form)
+  if (ctx->cell_cnt && ctx->ncells_alloc > 0)
+    cudaMemsetAsync(ctx->cell_cnt, 0, cell_count_words(ctx->ncells_alloc) * sizeof(int), ctx->stream);
 }
 
 void refresh_params(cr_ctx* ctx) {
@@ -281,6 +292,32 @@ int ensure_partials(cr_ctx* ctx) {
 }
 
 // Cell grid for the current box, radii and cutDistance (see cr_nbr.cu).
+// Cell scratch for grids of up to `ncells` cells (vertex and particle grids
+// share it): counts in the bucket form's layout (zeroed, the first array
+// current), starts and buckets.
+int alloc_cells(cr_ctx* ctx, int ncells) {
+  if (ncells <= ctx->ncells_alloc) return CR_OK;
+  drop_graphs(ctx);
+  int rc;
+  if ((rc = dalloc(ctx, &ctx->cell_cnt, cell_count_words(ncells)))) return rc;
+  if ((rc = dalloc(ctx, &ctx->cell_start, ncells + 1))) return rc;
+  const size_t nb = (size_t)ncells * kCellBucket;
+  if ((rc = dalloc(ctx, &ctx->cell_bucket, nb)) || (rc = dalloc(ctx, &ctx->bucket_pos, nb)) ||
+      (rc = dalloc(ctx, &ctx->bucket_rad, nb)) || (rc = dalloc(ctx, &ctx->bucket_ring, nb)) ||
+      (rc = dalloc(ctx, &ctx->bucket_pq, nb)))
+    return rc;
+  ctx->ncells_alloc = ncells;
+  return CR_OK;
+}
+
+// Every cell count zero and the first array current: after a build that
+// stopped part-way (a grid-barrier wait gave up), whose counts are unknown.
+int reset_cell_counts(cr_ctx* ctx) {
+  if (ctx->cell_cnt && ctx->ncells_alloc > 0)
+    CR_TRY(cudaMemsetAsync(ctx->cell_cnt, 0, cell_count_words(ctx->ncells_alloc) * sizeof(int), ctx->stream));
+  return CR_OK;
+}
+
 int setup_grid(cr_ctx* ctx, double cut) {
   const double cmin = (1.0 + cut) * 2.0 * ctx->rmax * (1.0 + 1e-9);
   int ncx = cmin > 0 ? (int)std::floor(ctx->p.lx / cmin) : 0;
@@ -291,12 +328,13 @@ int setup_grid(cr_ctx* ctx, double cut) {
     ctx->grid = CellGrid{0, 0, 0.0, 0.0};
     return CR_OK;
   }
-  // The build's stencil phase deals home cells to its warps in rounds; a last
-  // round that only a few warps take costs a whole round.  When the build
-  // fills the GPU and there are more cells than warps, coarsen the grid
-  // (larger cells hold every pair the smaller ones did) to a whole number of
-  // rounds: the lists hold the same neighbours, in the order of the coarser
-  // cells.  Smaller systems keep the finest grid.
+  // The sorted-cell stencil search (the multi-kernel build, and the one-launch
+  // build when a cell overflows its bucket) deals home cells to its warps in
+  // rounds; a last round that only a few warps take costs a whole round.
+  // When the build fills the GPU and there are more cells than warps, coarsen
+  // the grid (larger cells hold every pair the smaller ones did) to a whole
+  // number of rounds: the lists hold the same neighbours, in the order of the
+  // coarser cells.  Smaller systems keep the finest grid.
   {
     const int blocks = nbr_fused_blocks(ctx->nv, ctx->fused_max);
     const long warps = (long)blocks * 32;
@@ -312,14 +350,7 @@ int setup_grid(cr_ctx* ctx, double cut) {
   }
   ctx->grid = CellGrid{ncx, ncy, ctx->p.lx / ncx, ctx->p.ly / ncy};
   const int ncells = ncx * ncy;
-  if (ncells > ctx->ncells_alloc) {
-    drop_graphs(ctx);
-    int rc;
-    if ((rc = dalloc(ctx, &ctx->cell_cnt, ncells))) return rc;
-    if ((rc = dalloc(ctx, &ctx->cell_start, ncells + 1))) return rc;
-    ctx->ncells_alloc = ncells;
-  }
-  return CR_OK;
+  return alloc_cells(ctx, ncells);
 }
 
 NbrArgs nbr_args(cr_ctx* ctx, int buf, double cut) {
@@ -347,6 +378,12 @@ NbrArgs nbr_args(cr_ctx* ctx, int buf, double cut) {
   n.count_op = 0;
   n.count_update = 0;
   n.block_sum = ctx->block_sum;
+  n.bucket = ctx->cell_bucket;
+  n.bucket_pos = ctx->bucket_pos;
+  n.bucket_rad = ctx->bucket_rad;
+  n.bucket_ring = ctx->bucket_ring;
+  n.bucket_pq = ctx->bucket_pq;
+  n.cell_stride = ctx->ncells_alloc;
   return n;
 }
 
@@ -1059,7 +1096,8 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
                   ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec, ctx->diff_area, ctx->cg_state,
                   ctx->cg_part,
-                  ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum,
+                  ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum, ctx->cell_bucket, ctx->bucket_pos, ctx->bucket_rad,
+                  ctx->bucket_ring, ctx->bucket_pq,
                   ctx->prad, ctx->plast, ctx->pid, ctx->pnbr, ctx->pnbr_cnt, ctx->pstatus, ctx->pfire, ctx->pdraws,
                   ctx->snap_pos, ctx->snap_vel, ctx->snap_force, ctx->snap_last, ctx->snap_angle};
   for (void* p : ptrs)
@@ -1966,7 +2004,7 @@ int cr_set_multistep(cr_ctx* ctx, int on) {
 }
 
 int cr_set_spin_limit(cr_ctx* ctx, long long polls) {
-  if (!ctx || polls < 0) return CR_EINVAL;
+  if (!ctx) return CR_EINVAL;
   int rc = read_status(ctx);
   if (rc) return rc;
   ctx->status_h->spin_limit = polls;
@@ -2299,6 +2337,12 @@ static NbrArgs soft_nbr_args(cr_ctx* ctx, double cut) {
   n.count_op = 0;
   n.count_update = 0;
   n.block_sum = ctx->block_sum;
+  n.bucket = ctx->cell_bucket;
+  n.bucket_pos = ctx->bucket_pos;
+  n.bucket_rad = ctx->bucket_rad;
+  n.bucket_ring = ctx->bucket_ring;
+  n.bucket_pq = ctx->bucket_pq;
+  n.cell_stride = ctx->ncells_alloc;
   n.self_rsum = 1;
   return n;
 }
@@ -2316,13 +2360,7 @@ static int soft_setup_grid(cr_ctx* ctx, double cut) {
     return CR_OK;
   }
   ctx->pgrid = CellGrid{ncx, ncy, ctx->p.lx / ncx, ctx->p.ly / ncy};
-  if (ncx * ncy > ctx->ncells_alloc) {
-    drop_graphs(ctx);
-    if ((rc = dalloc(ctx, &ctx->cell_cnt, ncx * ncy))) return rc;
-    if ((rc = dalloc(ctx, &ctx->cell_start, ncx * ncy + 1))) return rc;
-    ctx->ncells_alloc = ncx * ncy;
-  }
-  return CR_OK;
+  return alloc_cells(ctx, ncx * ncy);
 }
 
 // DPM2D::calcParticleNeighborList (DPM2D.cu:3521-3545): the list size only
@@ -2338,7 +2376,10 @@ static int soft_build(cr_ctx* ctx, double cut) {
     CR_TRY(cudaGetLastError());
     DevStatus st;
     if ((rc = soft_read_status(ctx, &st))) return rc;
-    if (st.stalled) return ctx->fail(CR_ECUDA, "particle list build: a grid barrier timed out");
+    if (st.stalled) {
+      reset_cell_counts(ctx);
+      return ctx->fail(CR_ECUDA, "particle list build: a grid barrier timed out");
+    }
     if (!st.overflow) {
       if (st.max_count > 0) ctx->plist_size_ref = std::max<long long>(ctx->plist_size_ref, pow2ceil(st.max_count));
       ctx->pnbr_built = true;

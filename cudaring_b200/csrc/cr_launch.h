@@ -129,6 +129,11 @@ void launch_extract_hv(cudaStream_t st, int nv, const double* fhd, double* hv);
 void launch_sub_mean(cudaStream_t st, int nv, double* x, double mx, double my);
 
 // cr_nbr.cu
+// Vertex ids a cell bucket of the one-launch build holds; a build that finds
+// a fuller cell sorts by cell instead (same list).
+constexpr int kCellBucket = 16;
+// ints of the cell_cnt allocation for the bucket form over `ncells` cells
+inline size_t cell_count_words(int ncells) { return 2 * (size_t)ncells + 2; }
 struct CellGrid {
   int ncx, ncy;       // cells per dimension (>= 3 each), or 0 for brute force
   double cx, cy;      // cell sizes
@@ -160,6 +165,16 @@ struct NbrArgs {
   int count_op;       // 1: the build is one op of a step sequence (ops_done += 1)
   int count_update;   // 1: a displacement-triggered rebuild (DPM2D::updateCount += 1)
   int* block_sum = nullptr;  // [grid] per-CTA cell totals of the one-launch build
+  // bucket form of the one-launch build (all set, or bucket null): cell_cnt
+  // then holds two count arrays of cell_stride entries and two control words
+  // (which array is current, and whether a cell overflowed its bucket); each
+  // cell's bucket holds up to kCellBucket members, with their data
+  int* bucket = nullptr;           // [ncells][kCellBucket] vertex ids
+  double2* bucket_pos = nullptr;   // positions
+  double* bucket_rad = nullptr;    // radii
+  int* bucket_ring = nullptr;      // rings
+  int* bucket_pq = nullptr;        // packed ring-predecessor offsets (with nbr_pq)
+  int cell_stride = 0;
   // 1: the pair's radius sum is twice the listing vertex's own radius (the
   // particle list rule of kernelCalcParticleNeighborList, whose
   // extractOtherParticle returns the particle's own radius,

@@ -27,6 +27,10 @@
 
 namespace cr {
 
+// CTA size of the one-launch build (one CTA per SM)
+constexpr int kFusedBlock = 1024;
+constexpr int kFusedMinBlocks = 1;
+
 __device__ __forceinline__ int cell_coord(double x, double L, double invL, int nc) {
   double w = x - L * floor(x * invL);          // wrap into [0, L]
   int c = (int)(w * (nc * invL));
@@ -165,13 +169,22 @@ __device__ __forceinline__ bool is_neighbor(const SysParams& p, double2 xi, doub
   return pt >= 0 ? pt == 1 : exact_test(sq, rsum, cut);
 }
 
-__device__ __forceinline__ void publish_build(const NbrArgs& n, int my_max, int my_overflow) {
+// ctl (bucket form of the one-launch build): the control words after the two
+// count arrays; the last CTA makes the other array current when this build
+// left counts in the current one (bucket_pass), and clears the bucket
+// overflow word.
+__device__ __forceinline__ void publish_build(const NbrArgs& n, int my_max, int my_overflow, int* ctl = nullptr,
+                                              bool bucket_pass = false) {
   DevStatus* st = n.status;
   if (my_overflow) atomicOr(&st->overflow, 1);
   if (my_max > 0) atomicMax(&st->max_count, my_max);
   if (is_last_block(st)) {
     if (threadIdx.x == 0) {
       __threadfence();
+      if (ctl) {
+        if (bucket_pass) ctl[0] ^= 1;
+        ctl[1] = 0;
+      }
       if (st->max_count > st->max_ever) st->max_ever = st->max_count;
       if (st->abort) {
         // an earlier op of this sequence failed; leave its state alone
@@ -384,6 +397,228 @@ __device__ __forceinline__ int stencil_cell(const SysParams& p, int ncx, int ncy
   return maxc;
 }
 
+// Bucket form of the stencil search.  The home cells are dealt to the CTAs
+// in square tiles of T x T cells (T from the host: the smallest tile whose
+// count fits the grid, up to kStageTileMax).  A CTA stages its tile's cells
+// and their one-cell halo from the buckets into shared memory (cp.async,
+// every bucket slot and the counts), then converts: ids, rings, packed
+// offsets, radii in single precision and positions in single precision
+// relative to the tile's corner, each shifted by the box lengths its staged
+// cell was wrapped by (its minimum image whenever it lies within range of a
+// home vertex).  Every staged row of cells becomes one list, cell after cell
+// and ascending id inside a cell (bucket slots come in atomic order), so the
+// three stencil cells of a home vertex on one row are one contiguous run in
+// the sequential scan's order.  Three threads per home vertex, one per row
+// (dy = row - 1), ten vertices per warp (lanes 30 and 31 idle): pass 1 tests
+// the row's run with the single-precision pre-test of the sorted-cell search
+// (PreTest, here over T + 2 cells) and, inside its rounding band, with the
+// reference expression on the double positions (band_test), one bit per
+// hit; the rows' hit counts give each row its first slot (row 0 first);
+// pass 2 writes the hits in run order.  The list is the sorted-cell search's,
+// entry for entry.  Returns the largest count among the vertices this thread
+// completed.
+constexpr int kStageTileMax = 12;
+constexpr size_t kStageEntryBytes =
+    sizeof(double2) + sizeof(double) + sizeof(float2) + sizeof(float) + 4 * sizeof(int);
+__host__ __device__ constexpr size_t bucket_stage_bytes(int t) {
+  return (size_t)(t + 2) * (t + 2) * kCellBucket * kStageEntryBytes + (size_t)(t + 2) * (t + 2) * sizeof(int) +
+         (size_t)(t + 2) * (t + 3) * sizeof(int) + ((size_t)t * t + 1) * sizeof(int);
+}
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// staged cell sl of a tile with corner (ox, oy): its grid cell and the
+// number of box lengths it was wrapped by along x and y
+template <int SW>
+__device__ __forceinline__ int staged_cell(int sl, int ox, int oy, int ncx, int ncy, int& wx, int& wy) {
+  const int ux = ox - 1 + sl % SW, uy = oy - 1 + sl / SW;  // unwrapped cell
+  wx = ux < 0 ? -1 : (ux < ncx ? 0 : ux / ncx);
+  wy = uy < 0 ? -1 : (uy < ncy ? 0 : uy / ncy);
+  return (uy - wy * ncy) * ncx + (ux - wx * ncx);
+}
+
+// Inside the pre-test's rounding band: the reference expression on the
+// double positions of home vertex v and candidate c.  Out of line, so the
+// candidate loop branches over it instead of carrying it on every pass.
+__device__ __noinline__ int band_test(const SysParams& p, const NbrArgs& n, int v, int c) {
+  const double rv = n.rad[v];
+  return is_neighbor(p, n.pos[v], n.pos[c], rv + (n.self_rsum ? rv : n.rad[c]), n.cut_distance) ? 1 : 0;
+}
+
+template <int T>
+__device__ __forceinline__ int bucket_tiles(const SysParams& p, int ncx, int ncy, const NbrArgs& n, const int* cnt,
+                                            unsigned char* smem) {
+  constexpr unsigned kAll = 0xffffffffu;
+  constexpr int SW = T + 2, S = SW * SW, E = S * kCellBucket, H = T * T, RL = SW * kCellBucket;
+  double2* s_rpos = reinterpret_cast<double2*>(smem);  // bucket copies as stored
+  double* s_rrad = reinterpret_cast<double*>(s_rpos + E);
+  float2* s_xf = reinterpret_cast<float2*>(s_rrad + E);
+  float* s_rf = reinterpret_cast<float*>(s_xf + E);
+  int* s_ring = reinterpret_cast<int*>(s_rf + E);
+  int* s_id = s_ring + E;
+  int* s_pq = s_id + E;
+  int* s_row = s_pq + E;     // [SW][RL]: staged entries of each row of cells, in scan order
+  int* s_cnt = s_row + E;    // [S]
+  int* s_roff = s_cnt + S;   // [SW][SW + 1]: first run position of each cell in its row
+  int* s_pref = s_roff + SW * (SW + 1);  // [H + 1]: exclusive prefix of the home cells' counts
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int row = lane % 3, grp = lane - row;  // lanes grp .. grp + 2 share a home vertex
+  const int ntx = (ncx + T - 1) / T, nty = (ncy + T - 1) / T;
+  const double cw = p.lx / ncx, ch = p.ly / ncy;
+  // rounding of a staged coordinate (at most T + 2 cells from the corner)
+  const float e = (float)((T + 2) * fmax(cw, ch) * 0x1p-22);
+  const float e4 = 4.0f * e, ee4 = 4.0f * e * e;
+  const float opc = (float)(1.0 + n.cut_distance);
+  const bool pre_on = n.cut_distance > -0.5;
+  int maxc = 0;
+  for (int tile = blockIdx.x; tile < ntx * nty; tile += gridDim.x) {
+    const int ox = (tile % ntx) * T, oy = (tile / ntx) * T;
+    const int hxn = min(T, ncx - ox), hyn = min(T, ncy - oy);
+    const double cox = ox * cw, coy = oy * ch;
+    __syncthreads();  // the previous tile's readers are done with the stage
+    // every bucket slot and count of the staged cells, copied asynchronously
+    for (int i = threadIdx.x; i < E; i += kFusedBlock) {
+      const int sl = i / kCellBucket, el = i % kCellBucket;
+      int wx, wy;
+      const int cell = staged_cell<SW>(sl, ox, oy, ncx, ncy, wx, wy);
+      const size_t k = (size_t)cell * kCellBucket + el;
+      if (el == 0) cp_async4(s_cnt + sl, cnt + cell);
+      cp_async16(s_rpos + i, n.bucket_pos + k);
+      cp_async8(s_rrad + i, n.bucket_rad + k);
+      cp_async4(s_ring + i, n.bucket_ring + k);
+      cp_async4(s_id + i, n.bucket + k);
+      if (n.nbr_pq) cp_async4(s_pq + i, n.bucket_pq + k);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    if (warp < SW) {
+      // run offsets of the cells of staged row `warp`
+      const int c = lane < SW ? s_cnt[warp * SW + lane] : 0;
+      int incl = c;
+      for (int o = 1; o < 16; o <<= 1) {
+        const int y = __shfl_up_sync(kAll, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane < SW) s_roff[warp * (SW + 1) + lane] = incl - c;
+      if (lane == SW - 1) s_roff[warp * (SW + 1) + SW] = incl;
+    } else if (warp == 31) {
+      // exclusive prefix of the home cells' counts, tile row-major (cells
+      // past the grid's edge hold none); s_pref[H] = home vertices of the tile
+      constexpr int per = (H + 31) / 32;
+      const int hb = min(H, lane * per), he = min(H, hb + per);
+      int loc = 0;
+      for (int h = hb; h < he; h++)
+        loc += (h % T < hxn && h / T < hyn) ? s_cnt[(h / T + 1) * SW + h % T + 1] : 0;
+      int incl = loc;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kAll, incl, o);
+        if (lane >= o) incl += y;
+      }
+      int run = incl - loc;
+      for (int h = hb; h < he; h++) {
+        s_pref[h] = run;
+        run += (h % T < hxn && h / T < hyn) ? s_cnt[(h / T + 1) * SW + h % T + 1] : 0;
+      }
+      if (lane == 31) s_pref[H] = incl;
+    }
+    __syncthreads();
+    // single-precision positions relative to the tile's corner, in the
+    // staged cell's image; each entry to its place in its row's run
+    for (int i = threadIdx.x; i < E; i += kFusedBlock) {
+      const int sl = i / kCellBucket, el = i % kCellBucket, c = s_cnt[sl];
+      if (el < c) {
+        int wx, wy;
+        staged_cell<SW>(sl, ox, oy, ncx, ncy, wx, wy);
+        const double2 x = s_rpos[i];
+        const double xw = x.x - p.lx * floor(x.x * p.inv_lx) + wx * p.lx;
+        const double yw = x.y - p.ly * floor(x.y * p.inv_ly) + wy * p.ly;
+        s_xf[i] = make_float2((float)(xw - cox), (float)(yw - coy));
+        s_rf[i] = (float)s_rrad[i];
+        const int id = s_id[i];
+        int r = 0;
+        for (int k = 0; k < c; k++) r += s_id[sl * kCellBucket + k] < id ? 1 : 0;
+        const int y = sl / SW, x_ = sl % SW;
+        s_row[y * RL + s_roff[y * (SW + 1) + x_] + r] = i;
+      }
+    }
+    __syncthreads();
+    const int nhome = s_pref[H];
+    for (int m0 = 0; m0 < nhome; m0 += 10 * (kFusedBlock / 32)) {
+      const int m = m0 + warp * 10 + lane / 3;
+      const bool live = lane < 30 && m < nhome;
+      unsigned long long hit = 0ull;
+      int hq = 0, rb = 0;  // home entry; first run position of the row's three cells
+      if (live) {
+        // home cell: the last h with s_pref[h] <= m; the home vertex is its
+        // member of rank m - s_pref[h]
+        int lo = 0, hi = H - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (s_pref[mid] <= m) lo = mid;
+          else hi = mid - 1;
+        }
+        const int hx = lo % T, hy = lo / T;
+        hq = s_row[(hy + 1) * RL + s_roff[(hy + 1) * (SW + 1) + hx + 1] + (m - s_pref[lo])];
+        const int y = hy + row;
+        rb = y * RL + s_roff[y * (SW + 1) + hx];
+        const int re = y * RL + s_roff[y * (SW + 1) + hx + 3];
+        const float2 xh = s_xf[hq];
+        const float rh = s_rf[hq];
+        const int ringh = s_ring[hq];
+        for (int q = rb; q < re; q++) {
+          const int c = s_row[q];
+          const float2 xc = s_xf[c];
+          const float ddx = xc.x - xh.x, ddy = xc.y - xh.y;
+          const float sq = fmaf(ddy, ddy, ddx * ddx);
+          const float t = (rh + (n.self_rsum ? rh : s_rf[c])) * opc;
+          const float t2 = t * t;
+          const float mg = fmaf(1e-5f, t2, fmaf(e4, t, ee4));
+          int d = !pre_on ? -1 : (sq < t2 - mg ? 1 : (sq > t2 + mg ? 0 : -1));
+          if (d < 0) d = band_test(p, n, s_id[hq], s_id[c]);
+          if (d && s_ring[c] != ringh) hit |= 1ull << (q - rb);
+        }
+      }
+      const int nh = __popcll(hit);
+      const int h0 = __shfl_sync(kAll, nh, grp), h1 = __shfl_sync(kAll, nh, grp + 1),
+                h2 = __shfl_sync(kAll, nh, grp + 2);
+      if (live) {
+        const int v = s_id[hq];
+        int slot = row == 0 ? 0 : (row == 1 ? h0 : h0 + h1);
+        for (unsigned long long r = hit; r; r &= r - 1ull) {
+          const int c = s_row[rb + __ffsll((long long)r) - 1];
+          if (slot < n.cap) {
+            n.nbr[(size_t)slot * p.nv + v] = s_id[c];
+            if (n.nbr_pq) n.nbr_pq[(size_t)slot * p.nv + v] = s_pq[c];
+          }
+          slot++;
+        }
+        if (row == 0) {
+          const int tot = h0 + h1 + h2;
+          n.nbr_cnt[v] = tot;
+          n.last_pos[v] = n.pos[v];
+          maxc = max(maxc, tot);
+        }
+      }
+    }
+  }
+  return maxc;
+}
+
 // CTA-wide maximum of m (every thread calls it); the result on thread 0.
 __device__ __forceinline__ int block_max(int m) {
   for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -469,28 +704,31 @@ void launch_nbr_build(cudaStream_t stream, const SysParams& p, const CellGrid& g
 
 // ------------------------------------------------------- one-launch build
 //
-// The phases above in one launch, for step sequences captured in graphs: the
-// kernel follows every op that may arm a rebuild and returns at once unless
-// the op armed one, so a step that needs no rebuild pays one early-exit launch
-// instead of a conditional graph node.  When armed, the phases run back to
-// back with grid-wide barriers between them:
-//   1 cell + slot of every vertex             (k_cell_count)
-//   2 per-CTA totals of a contiguous cell range
-//   3 exclusive scan: CTA offset from the totals, then the range (k_cell_scan)
-//   4 scatter ids by cell                     (k_cell_fill)
-//   5 per vertex: rank in its cell by id, copy to that entry
-//                                             (k_cell_sort + k_cell_gather)
-//   6 stencil search, one warp per home cell  (k_nbr_cells)
+// The build in one launch, for step sequences captured in graphs: the kernel
+// follows every op that may arm a rebuild and returns at once unless the op
+// armed one, so a step that needs no rebuild pays one early-exit launch
+// instead of a conditional graph node.  When armed:
+//   1 cell + slot of every vertex (atomic count, as k_cell_count); with
+//     buckets, the vertex and its data also go to its cell's bucket slot,
+//     and the other count array is cleared for the next build
+//   -- grid barrier --
+//   2 every cell within its bucket: the tiled search on the buckets
+//     (bucket_tiles), then publish.  Otherwise the sorted-cell form:
+//   2' per-CTA totals of a contiguous cell range
+//   3' exclusive scan: CTA offset from the totals, then the range (k_cell_scan)
+//   4' scatter ids by cell                     (k_cell_fill)
+//   5' per vertex: rank in its cell by id, copy to that entry
+//                                              (k_cell_sort + k_cell_gather)
+//   6' stencil search, one warp per home cell  (k_nbr_cells)
+//     with grid barriers between them,
 // and the last CTA publishes the build exactly as the multi-kernel path does,
-// so both paths produce the same list.  The grid never exceeds the CTAs the
+// so every path produces the same list.  The grid never exceeds the CTAs the
 // GPU holds at once (occupancy x SMs, nbr_fused_max_blocks), so every CTA is
 // resident while the others wait.  Every wait is bounded: a barrier that does
 // not complete within status.spin_limit polls (default 2^20, about a second)
 // sets status.stalled and abort, and the CTAs return without finishing the
 // build.
 
-constexpr int kFusedBlock = 1024;
-constexpr int kFusedMinBlocks = 1;
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* a) {
   unsigned int v;
@@ -563,7 +801,8 @@ __device__ __forceinline__ int block_scan(int x, int* total) {
 }
 
 __global__ void __launch_bounds__(kFusedBlock, kFusedMinBlocks)
-    k_nbr_fused(const __grid_constant__ SysParams p, int ncx, int ncy, const __grid_constant__ NbrArgs n, int force) {
+    k_nbr_fused(const __grid_constant__ SysParams p, int ncx, int ncy, const __grid_constant__ NbrArgs n, int force,
+                int stage_tile) {
   // the status block and positions come from the step kernel before this
   // launch; the next kernel starts when this one exits (no early trigger, so
   // no later grid can take the SMs that the grid barriers need)
@@ -584,25 +823,71 @@ __global__ void __launch_bounds__(kFusedBlock, kFusedMinBlocks)
     return;
   }
   const int ncells = ncx * ncy;
-  // 1: cells and slots (the counts are zero between builds)
+  __shared__ HomeStage s_home[kFusedBlock / 32];
+  // bucket form: this build counts into the current count array and clears
+  // the other one, which the next build counts into
+  const bool dual = n.bucket != nullptr && n.cell_stride > 0;
+  int* ctl = dual ? n.cell_cnt + 2 * (size_t)n.cell_stride : nullptr;
+  const int sel = dual ? *(volatile int*)ctl : 0;
+  int* cnt = n.cell_cnt + (size_t)sel * n.cell_stride;
+  // 1: cells and slots (the current counts are zero between builds)
   if (gt == 0) {
     st->overflow = 0;
     st->max_count = 0;
   }
-  for (int v = gt; v < nv; v += nthreads) {
+  bool full = false;
+  // a contiguous range of vertices per CTA, so every CTA takes a share
+  const int per_cta = (nv + gridDim.x - 1) / gridDim.x;
+  const int vb = min(nv, (int)blockIdx.x * per_cta), ve = min(nv, vb + per_cta);
+  for (int v = vb + threadIdx.x; v < ve; v += kFusedBlock) {
     const double2 x = n.pos[v];
     const int c = cell_coord(x.y, p.ly, p.inv_ly, ncy) * ncx + cell_coord(x.x, p.lx, p.inv_lx, ncx);
     n.cell_of[v] = c;
-    n.slot[v] = atomicAdd(n.cell_cnt + c, 1);
+    const int s = atomicAdd(cnt + c, 1);
+    n.slot[v] = s;
+    if (dual) {
+      if (s < kCellBucket) {
+        const size_t k = (size_t)c * kCellBucket + s;
+        n.bucket[k] = v;
+        n.bucket_pos[k] = x;
+        n.bucket_rad[k] = n.rad[v];
+        n.bucket_ring[k] = n.ring_of[v];
+        if (n.nbr_pq) n.bucket_pq[k] = n.pq_pack[v];
+      } else {
+        full = true;
+      }
+    }
+  }
+  if (dual) {
+    if (full) atomicOr(ctl + 1, 1);
+    int* other = n.cell_cnt + (size_t)(sel ^ 1) * n.cell_stride;
+    for (int i = gt; i < n.cell_stride; i += nthreads) other[i] = 0;
   }
   if (!grid_barrier(st)) return;
-  // 2: this CTA's cells [cb, ce), this thread's [tb, te)
+  if (dual && *(volatile int*)(ctl + 1) == 0) {
+    // 2 (every cell within its bucket): the search on the buckets
+    extern __shared__ __align__(16) unsigned char s_stage[];
+    int m = 0;
+    switch (stage_tile) {
+      case 4: m = bucket_tiles<4>(p, ncx, ncy, n, cnt, s_stage); break;
+      case 6: m = bucket_tiles<6>(p, ncx, ncy, n, cnt, s_stage); break;
+      case 8: m = bucket_tiles<8>(p, ncx, ncy, n, cnt, s_stage); break;
+      case 9: m = bucket_tiles<9>(p, ncx, ncy, n, cnt, s_stage); break;
+      case 10: m = bucket_tiles<10>(p, ncx, ncy, n, cnt, s_stage); break;
+      default: m = bucket_tiles<kStageTileMax>(p, ncx, ncy, n, cnt, s_stage); break;
+    }
+    const int bm = block_max(m);
+    publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap, ctl, true);
+    return;
+  }
+  // 2 (a cell beyond its bucket, or no buckets): sort by cell.  This CTA's
+  // cells [cb, ce), this thread's [tb, te)
   const int per_block = (ncells + gridDim.x - 1) / gridDim.x;
   const int cb = min(ncells, (int)blockIdx.x * per_block), ce = min(ncells, cb + per_block);
   const int per_thread = (ce - cb + kFusedBlock - 1) / kFusedBlock;
   const int tb = min(ce, cb + (int)threadIdx.x * per_thread), te = min(ce, tb + per_thread);
   int sum = 0;
-  for (int c = tb; c < te; c++) sum += n.cell_cnt[c];
+  for (int c = tb; c < te; c++) sum += cnt[c];
   int cta_total = 0;
   const int incl = block_scan(sum, &cta_total);
   if (threadIdx.x == 0) n.block_sum[blockIdx.x] = cta_total;
@@ -614,10 +899,10 @@ __global__ void __launch_bounds__(kFusedBlock, kFusedMinBlocks)
   block_scan(part, &offset);
   int run = offset + incl - sum;
   for (int c = tb; c < te; c++) {
-    const int k = n.cell_cnt[c];
+    const int k = cnt[c];
     n.cell_start[c] = run;
     run += k;
-    n.cell_cnt[c] = 0;
+    cnt[c] = 0;
   }
   if (tb < te && te == ncells) n.cell_start[ncells] = run;
   if (!grid_barrier(st)) return;
@@ -641,19 +926,20 @@ __global__ void __launch_bounds__(kFusedBlock, kFusedMinBlocks)
   }
   if (!grid_barrier(st)) return;
   // 6: stencil search, one warp per home cell
-  __shared__ HomeStage s_home[kFusedBlock / 32];
   int m = 0;
   for (int c = gt / 32; c < ncells; c += nthreads / 32)
     m = max(m, stencil_cell(p, ncx, ncy, n, n.slot, c, gt & 31, s_home[threadIdx.x / 32]));
   const int bm = block_max(m);
-  publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap);
+  publish_build(n, threadIdx.x == 0 ? bm : 0, threadIdx.x == 0 && bm > n.cap, ctl, false);
 }
 
 int nbr_fused_max_blocks() {
   int dev = 0, sms = 0, occ = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_nbr_fused, kFusedBlock, 0) != cudaSuccess) return 0;
+  const int smem = (int)bucket_stage_bytes(kStageTileMax);
+  if (cudaFuncSetAttribute(k_nbr_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_nbr_fused, kFusedBlock, smem) != cudaSuccess) return 0;
   return occ * sms;
 }
 
@@ -662,9 +948,28 @@ int nbr_fused_blocks(int nv, int max_blocks) {
   return (int)std::max(1L, std::min<long>(want, max_blocks));
 }
 
+// Side of the bucket search's tiles: the smallest whose tiles number no more
+// than the CTAs, else the largest the stage allows.
+static int stage_tile(int ncx, int ncy, int blocks) {
+  for (int t : {4, 6, 8, 9, 10})
+    if ((long)((ncx + t - 1) / t) * ((ncy + t - 1) / t) <= blocks) return t;
+  return kStageTileMax;
+}
+
 void launch_nbr_fused(cudaStream_t st, const SysParams& p, const CellGrid& g, const NbrArgs& n, int blocks,
                       int force, bool pdl) {
-  launch_k(pdl, k_nbr_fused, dim3(blocks), dim3(kFusedBlock), st, p, g.ncx, g.ncy, n, force);
+  const int t = stage_tile(g.ncx, g.ncy, blocks);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kFusedBlock);
+  cfg.dynamicSmemBytes = (n.bucket && g.ncx >= 3 && g.ncy >= 3) ? bucket_stage_bytes(t) : 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, k_nbr_fused, p, g.ncx, g.ncy, n, force, t);
 }
 
 }  // namespace cr

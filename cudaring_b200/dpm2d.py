@@ -361,7 +361,8 @@ class DPM2D:
     def setMultistep(self, on): self._call("cr_set_multistep", int(bool(on)))
 
     def setSpinLimit(self, polls):
-        """Polls a grid-barrier wait makes before giving up (0: the default 2^20)."""
+        """Polls a grid-barrier wait makes before giving up (0: the default 2^20;
+        negative: the first poll that finds a barrier incomplete gives up)."""
         self._call("cr_set_spin_limit", C.c_longlong(int(polls)))
 
     def getDegraded(self):

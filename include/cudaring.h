@@ -339,8 +339,10 @@ int cr_set_use_graphs(cr_ctx* ctx, int on);
  * (cr_get_degraded reports it). */
 int cr_set_multistep(cr_ctx* ctx, int on);
 /* No reference counterpart.  Polls a grid-barrier wait makes before giving
- * up (default 2^20, about a second; 0 restores the default).  For GPUs shared
- * with other work and for tests of the fallback above. */
+ * up (default 2^20, about a second; 0 restores the default; a negative
+ * value: the first poll that finds a barrier incomplete gives up, which
+ * every wait but the last CTA's does).  For GPUs shared with other work and
+ * for tests of the fallback above. */
 int cr_set_spin_limit(cr_ctx* ctx, long long polls);
 /* No reference counterpart.  *out = 1 once a grid-barrier wait of this
  * context gave up and it runs one launch per op. */

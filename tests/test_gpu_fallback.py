@@ -3,8 +3,9 @@
 The multi-step kernel and the one-launch neighbour-list build wait on grid
 barriers that need every CTA of their grid resident at once; a GPU shared
 with other work may not hold them all.  Every such wait is bounded
-(cr_set_spin_limit).  Here the bound is one poll, so the waits give up at
-once: the kernels return an error status (nothing hangs), and the context
+(cr_set_spin_limit).  Here the bound is negative, so every wait that does
+not find its barrier complete gives up at once: the kernels return an
+error status (nothing hangs), and the context
 must go back to the state the call started from, switch to one launch per op
 with the multi-kernel list build, and finish the call on the same trajectory
 as a context that never used the barrier kernels.
@@ -46,7 +47,7 @@ def test_stalled_multistep_sequence_reruns_one_launch_per_op(packing):
     ref.setMultistep(0)
     ref.NVELoop(400)
     d, _ = _context(pk, c)
-    d.setSpinLimit(1)
+    d.setSpinLimit(-1)
     d.NVELoop(400)
     assert d.getDegraded()
     assert not ref.getDegraded()
@@ -67,7 +68,7 @@ def test_stalled_list_build_retries_with_the_multi_kernel_build(packing):
     pk, c = packing
     ref, cut = _context(pk, c)
     d, _ = _context(pk, c)
-    d.setSpinLimit(1)
+    d.setSpinLimit(-1)
     d.calcNeighborList(cut)
     assert d.getDegraded()
     assert np.array_equal(d.getMaxNeighborList(), ref.getMaxNeighborList())
