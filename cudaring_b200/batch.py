@@ -156,17 +156,25 @@ class Batch:
         self._call("cr_batch_scale_vertices", _f64(np.broadcast_to(scale, (self.S,))).ctypes.data)
 
     def compress(self, dphi=1e-3, min_dphi=1e-6, fire_dt=1e-2, tol0=1e-10, energy_tol=1e-20, max_fire_iters=100000,
-                 max_steps=1000, criterion="force"):
-        """Quasi-static compression to jamming of every system (cr_batch_compress)."""
+                 max_steps=1000, criterion="force", stepwise=False):
+        """Quasi-static compression to jamming of every system: the whole
+        protocol on the device as one graph launch (cr_batch_compress), or,
+        with stepwise=True, driven from the host between steps and FIRE
+        chunks (cr_batch_compress_stepwise); both give the same states."""
         prm = CompressParams(dphi, min_dphi, fire_dt, tol0, energy_tol, int(max_fire_iters), int(max_steps),
                              {"force": 0, "energy": 1}[criterion])
         phi = np.zeros(self.S)
         steps = np.zeros(self.S, dtype=np.int64)
         state = np.zeros(self.S, dtype=np.int32)
         iters = np.zeros(self.S, dtype=np.int64)
-        self._call("cr_batch_compress", C.byref(prm), phi.ctypes.data, steps.ctypes.data, state.ctypes.data,
-                   iters.ctypes.data)
+        fn = "cr_batch_compress_stepwise" if stepwise else "cr_batch_compress"
+        self._call(fn, C.byref(prm), phi.ctypes.data, steps.ctypes.data, state.ctypes.data, iters.ctypes.data)
         return {"phi": phi, "steps": steps, "state": state, "fire_iterations": iters}
+
+    def getListCapacity(self):
+        out = C.c_int()
+        self._call("cr_batch_get_list_capacity", C.byref(out))
+        return out.value
 
     def getLaunchCount(self):
         out = C.c_longlong()

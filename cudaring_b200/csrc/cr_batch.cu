@@ -30,6 +30,14 @@
 
 using namespace cr;
 
+// Compression protocol state of one system (cr_batch_compress on the device).
+struct CompSys {
+  double phi, prev, dphi;
+  long long steps, fire_total;
+  int state;  // 0 compressing, 1 jammed, 2 step limit, 3 step halved below min_dphi
+  int pad;
+};
+
 struct cr_batch {
   int device = 0;
   cudaStream_t stream = nullptr, side = nullptr;
@@ -81,6 +89,11 @@ struct cr_batch {
   double *save_rad = nullptr, *save_l0 = nullptr, *save_a0 = nullptr;
   FireParams fp{};
   bool fire_ready = false;
+  // compression on the device (compress_device)
+  CompSys* comp = nullptr;             // [S] per-system protocol state
+  int *sys_nv_d = nullptr, *sys_r0_d = nullptr, *sys_np_d = nullptr, *cells0_d = nullptr;
+  cudaStream_t cap_s2 = nullptr, cap_s3 = nullptr;  // capture streams of the nested loop bodies
+  cudaGraphExec_t comp_exec = nullptr;
   std::map<std::pair<long, int>, cudaGraphExec_t> graphs;  // (iterations, cap) -> FIRE chunk
   long long launches = 0;
   std::string err;
@@ -268,7 +281,11 @@ __global__ void __launch_bounds__(256) k_bfire_pre(const __grid_constant__ BFire
   if (!st->abort && v < f.nv) {
     const int s = f.vsys[v];
     BatchSys& bs = f.bsys[s];
-    if (bs.active && !bs.converged) {
+    if (bs.active && !bs.converged && bs.fire_cap > 0 && bs.fire_iters >= bs.fire_cap) {
+      // iteration limit of this run: the system stops as if converged (its
+      // tiles skip the force op that follows)
+      if (v == f.sys_v0[s]) bs.converged = 1;
+    } else if (bs.active && !bs.converged) {
       const long long it = bs.fire_iters;
       const double* cur = f.bfire + ((size_t)s * 2 + (it & 1)) * 4;
       double dt = cur[0], alpha = cur[1];
@@ -447,6 +464,185 @@ __global__ void k_bsave(int nv, int np, const int* vsys, const int* ring_sys, co
   }
 }
 
+// ------------------------------------------------------------------ compression on the device
+//
+// The compressFIRE protocol of cr_batch_compress as one CUDA graph: an outer
+// WHILE node over compression steps and, inside it, a WHILE node over chunks
+// of FIRE iterations (the chunk of the host loop, with its conditional
+// rebuild nodes).  Every decision the host loop makes between launches is
+// made here by a kernel, with the host loop's arithmetic in the host loop's
+// order (per-system sums run sequentially on one thread), so both loops
+// produce the same states.
+
+struct CompArgs {
+  CompSys* comp;
+  BatchSys* bsys;
+  double* bfire;
+  int4* sgrid;
+  const int* cells0;   // cells of each system's grid when the run started (its share of the cell arrays)
+  const double* rad;
+  const double* a0;
+  const int* sys_v0;
+  const int* sys_nv;
+  const int* sys_r0;
+  const int* sys_np;
+  const double* partials;  // per-tile packing-fraction numerators (k_btile_phi)
+  double* scale;           // [S] scale factor of the step
+  int* flag;               // [S] save / restore request
+  DevStatus* st;
+  int S;
+  double cutoff_, cut_distance;
+  double dphi0, min_dphi, fire_dt, tol0, energy_tol;
+  long long max_fire_iters, max_steps;
+  int criterion;
+  cudaGraphConditionalHandle outer, inner;
+};
+
+// Start of a compression step, one thread per system: the FIRE setup of the
+// host loop (cr_batch_init_fire with dt = fire_dt sigma, the tolerance
+// tol0 / sigma, the active set), the radius statistics behind the
+// displacement cutoff, and the cell grid for the current largest radius.
+__global__ void k_cstep_begin(const __grid_constant__ CompArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.S || a.st->abort) return;
+  BatchSys& bs = a.bsys[s];
+  double sa = 0.0;
+  for (int q = a.sys_r0[s]; q < a.sys_r0[s] + a.sys_np[s]; q++) sa += a.a0[q];
+  const double sigma = 2 * sqrt(sa / (kPi * a.sys_np[s]));  // DPM2D::getMeanParticleSize
+  const double dt = a.fire_dt * sigma, dmax = (10 * a.fire_dt) * (dt / a.fire_dt);
+  for (int par = 0; par < 2; par++) {
+    double* f = a.bfire + ((size_t)s * 2 + par) * 4;
+    f[0] = dt;
+    f[1] = 0.2;
+    f[2] = 0.0;
+    f[3] = dmax;
+  }
+  double m = 0.0, sr = 0.0;
+  for (int v = a.sys_v0[s]; v < a.sys_v0[s] + a.sys_nv[s]; v++) {
+    m = fmax(m, a.rad[v]);
+    sr += a.rad[v];
+  }
+  bs.fire_iters = 0;
+  bs.converged = 0;
+  bs.fire_tol = a.tol0 / sigma;
+  bs.rebuild = 0;
+  bs.done_ctr = 0;
+  bs.active = a.comp[s].state == 0 ? 1 : 0;
+  bs.fire_cap = a.max_fire_iters;
+  bs.disp_cutoff = a.cutoff_ * 2.0 * (sr / a.sys_nv[s]);
+  const double cmin = (1.0 + a.cut_distance) * 2.0 * m * (1.0 + 1e-9);
+  int ncx = cmin > 0 ? (int)floor(bs.box.lx / cmin) : 1;
+  int ncy = cmin > 0 ? (int)floor(bs.box.ly / cmin) : 1;
+  ncx = min(ncx, 4096);
+  ncy = min(ncy, 4096);
+  if (ncx < 3 || ncy < 3) ncx = ncy = 1;
+  // radii never fall below the run's starting radii, so the grid never
+  // outgrows the system's share of the cell arrays
+  if ((long long)ncx * ncy <= a.cells0[s]) {
+    a.sgrid[s].x = ncx;
+    a.sgrid[s].y = ncy;
+  }
+}
+
+// Status flags of a fresh FIRE run (clear_flags without the abort flag).
+__global__ void k_cclear(DevStatus* st) {
+  st->overflow = 0;
+  st->rebuild = 0;
+  st->nonfinite = 0;
+  st->converged = 0;
+  st->done_ctr = 0;
+}
+
+// Loop condition of the FIRE chunks: a system still running and no abort.
+__global__ void k_cfire_more(const __grid_constant__ CompArgs a) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  for (int s = threadIdx.x; s < a.S; s += blockDim.x)
+    if (a.bsys[s].active && !a.bsys[s].converged) s_any = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(a.inner, (s_any && !a.st->abort) ? 1u : 0u);
+}
+
+// The jammed / under-jammed / over-jammed decision (compressFIRE.cpp:141-172)
+// of every compressing system, on the sums of the relaxed state.
+__global__ void k_cdecide(const __grid_constant__ CompArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.S) return;
+  if (a.st->abort) {
+    // the step is run again: nothing saved, restored or scaled
+    a.flag[s] = 0;
+    a.scale[s] = 1.0;
+    return;
+  }
+  CompSys& c = a.comp[s];
+  const BatchSys& bs = a.bsys[s];
+  int flag = 0;
+  double scale = 1.0;
+  if (c.state == 0) {
+    c.fire_total += bs.fire_iters;
+    c.steps += 1;
+    const double fmax = sqrt(bs.sums[S_FMAX2]), tol = bs.fire_tol;
+    bool jam, over, under;
+    if (a.criterion == 1) {
+      const double u = bs.sums[S_PE] / a.sys_np[s];
+      jam = u > a.energy_tol && u < 2 * a.energy_tol;
+      over = u >= 2 * a.energy_tol;
+      under = u <= a.energy_tol;
+    } else {
+      jam = fmax > tol && fmax < 2 * tol;
+      over = fmax >= 2 * tol;
+      under = fmax <= tol;
+    }
+    if (jam) {
+      c.state = 1;
+    } else {
+      if (under) {
+        scale = sqrt((c.phi + c.dphi) / c.phi);
+        c.prev = c.phi;
+        flag = 1;
+      } else if (over) {
+        c.dphi *= 0.5;
+        scale = sqrt((c.prev + c.dphi) / c.prev);
+        flag = 2;
+      }
+      if (c.dphi < a.min_dphi) c.state = 3;
+    }
+  }
+  a.flag[s] = flag;
+  a.scale[s] = c.state != 0 ? 1.0 : scale;
+}
+
+// Packing fraction of every system after the step (the host loop's order:
+// tile numerators summed one after the other), the step limit, and the
+// outer loop's condition.
+__global__ void k_cstep_end(const __grid_constant__ CompArgs a, int count_step) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  if (!a.st->abort) {
+    for (int s = threadIdx.x; s < a.S; s += blockDim.x) {
+      CompSys& c = a.comp[s];
+      if (count_step) {
+        const BatchSys& bs = a.bsys[s];
+        double x = 0.0;
+        for (int t = bs.tile_begin; t < bs.tile_end; t++) x += a.partials[t];
+        c.phi = x / (bs.box.lx * bs.box.ly);
+        if (c.state == 0 && c.steps >= a.max_steps) c.state = 2;
+      }
+      if (c.state == 0) s_any = 1;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    cudaGraphSetConditional(a.outer, (s_any && a.max_steps > 0 && !a.st->abort) ? 1u : 0u);
+}
+
+__global__ void k_copy2(int n, const double2* src, double2* dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i];
+}
+
 // ------------------------------------------------------------------ host helpers
 
 template <typename T>
@@ -476,6 +672,8 @@ int download(cr_batch* b, void* dst, const void* src, size_t bytes) {
 void drop_graphs(cr_batch* b) {
   for (auto& kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
+  if (b->comp_exec) cudaGraphExecDestroy(b->comp_exec);
+  b->comp_exec = nullptr;
 }
 
 int read_status(cr_batch* b) { return download(b, b->status_h, b->status, sizeof(DevStatus)); }
@@ -713,18 +911,18 @@ LaunchCfg tile_cfg(cr_batch* b, cudaStream_t st) {
   return LaunchCfg{st, (int)b->tiles_h.size(), b->lanes, b->precision};
 }
 
-int force_all(cr_batch* b) {
+int force_all(cr_batch* b, cudaStream_t st = nullptr) {
   StepArgs s = step_args(b);
   s.kind = KIND_NONE;
   s.write_out = 1;
-  launch_tile_batch(tile_cfg(b, b->stream), b->potential, inter_kind(b), MODE_FORCE, b->p, arrays(b), s);
+  launch_tile_batch(tile_cfg(b, st ? st : b->stream), b->potential, inter_kind(b), MODE_FORCE, b->p, arrays(b), s);
   b->launches++;
   BT_TRY(cudaGetLastError());
   return CR_OK;
 }
 
-int reduce_sys(cr_batch* b, int set_converged) {
-  k_btile_reduce<128><<<(int)b->tiles_h.size(), 128, 0, b->stream>>>(
+int reduce_sys(cr_batch* b, int set_converged, cudaStream_t st = nullptr) {
+  k_btile_reduce<128><<<(int)b->tiles_h.size(), 128, 0, st ? st : b->stream>>>(
       b->tiles, b->vel, b->force, b->energy, b->p_energy, b->vtopo, inter_kind(b) == INT_SMOOTH, b->bsys,
       b->partials, set_converged);
   b->launches++;
@@ -764,41 +962,47 @@ void enqueue_fire_tile(cr_batch* b, cudaStream_t st) {
   b->launches++;
 }
 
-int capture_fire_chunk(cr_batch* b, long n, cudaGraphExec_t* out) {
-  cudaGraph_t graph;
-  BT_TRY(cudaGraphCreate(&graph, 0));
-  BT_TRY(cudaStreamBeginCaptureToGraph(b->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+// n FIRE iterations onto stream st, which is capturing into graph g: each
+// iteration's rebuild is a conditional node whose body is captured on side.
+int add_fire_iterations(cr_batch* b, cudaStream_t st, cudaStream_t side, cudaGraph_t g, long n) {
   for (long i = 0; i < n; i++) {
     cudaGraphConditionalHandle h = 0;
-    cudaError_t e = cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault);
-    if (e != cudaSuccess) {
-      cudaGraph_t dummy;
-      cudaStreamEndCapture(b->stream, &dummy);
-      cudaGraphDestroy(graph);
-      return b->fail(CR_ECUDA, std::string("cudaGraphConditionalHandleCreate: ") + cudaGetErrorString(e));
-    }
-    enqueue_fire_iteration(b, b->stream, true, h);
+    BT_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    enqueue_fire_iteration(b, st, true, h);
     cudaStreamCaptureStatus cs;
     cudaGraph_t cg;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
-    BT_TRY(cudaStreamGetCaptureInfo(b->stream, &cs, nullptr, &cg, &deps, &ndeps));
+    BT_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps));
     cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
     cp.conditional.handle = h;
     cp.conditional.type = cudaGraphCondTypeIf;
     cp.conditional.size = 1;
     cudaGraphNode_t node;
     BT_TRY(cudaGraphAddNode(&node, cg, deps, ndeps, &cp));
-    BT_TRY(cudaStreamUpdateCaptureDependencies(b->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    BT_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
     cudaGraph_t body = cp.conditional.phGraph_out[0];
-    BT_TRY(cudaStreamBeginCaptureToGraph(b->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    enqueue_build(b, b->side, 0);
+    BT_TRY(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_build(b, side, 0);
     cudaGraph_t body_out;
-    BT_TRY(cudaStreamEndCapture(b->side, &body_out));
-    enqueue_fire_tile(b, b->stream);
+    BT_TRY(cudaStreamEndCapture(side, &body_out));
+    enqueue_fire_tile(b, st);
   }
+  return CR_OK;
+}
+
+int capture_fire_chunk(cr_batch* b, long n, cudaGraphExec_t* out) {
+  cudaGraph_t graph;
+  BT_TRY(cudaGraphCreate(&graph, 0));
+  BT_TRY(cudaStreamBeginCaptureToGraph(b->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const int rc = add_fire_iterations(b, b->stream, b->side, graph, n);
   cudaGraph_t g;
-  BT_TRY(cudaStreamEndCapture(b->stream, &g));
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc) {
+    cudaGraphDestroy(graph);
+    return rc;
+  }
+  BT_TRY(e);
   BT_TRY(cudaGraphInstantiate(out, g, 0));
   cudaGraphDestroy(g);
   return CR_OK;
@@ -933,6 +1137,211 @@ int mean_particle_sizes(cr_batch* b, double* out) {
   return CR_OK;
 }
 
+
+// The device compression loop as one graph (see k_cstep_begin): an outer
+// WHILE node over compression steps, and inside it a WHILE node over chunks
+// of 64 FIRE iterations.  The loop bodies are captured on their own streams
+// while the enclosing capture is open.
+int add_while(cr_batch* b, cudaStream_t st, cudaGraphConditionalHandle h, cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  BT_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps));
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  BT_TRY(cudaGraphAddNode(&node, cg, deps, ndeps, &cp));
+  BT_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  *body = cp.conditional.phGraph_out[0];
+  return CR_OK;
+}
+
+int compress_body(cr_batch* b, CompArgs a, cudaGraph_t outer_body) {
+  cudaStream_t s2 = b->cap_s2, s3 = b->cap_s3;
+  BT_TRY(cudaGraphConditionalHandleCreate(&a.inner, outer_body, 0, cudaGraphCondAssignDefault));
+  const int nb = (b->nv + 255) / 256, sb = (b->S + 127) / 128;
+  // the step's starting positions and velocities, for a rerun after a list overflow
+  k_copy2<<<nb, 256, 0, s2>>>(b->nv, b->pos, b->snap_pos);
+  k_copy2<<<nb, 256, 0, s2>>>(b->nv, b->vel, b->snap_vel);
+  k_cstep_begin<<<sb, 128, 0, s2>>>(a);
+  k_cclear<<<1, 1, 0, s2>>>(b->status);
+  enqueue_build(b, s2, 1);
+  int rc;
+  if ((rc = force_all(b, s2)) || (rc = reduce_sys(b, 1, s2))) return rc;
+  k_cfire_more<<<1, 256, 0, s2>>>(a);
+  cudaGraph_t inner_body;
+  if ((rc = add_while(b, s2, a.inner, &inner_body))) return rc;
+  BT_TRY(cudaStreamBeginCaptureToGraph(s3, inner_body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  rc = add_fire_iterations(b, s3, b->side, inner_body, 64);
+  if (!rc) k_cfire_more<<<1, 256, 0, s3>>>(a);
+  cudaGraph_t ib_out;
+  const cudaError_t e = cudaStreamEndCapture(s3, &ib_out);
+  if (rc) return rc;
+  BT_TRY(e);
+  if ((rc = reduce_sys(b, 0, s2))) return rc;
+  k_cdecide<<<sb, 128, 0, s2>>>(a);
+  const int n = std::max(b->nv, b->np);
+  k_bsave<<<(n + 255) / 256, 256, 0, s2>>>(b->nv, b->np, b->vsys, b->ring_sys, b->sys_flag, b->pos, b->rad, b->l0,
+                                           b->a0, b->save_pos, b->save_rad, b->save_l0, b->save_a0);
+  if ((rc = force_all(b, s2))) return rc;  // ring centroids of the (restored) positions
+  k_bscale<<<(n + 255) / 256, 256, 0, s2>>>(b->nv, b->np, b->vsys, b->ring_sys, b->ring_of, b->ppos, b->sys_scalar,
+                                            b->pos, b->l0, b->rad, b->a0, b->area);
+  if ((rc = force_all(b, s2))) return rc;  // ring areas of the scaled rings
+  k_btile_phi<128><<<(int)b->tiles_h.size(), 128, 0, s2>>>(b->tiles, b->vtopo, b->area, b->rad, b->partials);
+  k_cstep_end<<<1, 256, 0, s2>>>(a, 1);
+  BT_TRY(cudaGetLastError());
+  return CR_OK;
+}
+
+int capture_compress(cr_batch* b, CompArgs a, cudaGraphExec_t* out) {
+  if (!b->cap_s2) BT_TRY(cudaStreamCreateWithFlags(&b->cap_s2, cudaStreamNonBlocking));
+  if (!b->cap_s3) BT_TRY(cudaStreamCreateWithFlags(&b->cap_s3, cudaStreamNonBlocking));
+  cudaGraph_t graph;
+  BT_TRY(cudaGraphCreate(&graph, 0));
+  BT_TRY(cudaGraphConditionalHandleCreate(&a.outer, graph, 0, cudaGraphCondAssignDefault));
+  BT_TRY(cudaStreamBeginCaptureToGraph(b->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  k_cstep_end<<<1, 256, 0, b->stream>>>(a, 0);
+  cudaGraph_t outer_body;
+  int rc = add_while(b, b->stream, a.outer, &outer_body);
+  if (!rc) {
+    const cudaError_t e2 = cudaStreamBeginCaptureToGraph(b->cap_s2, outer_body, nullptr, nullptr, 0,
+                                                         cudaStreamCaptureModeThreadLocal);
+    if (e2 != cudaSuccess) {
+      rc = b->fail(CR_ECUDA, std::string("capture of the compression step: ") + cudaGetErrorString(e2));
+    } else {
+      rc = compress_body(b, a, outer_body);
+      cudaGraph_t ob_out;
+      const cudaError_t e3 = cudaStreamEndCapture(b->cap_s2, &ob_out);
+      if (!rc && e3 != cudaSuccess) rc = b->fail(CR_ECUDA, std::string("capture: ") + cudaGetErrorString(e3));
+    }
+  }
+  cudaGraph_t g;
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc) {
+    cudaGraphDestroy(graph);
+    return rc;
+  }
+  BT_TRY(e);
+  BT_TRY(cudaGraphInstantiate(out, g, 0));
+  cudaGraphDestroy(g);
+  return CR_OK;
+}
+
+// cr_batch_compress: the protocol of compress_host with every step on the
+// device, one graph launch for the whole run.  A list overflow stops the
+// graph; the host restores the step's starting positions and velocities,
+// grows the lists and launches the loop again from that step.  A system's
+// FIRE run stops after max_fire_iters iterations exactly, as in the host loop.
+int compress_device(cr_batch* b, const cr_compress_params* prm, double* phiOut, long* stepsOut, int* stateOut,
+                    long* fireItersOut) {
+  const int S = b->S;
+  int rc;
+  if (!b->nbr_built && (rc = cr_batch_calc_neighbor_lists(b))) return rc;
+  if (!b->comp) {
+    if ((rc = dalloc(b, &b->comp, S)) || (rc = dalloc(b, &b->sys_nv_d, S)) || (rc = dalloc(b, &b->sys_r0_d, S)) ||
+        (rc = dalloc(b, &b->sys_np_d, S)) || (rc = dalloc(b, &b->cells0_d, S)))
+      return rc;
+    if ((rc = upload(b, b->sys_nv_d, b->sys_nv.data(), S * sizeof(int))) ||
+        (rc = upload(b, b->sys_r0_d, b->sys_r0.data(), S * sizeof(int))) ||
+        (rc = upload(b, b->sys_np_d, b->sys_np.data(), S * sizeof(int))))
+      return rc;
+  }
+  // every system's share of the cell arrays: its grid for the starting radii
+  if ((rc = refresh_radius_stats(b)) || (rc = apply_cutoffs(b)) || (rc = setup_grids(b))) return rc;
+  std::vector<int> cells0(S);
+  for (int s = 0; s < S; s++) cells0[s] = b->sgrid_h[s].x * b->sgrid_h[s].y;
+  if ((rc = upload(b, b->cells0_d, cells0.data(), S * sizeof(int)))) return rc;
+  // starting packing fractions; the starting configuration is the first saved state
+  std::vector<double> phi(S);
+  if ((rc = force_all(b)) || (rc = pull_sys(b)) || (rc = phis(b, b->area, phi.data()))) return rc;
+  std::vector<int> flag(S, 1);
+  if ((rc = upload(b, b->sys_flag, flag.data(), S * sizeof(int)))) return rc;
+  const int n = std::max(b->nv, b->np);
+  k_bsave<<<(n + 255) / 256, 256, 0, b->stream>>>(b->nv, b->np, b->vsys, b->ring_sys, b->sys_flag, b->pos, b->rad,
+                                                  b->l0, b->a0, b->save_pos, b->save_rad, b->save_l0, b->save_a0);
+  b->launches++;
+  BT_TRY(cudaGetLastError());
+  std::vector<CompSys> comp(S);
+  for (int s = 0; s < S; s++) comp[s] = CompSys{phi[s], phi[s], prm->dphi, 0, 0, 0, 0};
+  if ((rc = upload(b, b->comp, comp.data(), S * sizeof(CompSys)))) return rc;
+  // FIRE parameters of compressFIRE.cpp:106 ({a_start, f_dec, f_inc, f_a, dt,
+  // 10 dt, a}, minStep 20); each step's per-system dt comes from k_cstep_begin
+  b->fp.a_start = 0.2;
+  b->fp.f_dec = 0.5;
+  b->fp.f_inc = 1.1;
+  b->fp.f_a = 0.99;
+  b->fp.dt_max = 10 * prm->fire_dt;
+  b->fp.min_step = 20;
+  b->fp.tol = -1.0;
+  b->fire_ready = true;
+  CompArgs a{};
+  a.comp = b->comp;
+  a.bsys = b->bsys;
+  a.bfire = b->bfire;
+  a.sgrid = b->sgrid;
+  a.cells0 = b->cells0_d;
+  a.rad = b->rad;
+  a.a0 = b->a0;
+  a.sys_v0 = b->sys_v0_d;
+  a.sys_nv = b->sys_nv_d;
+  a.sys_r0 = b->sys_r0_d;
+  a.sys_np = b->sys_np_d;
+  a.partials = b->partials;
+  a.scale = b->sys_scalar;
+  a.flag = b->sys_flag;
+  a.st = b->status;
+  a.S = S;
+  a.cutoff_ = b->cutoff_;
+  a.cut_distance = b->cut_distance;
+  a.dphi0 = prm->dphi;
+  a.min_dphi = prm->min_dphi;
+  a.fire_dt = prm->fire_dt;
+  a.tol0 = prm->tol0;
+  a.energy_tol = prm->energy_tol;
+  a.max_fire_iters = prm->max_fire_iters;
+  a.max_steps = prm->max_steps;
+  a.criterion = prm->criterion;
+  if ((rc = clear_flags(b))) return rc;
+  for (int attempt = 0;; attempt++) {
+    drop_graphs(b);
+    if ((rc = capture_compress(b, a, &b->comp_exec))) return rc;
+    BT_TRY(cudaGraphLaunch(b->comp_exec, b->stream));
+    if ((rc = read_status(b))) return rc;
+    if (!b->status_h->abort) break;
+    if (b->status_h->nonfinite) return b->fail(CR_ENONFINITE, "non-finite force in a batched compression");
+    if (!b->status_h->overflow || attempt >= 8) return b->fail(CR_ECUDA, "batched compression aborted");
+    const size_t v2 = (size_t)b->nv * sizeof(double2);
+    BT_TRY(cudaMemcpyAsync(b->pos, b->snap_pos, v2, cudaMemcpyDeviceToDevice, b->stream));
+    BT_TRY(cudaMemcpyAsync(b->vel, b->snap_vel, v2, cudaMemcpyDeviceToDevice, b->stream));
+    if ((rc = alloc_lists(b, (int)pow2ceil(2LL * b->status_h->max_count)))) return rc;
+    if ((rc = clear_flags(b))) return rc;
+  }
+  drop_graphs(b);
+  if ((rc = download(b, comp.data(), b->comp, S * sizeof(CompSys)))) return rc;
+  long long iters = 0, steps = 0;
+  for (int s = 0; s < S; s++) {
+    if (phiOut) phiOut[s] = comp[s].phi;
+    if (stepsOut) stepsOut[s] = (long)comp[s].steps;
+    if (stateOut) stateOut[s] = comp[s].state;
+    if (fireItersOut) fireItersOut[s] = (long)comp[s].fire_total;
+    iters = std::max(iters, comp[s].fire_total);
+    steps = std::max(steps, comp[s].steps);
+  }
+  b->launches += 2 * iters + 24 * steps;  // FIRE iterations, and the kernels of each step
+  // the other entry points see every system active, no iteration limit, and
+  // the host-side radius statistics and grids of the final radii
+  if ((rc = pull_sys(b))) return rc;
+  for (BatchSys& bs : b->bsys_h) {
+    bs.active = 1;
+    bs.fire_cap = 0;
+  }
+  if ((rc = push_sys(b))) return rc;
+  if ((rc = refresh_radius_stats(b)) || (rc = setup_grids(b))) return rc;
+  return CR_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -1057,12 +1466,15 @@ int cr_batch_destroy(cr_batch* b) {
                   b->vsys, b->ring_sys, b->sys_v0_d, b->tiles, b->nbr, b->nbr_pq, b->nbr_cnt, b->cell_of, b->slot,
                   b->cell_cnt, b->cell_start, b->cell_vid, b->cell_ring, b->cell_pq, b->cell_pos, b->cell_rad,
                   b->sgrid, b->bsys, b->bfire, b->partials, b->sys_scalar, b->sys_flag, b->status, b->snap_pos,
-                  b->snap_vel, b->snap_bsys, b->snap_bfire, b->save_pos, b->save_rad, b->save_l0, b->save_a0};
+                  b->snap_vel, b->snap_bsys, b->snap_bfire, b->save_pos, b->save_rad, b->save_l0, b->save_a0,
+                  b->comp, b->sys_nv_d, b->sys_r0_d, b->sys_np_d, b->cells0_d};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (b->status_h) cudaFreeHost(b->status_h);
   if (b->stream) cudaStreamDestroy(b->stream);
   if (b->side) cudaStreamDestroy(b->side);
+  if (b->cap_s2) cudaStreamDestroy(b->cap_s2);
+  if (b->cap_s3) cudaStreamDestroy(b->cap_s3);
   delete b;
   return CR_OK;
 }
@@ -1373,6 +1785,15 @@ int cr_batch_compress(cr_batch* b, const cr_compress_params* prm, double* phiOut
                       long* fireItersOut) {
   if (!b || !prm) return CR_EINVAL;
   if (!(prm->dphi > 0) || prm->max_steps < 0 || prm->max_fire_iters <= 0) return b->fail(CR_EINVAL, "bad compress params");
+  return compress_device(b, prm, phiOut, stepsOut, stateOut, fireItersOut);
+}
+
+// The same protocol driven from the host: one host round trip per chunk of
+// 64 FIRE iterations and per compression step.
+int cr_batch_compress_stepwise(cr_batch* b, const cr_compress_params* prm, double* phiOut, long* stepsOut,
+                               int* stateOut, long* fireItersOut) {
+  if (!b || !prm) return CR_EINVAL;
+  if (!(prm->dphi > 0) || prm->max_steps < 0 || prm->max_fire_iters <= 0) return b->fail(CR_EINVAL, "bad compress params");
   const int S = b->S;
   std::vector<double> phi(S), prev(S), dphi(S, prm->dphi), sigma(S), tol(S), dts(S), scale(S);
   std::vector<int> state(S, 0), flag(S);
@@ -1528,6 +1949,12 @@ int cr_batch_autotune(cr_batch* b, long reps, int* lanes_out) {
   }
   if ((rc = cr_batch_set_lanes(b, best))) return rc;
   if (lanes_out) *lanes_out = best;
+  return CR_OK;
+}
+
+int cr_batch_get_list_capacity(const cr_batch* b, int* out) {
+  if (!b || !out) return CR_EINVAL;
+  *out = b->cap;
   return CR_OK;
 }
 

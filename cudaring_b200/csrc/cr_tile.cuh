@@ -41,6 +41,7 @@ struct BatchSys {
   int converged;           // FIRE reached fire_tol: the system is frozen
   int active;              // 0: the system takes no part in step ops
   unsigned int done_ctr;   // tiles of this system finished in the current op
+  long long fire_cap;      // > 0: FIRE stops (marks the system converged) after this many iterations
 };
 
 struct StepArgs {

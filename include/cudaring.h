@@ -493,7 +493,15 @@ typedef struct cr_compress_params {
 } cr_compress_params;
 int cr_batch_compress(cr_batch* b, const cr_compress_params* params, double* phi, long* steps, int* state,
                       long* fireIterations);
+/* The same protocol with the host between steps and between chunks of 64
+ * FIRE iterations (cr_batch_compress runs the whole loop as one CUDA graph,
+ * conditional WHILE nodes over the steps and the chunks); both give the same
+ * states. */
+int cr_batch_compress_stepwise(cr_batch* b, const cr_compress_params* params, double* phi, long* steps, int* state,
+                               long* fireIterations);
 int cr_batch_get_launch_count(const cr_batch* b, long long* out);
+/* Entries per vertex the batch's neighbour lists hold (grown on overflow). */
+int cr_batch_get_list_capacity(const cr_batch* b, int* out);
 
 #ifdef __cplusplus
 }

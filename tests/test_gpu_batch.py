@@ -146,6 +146,32 @@ def test_batch_compress_matches_per_system_loop(cuda_device):
         d.close()
 
 
+@pytest.mark.parametrize("criterion,max_fire_iters,energy_tol", [("force", 50000, 0.0), ("force", 150, 0.0),
+                                                                 ("energy", 50000, 1e-9)])
+def test_batch_compress_device_loop_matches_stepwise(cuda_device, criterion, max_fire_iters, energy_tol):
+    # the whole protocol as one graph launch against the host-driven loop on
+    # the same systems: the same kernels in the same order, so the same
+    # states bit for bit (150 iterations: the FIRE limit binds every step)
+    pks = batch_packings(4, seed=11, rings=(16, 40))
+    kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
+    prm = dict(dphi=2e-2, min_dphi=2e-3, fire_dt=1e-2, tol0=1e-6, max_fire_iters=max_fire_iters, max_steps=8,
+               criterion=criterion, energy_tol=energy_tol)
+    out = []
+    for stepwise in (False, True):
+        b = Batch.from_packings(pks, **kw)
+        b.setDisplacementCutoff(0.5)
+        res = b.compress(stepwise=stepwise, **prm)
+        out.append((res, b.getVertexPositions(), b.getVertexRadii()))
+    (dev, xd, rd), (host, xh, rh) = out
+    assert np.all(dev["steps"] >= 1)
+    for k in ("steps", "state", "fire_iterations"):
+        assert np.array_equal(dev[k], host[k]), k
+    assert np.array_equal(dev["phi"], host["phi"])
+    assert np.array_equal(xd, xh) and np.array_equal(rd, rh)
+    if max_fire_iters == 150:
+        assert np.all(dev["fire_iterations"] <= 150 * dev["steps"])
+
+
 def test_batch_autotune_and_lanes(cuda_device):
     pks = _systems("smooth_lj", [16, 32], 0.40, seed=9)
     kw = dict(potential="lennardJones", interaction="vertexSmooth", ea=1.0, el=1.0, eb=0.01, ec=1.0, LJcutoff=2.5)
