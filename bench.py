@@ -572,6 +572,7 @@ def main():
         scale = scale_up_measurement(d, c, args, world, peaks)
 
     batch = None if args.no_batch else batched_fire_measurement(args.batch_systems, world, rank)
+    jam = None if (args.no_batch or rank != 0) else jamming_measurement()
 
     rigid = None
     if rank == 0 and not args.no_rigid:
@@ -602,7 +603,7 @@ def main():
                        "lanes_per_vertex": lanes},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": run["launches"],
             "clocks": run["clocks"], "precision_comparison": comparison, "scale_up": scale,
-            "batched_systems": batch, "rigid_ellipses": rigid, "derivatives": deriv,
+            "batched_systems": batch, "compression_to_jamming": jam, "rigid_ellipses": rigid, "derivatives": deriv,
         }
         print(json.dumps(line), flush=True)
     d.close()
@@ -697,7 +698,8 @@ def batched_fire_measurement(num_systems: int, world: int, rank: int, fire_iters
     pos, rad, l0, a0 = b.getVertexPositions(), b.getVertexRadii(), b.getRestLengths(), b.getRestAreas()
     out = {"workload": f"{num_systems} systems, {nv_all} vertices, rings U[16,512] nv 16/22, harmonic, "
                        f"phi 0.60, FIRE to 1e-10/sigma (<= {fire_iters} iterations)",
-           "unit": "vertex-iterations/s", "lanes_per_vertex": lanes, "prep_seconds": t_prep,
+           "unit": "vertex-iterations/s", "lanes_per_vertex": lanes, "tile_shape": list(b.getTileShape()),
+           "prep_seconds": t_prep,
            "ranks": world, "rank0_block": [blk.start, blk.stop]}
     for prec in ("fp64", "mixed"):
         b.setVertexPositions(pos)
@@ -754,6 +756,71 @@ def batched_fire_measurement(num_systems: int, world: int, rank: int, fire_iters
     out["compression_sample"] = {"steps": 3, "dphi": 1e-3, "seconds": dt, "value": vi / dt,
                                  "phi_mean": float(np.mean(phis))}
     b.close()
+    return out
+
+
+def jamming_measurement(num_systems: int = 8) -> dict:
+    """Compression to jamming of a small batch, three ways: the protocol as
+    one graph launch on the device (cr_batch_compress), the same protocol
+    driven from the host between steps and FIRE chunks
+    (cr_batch_compress_stepwise; the same states are required), and every
+    system through its own single-system context (compress.compress_system).
+    Rank 0 only: a secondary measurement."""
+    import torch
+
+    from cudaring_b200 import DPM2D, synth
+    from cudaring_b200.batch import Batch
+    from cudaring_b200.compress import batch_packings, compress_system, prepare_batch
+
+    kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
+    pks = batch_packings(num_systems, seed=17, rings=(16, 32))
+    b = Batch.from_packings(pks, **kw)
+    prepare_batch(b, phi0=0.70)
+    pos, rad, l0, a0 = b.getVertexPositions(), b.getVertexRadii(), b.getRestLengths(), b.getRestAreas()
+    prm = dict(dphi=2e-2, min_dphi=2e-3, fire_dt=1e-2, tol0=1e-6, max_fire_iters=20000, max_steps=40)
+    out = {"workload": f"{num_systems} systems, rings U[16,32] nv 16/22, harmonic, from phi 0.70: dphi 0.02 halved "
+                       "on overshoot down to 0.002, FIRE to 1e-6/sigma, at most 40 steps",
+           "vertices": int(sum(p.num_vertices for p in pks))}
+    res = {}
+    for mode in ("device", "stepwise"):
+        b.setVertexPositions(pos)
+        b.setVertexVelocities(np.zeros_like(pos))
+        b.setVertexRadii(rad)
+        b.setRestLengths(l0)
+        b.setRestAreas(a0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = b.compress(stepwise=mode == "stepwise", **prm)
+        torch.cuda.synchronize()
+        res[mode] = (time.perf_counter() - t0, r)
+    b.close()
+    t_dev, r_dev = res["device"]
+    t_host, r_host = res["stepwise"]
+    same = all(np.array_equal(r_dev[k], r_host[k]) for k in ("phi", "steps", "state", "fire_iterations"))
+    out["device"] = {"seconds": t_dev, "phi": [round(float(x), 5) for x in r_dev["phi"]],
+                     "steps": [int(x) for x in r_dev["steps"]], "state": [int(x) for x in r_dev["state"]],
+                     "fire_iterations": int(r_dev["fire_iterations"].sum())}
+    out["stepwise"] = {"seconds": t_host, "same_states_as_device": bool(same)}
+    # every system through its own context, from the same prepared state
+    vo = np.cumsum([0] + [p.num_vertices for p in pks])
+    ro = np.cumsum([0] + [p.num_particles for p in pks])
+    t0 = time.perf_counter()
+    phis = []
+    for s, pk in enumerate(pks):
+        one_pk = synth.Packing(nv_list=pk.nv_list, pos=pos[2 * vo[s]:2 * vo[s + 1]], vel=np.zeros(2 * pk.num_vertices),
+                               rad=rad[vo[s]:vo[s + 1]], l0=l0[vo[s]:vo[s + 1]], theta0=pk.theta0,
+                               a0=a0[ro[s]:ro[s + 1]], box=pk.box, centres=pk.centres)
+        d = DPM2D.from_packing(one_pk, **kw)
+        d.calcNeighborList(d.setDisplacementCutoff(0.5, 2.0 * d.getMeanVertexRadius()))
+        phis.append(round(float(compress_system(d, **prm)["phi"]), 5))
+        d.close()
+    torch.cuda.synchronize()
+    t_loop = time.perf_counter() - t0
+    out["per_system_loop"] = {"seconds": t_loop, "systems": num_systems, "phi": phis,
+                              "note": "the FIRE sums reduce in another order, so decisions at the 2 tol margin can "
+                                      "flip and the paths to jamming part"}
+    out["device_over_stepwise"] = t_host / t_dev
+    out["device_over_loop"] = t_loop / t_dev
     return out
 
 

@@ -95,7 +95,18 @@ class Batch:
         self._call("cr_batch_get_lanes", C.byref(out))
         return out.value
 
+    def setTileShape(self, lanes, block):
+        self._call("cr_batch_set_tile_shape", int(lanes), int(block))
+
+    def getTileShape(self):
+        lanes, block = C.c_int(), C.c_int()
+        self._call("cr_batch_get_tile_shape", C.byref(lanes), C.byref(block))
+        return lanes.value, block.value
+
     def autotune(self, reps=20):
+        """Times the batched FIRE force kernel for every tile shape whose tile
+        holds the longest ring and keeps the fastest; returns its lane count
+        (getTileShape gives the shape)."""
         out = C.c_int()
         self._call("cr_batch_autotune", int(reps), C.byref(out))
         return out.value

@@ -52,6 +52,7 @@ struct cr_batch {
   int potential = CR_POTENTIAL_HARMONIC;
   int interaction = CR_INTERACTION_VERTEX_VERTEX;
   int lanes = 1;
+  int block = 0;  // threads per tile CTA (0: the lane count's default)
   int precision = CR_PRECISION_FP64;
   double cutoff_ = 0.5;
   double cut_distance = 1.5;
@@ -689,11 +690,15 @@ int inter_kind(const cr_batch* b) {
                                                                                                   : INT_SMOOTH;
 }
 
-int tile_capacity(int lanes) { return tile_vertices(lanes); }  // the single-system tiles' capacity
+// vertices a batch tile of this shape holds (0: unsupported shape)
+int tile_capacity(int lanes, int block = 0) {
+  const int bl = batch_tile_block(lanes, block);
+  return bl ? bl / lanes : 0;
+}
 
 // Tiles of whole rings that never cross a system.
 void make_tiles(cr_batch* b) {
-  const int tv = tile_capacity(b->lanes);
+  const int tv = tile_capacity(b->lanes, b->block);
   b->tiles_h.clear();
   for (int s = 0; s < b->S; s++) {
     b->bsys_h[s].tile_begin = (int)b->tiles_h.size();
@@ -908,7 +913,9 @@ StepArgs step_args(cr_batch* b) {
 }
 
 LaunchCfg tile_cfg(cr_batch* b, cudaStream_t st) {
-  return LaunchCfg{st, (int)b->tiles_h.size(), b->lanes, b->precision};
+  LaunchCfg c{st, (int)b->tiles_h.size(), b->lanes, b->precision};
+  c.block = b->block;
+  return c;
 }
 
 int force_all(cr_batch* b, cudaStream_t st = nullptr) {
@@ -1364,7 +1371,7 @@ int cr_batch_create(long numSystems, const long* numParticles, const long* nvLis
     long nvs = 0;
     for (long q = 0; q < numParticles[s]; q++) {
       const long n = nvList[rings + q];
-      if (n < 3 || n > tile_capacity(1)) {
+      if (n < 3 || n > 192) {
         delete b;
         return n < 3 ? CR_EINVAL : CR_ENOTSUP;
       }
@@ -1407,6 +1414,9 @@ int cr_batch_create(long numSystems, const long* numParticles, const long* nvLis
     bs.fire_tol = -1.0;
     bs.active = 1;
   }
+  // rings longer than the default tile's 128 vertices take the 192-vertex tile
+  for (int n : b->ring_nv_h)
+    if (n > 128) b->block = 192;
   make_tiles(b);
   if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess) {
@@ -1541,18 +1551,33 @@ int cr_batch_set_precision(cr_batch* b, int precision) {
   return CR_OK;
 }
 
-int cr_batch_set_lanes(cr_batch* b, int lanes) {
-  if (!b || (lanes != 1 && lanes != 2 && lanes != 4)) return CR_EINVAL;
+int cr_batch_set_tile_shape(cr_batch* b, int lanes, int block) {
+  if (!b) return CR_EINVAL;
+  const int cap = tile_capacity(lanes, block);
+  if (!cap) return b->fail(CR_EINVAL, "unsupported tile shape");
   for (int n : b->ring_nv_h)
-    if (n > tile_capacity(lanes)) return b->fail(CR_EINVAL, "a ring does not fit the tile of this lane count");
+    if (n > cap) return b->fail(CR_EINVAL, "a ring does not fit the tile of this shape");
   int rc;
   if ((rc = pull_sys(b))) return rc;
   b->lanes = lanes;
+  b->block = batch_tile_block(lanes, block);
   make_tiles(b);
   if ((rc = upload_tiles(b))) return rc;
   if ((rc = push_sys(b))) return rc;
   drop_graphs(b);
   return CR_OK;
+}
+
+int cr_batch_get_tile_shape(const cr_batch* b, int* lanes, int* block) {
+  if (!b || !lanes || !block) return CR_EINVAL;
+  *lanes = b->lanes;
+  *block = batch_tile_block(b->lanes, b->block);
+  return CR_OK;
+}
+
+int cr_batch_set_lanes(cr_batch* b, int lanes) {
+  if (!b || (lanes != 1 && lanes != 2 && lanes != 4)) return CR_EINVAL;
+  return cr_batch_set_tile_shape(b, lanes, 0);
 }
 
 int cr_batch_get_lanes(const cr_batch* b, int* lanes) {
@@ -1934,21 +1959,23 @@ int cr_batch_autotune(cr_batch* b, long reps, int* lanes_out) {
   if (!b || reps <= 0) return CR_EINVAL;
   int maxnv = 0;
   for (int n : b->ring_nv_h) maxnv = std::max(maxnv, n);
-  int best = b->lanes;
+  int best_l = b->lanes, best_b = b->block;
   double best_ms = 1e300;
   int rc;
-  for (int lanes : {1, 2, 4}) {
-    if (maxnv > tile_capacity(lanes)) continue;
-    if ((rc = cr_batch_set_lanes(b, lanes))) return rc;
+  static const int shapes[][2] = {{1, 128}, {1, 192}, {2, 128}, {2, 192}, {4, 256}};
+  for (const auto& sh : shapes) {
+    if (maxnv > tile_capacity(sh[0], sh[1])) continue;
+    if ((rc = cr_batch_set_tile_shape(b, sh[0], sh[1]))) return rc;
     double ms = 0.0;
     if ((rc = cr_batch_profile_fire_tile(b, reps, &ms))) return rc;
     if (ms < best_ms) {
       best_ms = ms;
-      best = lanes;
+      best_l = sh[0];
+      best_b = sh[1];
     }
   }
-  if ((rc = cr_batch_set_lanes(b, best))) return rc;
-  if (lanes_out) *lanes_out = best;
+  if ((rc = cr_batch_set_tile_shape(b, best_l, best_b))) return rc;
+  if (lanes_out) *lanes_out = best_l;
   return CR_OK;
 }
 

@@ -14,6 +14,7 @@ struct LaunchCfg {
   int lanes;   // lanes per vertex in the pair phase (1, 2, 4, 8)
   int precision = CR_PRECISION_FP64;  // CR_PRECISION_* (deformable tile kernel)
   bool pdl = false;   // programmatic dependent launch (inside step graphs)
+  int block = 0;      // batch tiles: threads per CTA (0: the lane count's default, batch_tile_block)
 };
 
 // cr_tile.cu
@@ -21,7 +22,10 @@ void launch_tile(const LaunchCfg& c, int pot, int inter, int mode, const SysPara
                  const StepArgs& s);
 int tile_vertices(int lanes);
 // cr_tile_batch.cu: the same kernel over the tiles of many systems (tile.x =
-// system, s.bsys the per-system table); lanes 1, 2 or 4
+// system, s.bsys the per-system table).  Tile shapes (lanes per vertex,
+// threads per CTA): (1, 128), (1, 192), (2, 128), (2, 192), (4, 256); a
+// tile holds threads / lanes vertices.
+int batch_tile_block(int lanes, int block);   // the shape's CTA size (0: the lane count's default), or 0 if unsupported
 void launch_tile_batch(const LaunchCfg& c, int pot, int inter, int mode, const SysParams& p, const SysArrays& a,
                        const StepArgs& s);
 // Multi-step kernel (k_tile_steps): up to s.persist_max middle steps per

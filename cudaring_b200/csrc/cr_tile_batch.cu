@@ -5,11 +5,25 @@
 
 namespace cr {
 
+int batch_tile_block(int lanes, int block) {
+  if (lanes == 1) return block == 0 ? 128 : ((block == 128 || block == 192) ? block : 0);
+  if (lanes == 2) return block == 0 ? 192 : ((block == 128 || block == 192) ? block : 0);
+  if (lanes == 4) return (block == 0 || block == 256) ? 256 : 0;
+  return 0;
+}
+
 template <int POT, int INTER, int MODE, int PREC>
 static void launch_batch_t(const LaunchCfg& c, const SysParams& p, const SysArrays& a, const StepArgs& s) {
-  if (c.lanes == 1) k_tile<POT, INTER, MODE, 128, 1, PREC, true><<<c.grid, 128, 0, c.stream>>>(p, a, s);
-  else if (c.lanes == 4) k_tile<POT, INTER, MODE, 256, 4, PREC, true><<<c.grid, 256, 0, c.stream>>>(p, a, s);
-  else k_tile<POT, INTER, MODE, 192, 2, PREC, true><<<c.grid, 192, 0, c.stream>>>(p, a, s);
+  const int block = batch_tile_block(c.lanes, c.block);
+  if (c.lanes == 1) {
+    if (block == 192) k_tile<POT, INTER, MODE, 192, 1, PREC, true><<<c.grid, 192, 0, c.stream>>>(p, a, s);
+    else k_tile<POT, INTER, MODE, 128, 1, PREC, true><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+  } else if (c.lanes == 4) {
+    k_tile<POT, INTER, MODE, 256, 4, PREC, true><<<c.grid, 256, 0, c.stream>>>(p, a, s);
+  } else {
+    if (block == 128) k_tile<POT, INTER, MODE, 128, 2, PREC, true><<<c.grid, 128, 0, c.stream>>>(p, a, s);
+    else k_tile<POT, INTER, MODE, 192, 2, PREC, true><<<c.grid, 192, 0, c.stream>>>(p, a, s);
+  }
 }
 
 template <int PREC>

@@ -436,10 +436,17 @@ int cr_batch_set_energy_costs(cr_batch* b, double ea, double el, double eb, doub
 int cr_batch_set_lj_cutoff(cr_batch* b, double LJcutoff);
 int cr_batch_set_attraction_constants(cr_batch* b, double l1, double l2);
 int cr_batch_set_precision(cr_batch* b, int precision);
-/* lanes per vertex of the batched tile kernel: 1, 2 or 4 */
+/* lanes per vertex of the batched tile kernel: 1, 2 or 4 (with that lane
+ * count's default tile: 128, 96 or 64 vertices) */
 int cr_batch_set_lanes(cr_batch* b, int lanes);
 int cr_batch_get_lanes(const cr_batch* b, int* lanes);
-/* times the batched FIRE force kernel for each admissible lane count and keeps the fastest */
+/* Tile shape of the batched tile kernel: (lanes per vertex, threads per CTA)
+ * in (1, 128), (1, 192), (2, 128), (2, 192), (4, 256); a tile holds
+ * threads / lanes vertices of whole rings of one system.  Rings longer than
+ * 128 vertices need (1, 192). */
+int cr_batch_set_tile_shape(cr_batch* b, int lanes, int block);
+int cr_batch_get_tile_shape(const cr_batch* b, int* lanes, int* block);
+/* times the batched FIRE force kernel for each admissible tile shape and keeps the fastest */
 int cr_batch_autotune(cr_batch* b, long reps, int* lanes_out);
 int cr_batch_profile_fire_tile(cr_batch* b, long reps, double* ms_per_launch);
 /* boxSizes[2 S] = {Lx_0, Ly_0, Lx_1, ...} */

@@ -182,6 +182,13 @@ def test_batch_autotune_and_lanes(cuda_device):
     f1 = b.getVertexForces()
     lanes = b.autotune(5)
     assert lanes in (1, 2, 4)
+    assert b.getTileShape() in [(1, 128), (1, 192), (2, 128), (2, 192), (4, 256)]
+    assert b.getTileShape()[0] == lanes
+    for shape in [(1, 128), (1, 192), (2, 128), (2, 192), (4, 256)]:
+        b.setTileShape(*shape)
+        assert b.getTileShape() == shape
+        b.calcForceEnergy()
+        assert rel_inf(b.getVertexForces(), f1) < 1e-12
     for L in (1, 2, 4):
         b.setLanes(L)
         b.calcForceEnergy()
