@@ -110,7 +110,9 @@ struct cr_ctx {
   double* diff_vec = nullptr; // [5][2 nv] CG vectors
   double* diff_area = nullptr; // [np][4] hyper-dual ring areas
   CgState* cg_state = nullptr;
-  double* cg_part = nullptr;   // [148][4] CG reduction partials
+  double* cg_part = nullptr;   // [148][8] CG reduction partials
+  double* cg_minv = nullptr;   // [nv][3] inverse diagonal Hessian blocks (block-Jacobi preconditioner)
+  int cg_precond = 1;          // 1: block-Jacobi preconditioner in cr_hessian_solve; 0: none
   int partials_n = 0;
   DevStatus* status = nullptr;
   DevStatus* status_h = nullptr;  // pinned
@@ -1095,7 +1097,7 @@ int cr_destroy(cr_ctx* ctx) {
                   ctx->cell_cnt, ctx->cell_start, ctx->cell_vid, ctx->cell_ring, ctx->cell_pos, ctx->cell_rad,
                   ctx->partials, ctx->status, ctx->fire_state, ctx->p_vel, ctx->p_force, ctx->p_angvel,
                   ctx->diff_f, ctx->diff_e, ctx->diff_dot, ctx->diff_vec, ctx->diff_area, ctx->cg_state,
-                  ctx->cg_part,
+                  ctx->cg_part, ctx->cg_minv,
                   ctx->p_torque, ctx->p_moi, ctx->v_torque, ctx->sp_angle, ctx->block_sum, ctx->cell_bucket, ctx->bucket_pos, ctx->bucket_rad,
                   ctx->bucket_ring, ctx->bucket_pq,
                   ctx->prad, ctx->plast, ctx->pid, ctx->pnbr, ctx->pnbr_cnt, ctx->pstatus, ctx->pfire, ctx->pdraws,
@@ -2034,7 +2036,7 @@ static int diff_ready(cr_ctx* ctx) {
     if ((rc = dalloc(ctx, &ctx->diff_f, (size_t)8 * ctx->nv)) || (rc = dalloc(ctx, &ctx->diff_e, (size_t)4 * ctx->nv)) ||
         (rc = dalloc(ctx, &ctx->diff_dot, 256)) || (rc = dalloc(ctx, &ctx->diff_vec, (size_t)10 * ctx->nv)) ||
         (rc = dalloc(ctx, &ctx->diff_area, (size_t)4 * ctx->np)) || (rc = dalloc(ctx, &ctx->cg_state, 1)) ||
-        (rc = dalloc(ctx, &ctx->cg_part, (size_t)4 * 148)))
+        (rc = dalloc(ctx, &ctx->cg_part, (size_t)8 * 148)) || (rc = dalloc(ctx, &ctx->cg_minv, (size_t)3 * ctx->nv)))
       return rc;
   }
   return CR_OK;
@@ -2195,19 +2197,37 @@ extern "C" int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double 
   double* r = xd + n;
   double* pv = r + n;
   double* hp = pv + n;
-  // conjugate gradients on the Hessian restricted to vectors without a
-  // uniform translation (its null space in a periodic box): b is projected,
-  // and each H p loses its mean, so every iterate stays in that subspace
+  double* zv = hp + n;
+  // preconditioned conjugate gradients on the Hessian restricted to vectors
+  // without a uniform translation (its null space in a periodic box): b is
+  // projected, each H p and each preconditioned residual lose their means,
+  // so every iterate stays in that subspace.  The preconditioner is
+  // block-Jacobi: the inverse 2 x 2 diagonal block of every vertex, from one
+  // hyper-dual launch seeding each vertex's own coordinates.
+  const double* minv = nullptr;
+  if (ctx->cg_precond) {
+    DiffArgs gd = diff_args(ctx);
+    gd.diag = 1;
+    launch_diff(ctx->stream, ctx->potential, inter_kind(ctx), gd, ctx->ring_first, ctx->ring_nv);
+    launch_cg_prec(ctx->stream, ctx->nv, ctx->diff_f, ctx->cg_minv);
+    ctx->launches += 3;
+    CR_TRY(cudaGetLastError());
+    minv = ctx->cg_minv;
+  }
   if ((rc = upload(ctx, r, b, (size_t)n * sizeof(double)))) return rc;
   if ((rc = dev_project(ctx, r))) return rc;
   CR_TRY(cudaMemsetAsync(xd, 0, (size_t)n * sizeof(double), ctx->stream));
-  CR_TRY(cudaMemcpyAsync(pv, r, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  double bb;
-  if ((rc = dev_dot(ctx, r, r, n, &bb))) return rc;
+  launch_cg_apply(ctx->stream, ctx->nv, minv, r, zv);
+  CR_TRY(cudaGetLastError());
+  if ((rc = dev_project(ctx, zv))) return rc;
+  CR_TRY(cudaMemcpyAsync(pv, zv, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  double bb, rz;
+  if ((rc = dev_dot(ctx, r, r, n, &bb)) || (rc = dev_dot(ctx, r, zv, n, &rz))) return rc;
   CgState cs;
   memset(&cs, 0, sizeof(cs));
   cs.rr = bb;
   cs.bb = bb;
+  cs.rz = rz;
   cs.tol = tol;
   cs.max_iters = maxIter;
   cs.done = (maxIter == 0 || !(bb > 0.0) || !(std::sqrt(cs.rr / bb) > tol)) ? 1 : 0;
@@ -2229,6 +2249,8 @@ extern "C" int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double 
   a.st = ctx->cg_state;
   a.partials = ctx->cg_part;
   a.nblk = cg_blocks(ctx->nv);
+  a.z = zv;
+  a.minv = minv;
   cudaGraphExec_t exec = nullptr;
   if (!cs.done) {
     cudaGraph_t graph = nullptr;
@@ -2258,6 +2280,32 @@ extern "C" int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double 
   if (iters) *iters = (long)cs.iters;
   if (relres) *relres = bb > 0.0 ? std::sqrt(cs.rr / bb) : 0.0;
   return download(ctx, x, xd, (size_t)n * sizeof(double));
+}
+
+int cr_hessian_diag_blocks(cr_ctx* ctx, double* out) {
+  if (!ctx || !out) return CR_EINVAL;
+  int rc;
+  if ((rc = diff_ready(ctx))) return rc;
+  DiffArgs gd = diff_args(ctx);
+  gd.diag = 1;
+  launch_diff(ctx->stream, ctx->potential, inter_kind(ctx), gd, ctx->ring_first, ctx->ring_nv);
+  ctx->launches += 2;
+  CR_TRY(cudaGetLastError());
+  std::vector<double> f((size_t)8 * ctx->nv);
+  if ((rc = download(ctx, f.data(), ctx->diff_f, f.size() * sizeof(double)))) return rc;
+  for (int v = 0; v < ctx->nv; v++) {
+    const double* q = f.data() + (size_t)8 * v;
+    out[3 * v] = -q[1];
+    out[3 * v + 1] = -0.5 * (q[2] + q[5]);
+    out[3 * v + 2] = -q[6];
+  }
+  return CR_OK;
+}
+
+int cr_set_cg_preconditioner(cr_ctx* ctx, int kind) {
+  if (!ctx || kind < 0 || kind > 1) return CR_EINVAL;
+  ctx->cg_precond = kind;
+  return CR_OK;
 }
 
 int cr_get_launch_count(const cr_ctx* ctx, long long* out) {

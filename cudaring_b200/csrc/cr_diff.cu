@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(64) k_ring_area_hd(const __grid_constant__ Dif
   const HD area = 0.5 * habs(sum);
   double* o = g.ring_area + (size_t)4 * q;
   o[0] = area.a;
-  o[1] = area.b;
+  o[1] = g.diag ? (sum.a >= 0.0 ? 1.0 : -1.0) : area.b;  // diag mode: the ring's orientation
   o[2] = area.c;
   o[3] = area.d;
 }
@@ -208,9 +208,15 @@ __global__ void __launch_bounds__(64) k_diff(const __grid_constant__ DiffArgs g)
   const int vp = at(k - 1), vn = at(k + 1), vpp = at(k - 2), vnn = at(k + 2);
 
   const double* ra = g.ring_area + (size_t)4 * ring;
-  const HD area{ra[0], ra[1], ra[2], ra[3]};
-  const HD2 x = load_x(g, v), xn = load_x(g, vn), xp = load_x(g, vp);
+  HD2 x = load_x(g, v);
+  const HD2 xn = load_x(g, vn), xp = load_x(g, vp);
+  if (g.diag) x = HD2{HD{x.x.a, 1.0, 0.0, 0.0}, HD{x.y.a, 0.0, 1.0, 0.0}};
   const HD2 ns = pbc2_hd(xn, x, bx), ps = pbc2_hd(x, xp, bx);
+  // ring area; with the own-vertex seeding its tangents are the shoelace
+  // derivatives dA/dx_v = s (y_next - y_prev) / 2, dA/dy_v = s (x_prev - x_next) / 2
+  // (s the ring's orientation), second derivative zero
+  const HD area = g.diag ? HD{ra[0], 0.5 * ra[1] * (ns.y.a + ps.y.a), -0.5 * ra[1] * (ns.x.a + ps.x.a), 0.0}
+                         : HD{ra[0], ra[1], ra[2], ra[3]};
   const HD2 pps = pbc2_hd(xp, load_x(g, vpp), bx), nns = pbc2_hd(load_x(g, vnn), xn, bx);
   const HD th = angle(ns, ps), thp = angle(ps, pps), thn = angle(nns, ns);
 
@@ -409,19 +415,19 @@ __global__ void __launch_bounds__(kCgBlock) k_cg_hp(const __grid_constant__ CgAr
   double out[3];
   cg_block_sums(acc, 3, out);
   if (threadIdx.x == 0)
-    for (int q = 0; q < 3; q++) a.partials[(size_t)4 * blockIdx.x + q] = out[q];
+    for (int q = 0; q < 3; q++) a.partials[(size_t)8 * blockIdx.x + q] = out[q];
 }
 
-// one thread: the mean of H p and the step alpha = |r|^2 / p.Hp (p carries no
+// one thread: the mean of H p and the step alpha = r.z / p.Hp (p carries no
 // translation, so p.Hp is the curvature along p of the projected Hessian)
 __global__ void k_cg_alpha(const __grid_constant__ CgArgs a) {
   CgState& st = *a.st;
   if (st.done) return;
   double sx = 0.0, sy = 0.0, php = 0.0;
   for (int b = 0; b < a.nblk; b++) {
-    sx += a.partials[4 * b];
-    sy += a.partials[4 * b + 1];
-    php += a.partials[4 * b + 2];
+    sx += a.partials[8 * b];
+    sy += a.partials[8 * b + 1];
+    php += a.partials[8 * b + 2];
   }
   st.mx = sx / a.nv;
   st.my = sy / a.nv;
@@ -430,49 +436,115 @@ __global__ void k_cg_alpha(const __grid_constant__ CgArgs a) {
     st.done = 1;
     return;
   }
-  st.alpha = st.rr / php;
+  st.alpha = st.rz / php;
 }
 
-// x += alpha p; r -= alpha (H p - mean); partials: |r|^2
+// z = M^-1 r at vertex v (2 x 2 block), or z = r without a preconditioner
+__device__ __forceinline__ double2 cg_precondition(const double* minv, int v, double rx, double ry) {
+  if (!minv) return make_double2(rx, ry);
+  const double* m = minv + (size_t)3 * v;
+  return make_double2(m[0] * rx + m[1] * ry, m[1] * rx + m[2] * ry);
+}
+
+// x += alpha p; r -= alpha (H p - mean); z = M^-1 r; partials: |r|^2, r.z,
+// sum z.x, sum z.y (one vertex, both components, per thread)
 __global__ void __launch_bounds__(kCgBlock) k_cg_update(const __grid_constant__ CgArgs a) {
   const CgState st = *(const CgState*)a.st;
   if (st.done) return;
-  double acc[1] = {0.0};
-  for (int i = blockIdx.x * kCgBlock + threadIdx.x; i < 2 * a.nv; i += a.nblk * kCgBlock) {
-    const double m = (i & 1) ? st.my : st.mx;
-    a.x[i] += st.alpha * a.p[i];
-    const double r = a.r[i] - st.alpha * (a.hp[i] - m);
-    a.r[i] = r;
-    acc[0] += r * r;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int v = blockIdx.x * kCgBlock + threadIdx.x; v < a.nv; v += a.nblk * kCgBlock) {
+    a.x[2 * v] += st.alpha * a.p[2 * v];
+    a.x[2 * v + 1] += st.alpha * a.p[2 * v + 1];
+    const double rx = a.r[2 * v] - st.alpha * (a.hp[2 * v] - st.mx);
+    const double ry = a.r[2 * v + 1] - st.alpha * (a.hp[2 * v + 1] - st.my);
+    a.r[2 * v] = rx;
+    a.r[2 * v + 1] = ry;
+    const double2 z = cg_precondition(a.minv, v, rx, ry);
+    a.z[2 * v] = z.x;
+    a.z[2 * v + 1] = z.y;
+    acc[0] += rx * rx + ry * ry;
+    acc[1] += rx * z.x + ry * z.y;
+    acc[2] += z.x;
+    acc[3] += z.y;
   }
-  double out[1];
-  cg_block_sums(acc, 1, out);
-  if (threadIdx.x == 0) a.partials[(size_t)4 * blockIdx.x + 3] = out[0];
+  double out[4];
+  cg_block_sums(acc, 4, out);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < 4; q++) a.partials[(size_t)8 * blockIdx.x + 3 + q] = out[q];
 }
 
-// one thread: the new |r|^2, beta, the iteration count and the stop tests of
-// the host loop (relative residual, iteration limit)
+// one thread: the new |r|^2 and r.z, beta = r.z / previous r.z, the mean of
+// z, the iteration count and the stop tests of the host loop (relative
+// residual, iteration limit)
 __global__ void k_cg_beta(const __grid_constant__ CgArgs a) {
   CgState& st = *a.st;
   if (st.done) return;
-  double rr2 = 0.0;
-  for (int b = 0; b < a.nblk; b++) rr2 += a.partials[4 * b + 3];
-  st.beta = rr2 / st.rr;
+  double rr2 = 0.0, rz2 = 0.0, zx = 0.0, zy = 0.0;
+  for (int b = 0; b < a.nblk; b++) {
+    rr2 += a.partials[8 * b + 3];
+    rz2 += a.partials[8 * b + 4];
+    zx += a.partials[8 * b + 5];
+    zy += a.partials[8 * b + 6];
+  }
+  st.beta = rz2 / st.rz;
+  st.rz = rz2;
   st.rr = rr2;
+  st.zx = zx / a.nv;
+  st.zy = zy / a.nv;
   st.iters += 1;
   if (!(sqrt(st.rr / st.bb) > st.tol) || st.iters >= st.max_iters) st.done = 1;
 }
 
-// p = r + beta p
+// p = (z - mean z) + beta p: the preconditioned residual without its
+// translation (r carries none, so r.z needs no correction)
 __global__ void __launch_bounds__(kCgBlock) k_cg_direction(const __grid_constant__ CgArgs a) {
   const CgState st = *(const CgState*)a.st;
   if (st.done) return;
   for (int i = blockIdx.x * kCgBlock + threadIdx.x; i < 2 * a.nv; i += a.nblk * kCgBlock)
-    a.p[i] = a.r[i] + st.beta * a.p[i];
+    a.p[i] = (a.z[i] - ((i & 1) ? st.zy : st.zx)) + st.beta * a.p[i];
+}
+
+// inverse diagonal blocks from a diag-mode launch: H_vv = -[[Fx.b, Fx.c],
+// [Fy.b, Fy.c]] symmetrised; where it is not positive definite, the inverse
+// of its diagonal's magnitudes (floored at 1e-3 of the larger), and the
+// identity for a zero block
+__global__ void k_cg_prec(int nv, const double* fhd, double* minv) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const double* f = fhd + (size_t)8 * v;
+  const double h11 = -f[1], h22 = -f[6], h12 = -0.5 * (f[2] + f[5]);
+  const double det = h11 * h22 - h12 * h12;
+  double* m = minv + (size_t)3 * v;
+  if (h11 > 0.0 && h22 > 0.0 && det > 1e-12 * h11 * h22) {
+    m[0] = h22 / det;
+    m[1] = -h12 / det;
+    m[2] = h11 / det;
+  } else {
+    const double s = fmax(fabs(h11), fabs(h22));
+    m[0] = s > 0.0 ? 1.0 / fmax(fabs(h11), 1e-3 * s) : 1.0;
+    m[1] = 0.0;
+    m[2] = s > 0.0 ? 1.0 / fmax(fabs(h22), 1e-3 * s) : 1.0;
+  }
+}
+
+__global__ void k_cg_apply(int nv, const double* minv, const double* r, double* z) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const double2 q = cg_precondition(minv, v, r[2 * v], r[2 * v + 1]);
+  z[2 * v] = q.x;
+  z[2 * v + 1] = q.y;
 }
 }  // namespace
 
-int cg_blocks(int nv) { return std::max(1, std::min(148, (2 * nv + kCgBlock - 1) / kCgBlock)); }
+int cg_blocks(int nv) { return std::max(1, std::min(148, (nv + kCgBlock - 1) / kCgBlock)); }
+
+void launch_cg_prec(cudaStream_t st, int nv, const double* fhd, double* minv) {
+  k_cg_prec<<<(nv + 127) / 128, 128, 0, st>>>(nv, fhd, minv);
+}
+
+void launch_cg_apply(cudaStream_t st, int nv, const double* minv, const double* r, double* z) {
+  k_cg_apply<<<(nv + 127) / 128, 128, 0, st>>>(nv, minv, r, z);
+}
 
 void launch_cg_iteration(cudaStream_t st, const CgArgs& a) {
   k_cg_hp<<<a.nblk, kCgBlock, 0, st>>>(a);

@@ -101,6 +101,10 @@ struct DiffArgs {
   double* energy_out;  // [nv][4]
   double* ring_area;   // [np][4] scratch: hyper-dual ring areas (filled by the launch)
   const int* skip;     // nullable: nothing is evaluated while *skip != 0
+  // 1: each thread seeds its own vertex only (x tangent e1, y tangent e2;
+  // t1, t2 null), so the e1 and e2 parts of the force on v are the columns
+  // of -H_vv, the vertex's 2 x 2 diagonal block of the Hessian
+  int diag;
 };
 void launch_diff(cudaStream_t st, int pot, int inter, const DiffArgs& g, const int* ring_first, const int* ring_nv);
 // Device-resident conjugate-gradient iterations on the projected Hessian
@@ -113,6 +117,8 @@ struct CgState {
   long long iters, max_iters;
   int done;               // converged, iteration limit, or non-positive curvature
   int bad;                // 1: a non-positive curvature p.Hp was met
+  double rz;              // r.z with z = M^-1 r (the preconditioned residual; = |r|^2 without one)
+  double zx, zy;          // mean of z over the vertices (removed: translations)
 };
 struct CgArgs {
   int nv;
@@ -122,10 +128,17 @@ struct CgArgs {
   double* hp;
   const double* fhd;  // hyper-dual forces of the H p launch
   CgState* st;
-  double* partials;   // [nblk][4]
+  double* partials;   // [nblk][8]
   int nblk;
+  double* z;          // preconditioned residual M^-1 r
+  const double* minv; // [nv][3] inverse diagonal blocks (a, b, d of [[a, b], [b, d]]); null: no preconditioner
 };
 void launch_cg_iteration(cudaStream_t st, const CgArgs& a);
+// Block-Jacobi preconditioner from a diag-mode hyper-dual launch: minv[v] the
+// inverse of the vertex's 2 x 2 Hessian block (its positive part where the
+// block is not positive definite); z = M^-1 r.
+void launch_cg_prec(cudaStream_t st, int nv, const double* fhd, double* minv);
+void launch_cg_apply(cudaStream_t st, int nv, const double* minv, const double* r, double* z);
 int cg_blocks(int nv);
 void launch_dot_partials(cudaStream_t st, int n, const double* a, const double* b, double* out, int nblocks);
 void launch_axpby(cudaStream_t st, int n, double a, const double* x, double b, double* y);

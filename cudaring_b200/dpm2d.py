@@ -234,6 +234,16 @@ class DPM2D:
                    dF.ctypes.data, dPdx.ctypes.data)
         return dU.value, dP.value, dF, dPdx
 
+    def hessianDiagBlocks(self):
+        """(Nv, 3) array of the Hessian's 2 x 2 vertex blocks (xx, xy, yy)."""
+        out = np.empty(3 * self.numVertices)
+        self._call("cr_hessian_diag_blocks", out.ctypes.data)
+        return out.reshape(-1, 3)
+
+    def setCGPreconditioner(self, kind):
+        """Preconditioner of hessianSolve: "block_jacobi" (default) or "none"."""
+        self._call("cr_set_cg_preconditioner", {"none": 0, "block_jacobi": 1}.get(kind, kind))
+
     def hessianSolve(self, b, tol=1e-10, maxIter=100000):
         x = np.empty(2 * self.numVertices)
         it, rr = C.c_long(), C.c_double()

@@ -410,9 +410,17 @@ int cr_calc_pressure(cr_ctx* ctx, double* P);
 int cr_param_derivatives(cr_ctx* ctx, int param, double* dU, double* dP, double* dF, double* dPdx);
 /* conjugate-gradient solve of H x = b (H the Hessian at the current
  * positions) on the complement of the uniform translations, to relative
- * residual tol */
+ * residual tol; preconditioned (cr_set_cg_preconditioner) */
 int cr_hessian_solve(cr_ctx* ctx, const double* b, double* x, double tol, long maxIter, long* iterations,
                      double* relres);
+/* No reference counterpart.  Preconditioner of cr_hessian_solve: 1
+ * (default) block-Jacobi, the inverse 2 x 2 diagonal Hessian block of every
+ * vertex (its diagonal's magnitudes where the block is not positive
+ * definite); 0 none. */
+int cr_set_cg_preconditioner(cr_ctx* ctx, int kind);
+/* No reference counterpart.  The 2 x 2 diagonal blocks of the Hessian,
+ * d2U / dx_v dx_v: out[3 v .. 3 v + 2] = (xx, xy, yy) for every vertex. */
+int cr_hessian_diag_blocks(cr_ctx* ctx, double* out);
 
 /* ---- batches of independent systems -------------------------------------
  * No single reference counterpart: the reference holds one system per process

@@ -170,7 +170,8 @@ def test_parameter_derivatives(cuda_device, param):
     assert float(dPdx @ w) == pytest.approx((P2[0] - P2[1]) / (2 * h), rel=1e-5, abs=1e-8)
 
 
-def test_hessian_solve(cuda_device):
+@pytest.mark.parametrize("precond", ["block_jacobi", "none"])
+def test_hessian_solve(cuda_device, precond):
     d, pk, args = _system(n=16, phi=0.80, seed=6)
     # minimise so that H is positive on the complement of the translations
     d.initFIRE([0.2, 0.5, 1.1, 0.99, 1e-2, 1e-1, 0.2], 20, 0, d.numVertices)
@@ -180,10 +181,28 @@ def test_hessian_solve(cuda_device):
     # a right-hand side in the range of H (rings without contacts add zero
     # modes beyond the uniform translations)
     b = d.hvp(np.random.default_rng(3).normal(size=2 * d.numVertices))
+    d.setCGPreconditioner(precond)
     x, it, rr = d.hessianSolve(b, 1e-10, 200000)
     assert rr <= 1e-10
     hx = d.hvp(x)
     assert np.linalg.norm(hx - b) / np.linalg.norm(b) < 1e-8
+
+
+@pytest.mark.parametrize("interaction,potential", [("vertexVertex", "harmonic"), ("vertexSmooth", "lennardJones"),
+                                                   ("vertexSmooth", "harmonic")])
+def test_hessian_diag_blocks_match_hvp(cuda_device, interaction, potential):
+    # the block-Jacobi preconditioner's 2 x 2 blocks (one hyper-dual launch,
+    # each thread seeding its own vertex) against H e for unit vectors e
+    d, pk, args = _system(n=16, phi=0.80, seed=9, interaction=interaction, potential=potential)
+    blocks = d.hessianDiagBlocks()
+    nv = d.numVertices
+    for v in (0, 7, nv // 2, nv - 1):
+        for c in (0, 1):
+            e = np.zeros(2 * nv)
+            e[2 * v + c] = 1.0
+            col = d.hvp(e)[2 * v:2 * v + 2]
+            want = blocks[v, [0, 1]] if c == 0 else blocks[v, [1, 2]]
+            assert np.allclose(col, want, rtol=1e-10, atol=1e-10 * np.abs(blocks).max())
 
 
 class MinimizedEnergyPressure(torch.autograd.Function):
