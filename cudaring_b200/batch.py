@@ -182,6 +182,10 @@ class Batch:
         self._call(fn, C.byref(prm), phi.ctypes.data, steps.ctypes.data, state.ctypes.data, iters.ctypes.data)
         return {"phi": phi, "steps": steps, "state": state, "fire_iterations": iters}
 
+    def setPersistent(self, on):
+        """Persistent FIRE kernel for batches that fit the GPU at once (default on)."""
+        self._call("cr_batch_set_persistent", int(bool(on)))
+
     def getListCapacity(self):
         out = C.c_int()
         self._call("cr_batch_get_list_capacity", C.byref(out))

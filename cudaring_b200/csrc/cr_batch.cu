@@ -25,6 +25,7 @@
 #include <string>
 #include <vector>
 
+#include "cr_bfire.cuh"
 #include "cr_launch.h"
 #include "cr_tile.cuh"
 
@@ -95,6 +96,11 @@ struct cr_batch {
   int *sys_nv_d = nullptr, *sys_r0_d = nullptr, *sys_np_d = nullptr, *cells0_d = nullptr;
   cudaStream_t cap_s2 = nullptr, cap_s3 = nullptr;  // capture streams of the nested loop bodies
   cudaGraphExec_t comp_exec = nullptr;
+  // persistent batched FIRE (k_bfire_steps): off by request or after a
+  // grid-barrier wait gave up; the chunk graph of the current list capacity
+  bool no_persist = false;
+  std::map<BFireStepsFn, int> persist_max;  // CTAs each kernel holds resident at once
+  cudaGraphExec_t pchunk = nullptr;
   std::map<std::pair<long, int>, cudaGraphExec_t> graphs;  // (iterations, cap) -> FIRE chunk
   long long launches = 0;
   std::string err;
@@ -257,85 +263,13 @@ __global__ void __launch_bounds__(256) k_bnbr(const __grid_constant__ BNbr n) {
   }
 }
 
-struct BFire {
-  double2* pos;
-  double2* vel;
-  const double2* force;
-  const double2* last_pos;
-  const int* vsys;
-  const int* sys_v0;
-  BatchSys* bsys;
-  double* bfire;
-  FireParams fp;
-  DevStatus* st;
-  int nv;
-  int use_cond;
-  cudaGraphConditionalHandle cond;
-};
-
 // FIRE iteration up to the position update, per system (the single-system
 // k_fire_pre: FIRE::minimizerVertexLoop, src/FIRE.cu:338-406) with each
-// system's own scalars, sums and convergence.
+// system's own scalars, sums and convergence (bfire_prekick, cr_bfire.cuh).
 __global__ void __launch_bounds__(256) k_bfire_pre(const __grid_constant__ BFire f) {
   DevStatus* st = f.st;
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
-  if (!st->abort && v < f.nv) {
-    const int s = f.vsys[v];
-    BatchSys& bs = f.bsys[s];
-    if (bs.active && !bs.converged && bs.fire_cap > 0 && bs.fire_iters >= bs.fire_cap) {
-      // iteration limit of this run: the system stops as if converged (its
-      // tiles skip the force op that follows)
-      if (v == f.sys_v0[s]) bs.converged = 1;
-    } else if (bs.active && !bs.converged) {
-      const long long it = bs.fire_iters;
-      const double* cur = f.bfire + ((size_t)s * 2 + (it & 1)) * 4;
-      double dt = cur[0], alpha = cur[1];
-      long long nstep = (long long)cur[2];
-      const double dt_max = cur[3];  // the system's own bound (10 x its starting dt in the reference drivers)
-      const double P = bs.sums[S_VF], vv = bs.sums[S_VV], ff = bs.sums[S_FF];
-      bool rollback = false;
-      if (P > 0) {
-        nstep++;
-        if (nstep > f.fp.min_step) {
-          dt = fmin(dt * f.fp.f_inc, dt_max);
-          alpha *= f.fp.f_a;
-        }
-      } else {
-        nstep = 0;
-        dt = fmax(dt * f.fp.f_dec, dt_max / 10);
-        alpha = f.fp.a_start;
-        rollback = true;
-      }
-      if (v == f.sys_v0[s]) {
-        double* nxt = f.bfire + ((size_t)s * 2 + ((it + 1) & 1)) * 4;
-        nxt[0] = dt;
-        nxt[1] = alpha;
-        nxt[2] = (double)nstep;
-        nxt[3] = dt_max;
-      }
-      const double h = 0.5 * dt;
-      const double vpost2 = rollback ? (h * h) * ff : vv + dt * P + (h * h) * ff;
-      double2 x = f.pos[v];
-      double2 vel = f.vel[v];
-      const double2 fv = f.force[v];
-      if (rollback) {
-        x = make_double2(x.x - h * vel.x, x.y - h * vel.y);
-        vel = make_double2(0.0, 0.0);
-      }
-      vel = make_double2(vel.x + h * fv.x, vel.y + h * fv.y);
-      if (ff > 0) {
-        const double ratio = sqrt(vpost2 / ff);
-        vel = make_double2((1 - alpha) * vel.x + alpha * fv.x * ratio, (1 - alpha) * vel.y + alpha * fv.y * ratio);
-      }
-      x = make_double2(x.x + dt * vel.x, x.y + dt * vel.y);
-      f.pos[v] = x;
-      f.vel[v] = vel;
-      if (3.0 * dist_of(pbc2(bs.box, x, f.last_pos[v])) > bs.disp_cutoff) {
-        bs.rebuild = 1;
-        st->rebuild = 1;
-      }
-    }
-  }
+  if (!st->abort && v < f.nv) bfire_prekick(f, v);
   if (is_last_block(st)) {
     if (threadIdx.x == 0) {
       st->done_ctr = 0;
@@ -552,6 +486,8 @@ __global__ void k_cclear(DevStatus* st) {
   st->nonfinite = 0;
   st->converged = 0;
   st->done_ctr = 0;
+  st->pbar = 0;
+  st->bpending = 0;
 }
 
 // Loop condition of the FIRE chunks: a system still running and no abort.
@@ -675,6 +611,8 @@ void drop_graphs(cr_batch* b) {
   b->graphs.clear();
   if (b->comp_exec) cudaGraphExecDestroy(b->comp_exec);
   b->comp_exec = nullptr;
+  if (b->pchunk) cudaGraphExecDestroy(b->pchunk);
+  b->pchunk = nullptr;
 }
 
 int read_status(cr_batch* b) { return download(b, b->status_h, b->status, sizeof(DevStatus)); }
@@ -850,6 +788,9 @@ int clear_flags(cr_batch* b) {
   b->status_h->nonfinite = 0;
   b->status_h->converged = 0;
   b->status_h->done_ctr = 0;
+  b->status_h->pbar = 0;
+  b->status_h->bpending = 0;
+  b->status_h->stalled = 0;
   return write_status(b);
 }
 
@@ -940,6 +881,24 @@ int reduce_sys(cr_batch* b, int set_converged, cudaStream_t st = nullptr) {
 // One FIRE iteration over every unconverged system: pre-kick (with the
 // displacement check), conditional rebuild of the flagged systems, force +
 // second kick with per-system sums and convergence.
+BFire bfire_args(cr_batch* b, bool use_cond, cudaGraphConditionalHandle h) {
+  BFire f;
+  f.pos = b->pos;
+  f.vel = b->vel;
+  f.force = b->force;
+  f.last_pos = b->last_pos;
+  f.vsys = b->vsys;
+  f.sys_v0 = b->sys_v0_d;
+  f.bsys = b->bsys;
+  f.bfire = b->bfire;
+  f.fp = b->fp;
+  f.st = b->status;
+  f.nv = b->nv;
+  f.use_cond = use_cond ? 1 : 0;
+  f.cond = h;
+  return f;
+}
+
 void enqueue_fire_iteration(cr_batch* b, cudaStream_t st, bool use_cond, cudaGraphConditionalHandle h) {
   BFire f;
   f.pos = b->pos;
@@ -998,6 +957,80 @@ int add_fire_iterations(cr_batch* b, cudaStream_t st, cudaStream_t side, cudaGra
   return CR_OK;
 }
 
+// The persistent FIRE kernel of the batch's configuration, when it has one
+// and the GPU holds all of its CTAs at once; *block its CTA size.
+BFireStepsFn persist_fn(cr_batch* b, int* block) {
+  if (b->no_persist || b->precision != CR_PRECISION_FP64) return nullptr;
+  const int bl = batch_tile_block(b->lanes, b->block);
+  BFireStepsFn fn = bfire_steps_fn(b->potential, inter_kind(b), b->lanes, bl);
+  if (!fn) return nullptr;
+  auto it = b->persist_max.find(fn);
+  if (it == b->persist_max.end()) it = b->persist_max.emplace(fn, bfire_steps_max_blocks(fn, bl)).first;
+  if ((int)b->tiles_h.size() > it->second) return nullptr;
+  *block = bl;
+  return fn;
+}
+
+// FIRE iterations with the persistent kernel onto stream st (capturing into
+// graph g): `launches` launches of up to 64 iterations, each followed by a
+// conditional rebuild (body captured on side) that runs when the launch
+// left with a system's displacement check fired, then one launch that only
+// completes a force op left pending, so the chunk ends on a whole iteration.
+int add_fire_persistent(cr_batch* b, cudaStream_t st, cudaStream_t side, cudaGraph_t g, int launches,
+                        BFireStepsFn fn, int block) {
+  StepArgs s = step_args(b);
+  s.kind = KIND_FIRE;
+  s.advance = 0;
+  s.accumulate = 1;
+  s.write_out = 1;
+  s.use_cond = 0;
+  const SysParams p = with_f32_constants(b->p);
+  for (int i = 0; i < launches; i++) {
+    cudaGraphConditionalHandle h = 0;
+    BT_TRY(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    launch_bfire_steps(fn, tile_cfg(b, st), block, p, arrays(b), s, bfire_args(b, true, h), 64);
+    b->launches++;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    BT_TRY(cudaStreamGetCaptureInfo(st, &cs, nullptr, &cg, &deps, &ndeps));
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    BT_TRY(cudaGraphAddNode(&node, cg, deps, ndeps, &cp));
+    BT_TRY(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    BT_TRY(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    enqueue_build(b, side, 0);
+    cudaGraph_t body_out;
+    BT_TRY(cudaStreamEndCapture(side, &body_out));
+  }
+  launch_bfire_steps(fn, tile_cfg(b, st), block, p, arrays(b), s, bfire_args(b, false, 0), 0);
+  b->launches++;
+  BT_TRY(cudaGetLastError());
+  return CR_OK;
+}
+
+int capture_fire_persistent(cr_batch* b, BFireStepsFn fn, int block, cudaGraphExec_t* out) {
+  cudaGraph_t graph;
+  BT_TRY(cudaGraphCreate(&graph, 0));
+  BT_TRY(cudaStreamBeginCaptureToGraph(b->stream, graph, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const int rc = add_fire_persistent(b, b->stream, b->side, graph, 4, fn, block);
+  cudaGraph_t g;
+  const cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  if (rc) {
+    cudaGraphDestroy(graph);
+    return rc;
+  }
+  BT_TRY(e);
+  BT_TRY(cudaGraphInstantiate(out, g, 0));
+  cudaGraphDestroy(g);
+  return CR_OK;
+}
+
 int capture_fire_chunk(cr_batch* b, long n, cudaGraphExec_t* out) {
   cudaGraph_t graph;
   BT_TRY(cudaGraphCreate(&graph, 0));
@@ -1050,6 +1083,41 @@ int fire_loop(cr_batch* b, long maxIter, long* done_out) {
   int rc;
   long done = 0;
   const long chunk = 64;
+  if (maxIter <= 0) {
+    if (done_out) *done_out = 0;
+    return CR_OK;
+  }
+  // persistent FIRE: chunks of up to 4 x 64 iterations; every system stops at
+  // its iteration limit (fire_cap, set by the caller), so the loop ends when
+  // every system has converged or reached it
+  int block = 0;
+  while (BFireStepsFn fn = persist_fn(b, &block)) {
+    if ((rc = pull_sys(b))) return rc;
+    bool any = false;
+    for (const BatchSys& s : b->bsys_h) any = any || (s.active && !s.converged);
+    if (!any) {
+      if (done_out) *done_out = maxIter;
+      return CR_OK;
+    }
+    if ((rc = snapshot(b, false))) return rc;
+    if (!b->pchunk && (rc = capture_fire_persistent(b, fn, block, &b->pchunk))) return rc;
+    BT_TRY(cudaGraphLaunch(b->pchunk, b->stream));
+    if ((rc = read_status(b))) return rc;
+    if (b->status_h->abort) {
+      if (b->status_h->nonfinite) return b->fail(CR_ENONFINITE, "non-finite force in a batched FIRE run");
+      if ((rc = snapshot(b, true))) return rc;
+      if (b->status_h->stalled) {
+        // a grid-barrier wait gave up: one launch per op from here on
+        b->no_persist = true;
+        drop_graphs(b);
+      } else if (b->status_h->overflow) {
+        if ((rc = alloc_lists(b, (int)pow2ceil(2LL * b->status_h->max_count)))) return rc;
+      } else {
+        return b->fail(CR_ECUDA, "batched FIRE chunk aborted");
+      }
+      if ((rc = fire_prologue(b))) return rc;  // same state, fresh lists, sums and flags
+    }
+  }
   while (done < maxIter) {
     if ((rc = pull_sys(b))) return rc;
     bool any = false;
@@ -1182,7 +1250,9 @@ int compress_body(cr_batch* b, CompArgs a, cudaGraph_t outer_body) {
   cudaGraph_t inner_body;
   if ((rc = add_while(b, s2, a.inner, &inner_body))) return rc;
   BT_TRY(cudaStreamBeginCaptureToGraph(s3, inner_body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  rc = add_fire_iterations(b, s3, b->side, inner_body, 64);
+  int block = 0;
+  if (BFireStepsFn fn = persist_fn(b, &block)) rc = add_fire_persistent(b, s3, b->side, inner_body, 4, fn, block);
+  else rc = add_fire_iterations(b, s3, b->side, inner_body, 64);
   if (!rc) k_cfire_more<<<1, 256, 0, s3>>>(a);
   cudaGraph_t ib_out;
   const cudaError_t e = cudaStreamEndCapture(s3, &ib_out);
@@ -1319,11 +1389,13 @@ int compress_device(cr_batch* b, const cr_compress_params* prm, double* phiOut, 
     if ((rc = read_status(b))) return rc;
     if (!b->status_h->abort) break;
     if (b->status_h->nonfinite) return b->fail(CR_ENONFINITE, "non-finite force in a batched compression");
-    if (!b->status_h->overflow || attempt >= 8) return b->fail(CR_ECUDA, "batched compression aborted");
+    if ((!b->status_h->overflow && !b->status_h->stalled) || attempt >= 8)
+      return b->fail(CR_ECUDA, "batched compression aborted");
     const size_t v2 = (size_t)b->nv * sizeof(double2);
     BT_TRY(cudaMemcpyAsync(b->pos, b->snap_pos, v2, cudaMemcpyDeviceToDevice, b->stream));
     BT_TRY(cudaMemcpyAsync(b->vel, b->snap_vel, v2, cudaMemcpyDeviceToDevice, b->stream));
-    if ((rc = alloc_lists(b, (int)pow2ceil(2LL * b->status_h->max_count)))) return rc;
+    if (b->status_h->stalled) b->no_persist = true;  // a grid-barrier wait gave up: one launch per op
+    else if ((rc = alloc_lists(b, (int)pow2ceil(2LL * b->status_h->max_count)))) return rc;
     if ((rc = clear_flags(b))) return rc;
   }
   drop_graphs(b);
@@ -1756,12 +1828,15 @@ int cr_batch_fire_minimize(cr_batch* b, const double* tol, long maxIter, long* i
     b->bsys_h[s].rebuild = 0;
     b->bsys_h[s].done_ctr = 0;
     it0[s] = b->bsys_h[s].fire_iters;
+    b->bsys_h[s].fire_cap = it0[s] + maxIter;  // every system stops after maxIter iterations
   }
   if ((rc = push_sys(b))) return rc;
   if ((rc = refresh_radius_stats(b)) || (rc = apply_cutoffs(b))) return rc;
   if ((rc = fire_prologue(b))) return rc;
   if ((rc = fire_loop(b, maxIter, nullptr))) return rc;
   if ((rc = reduce_sys(b, 0)) || (rc = pull_sys(b))) return rc;
+  for (BatchSys& bs : b->bsys_h) bs.fire_cap = 0;
+  if ((rc = push_sys(b))) return rc;
   for (int s = 0; s < b->S; s++) {
     if (iterations) iterations[s] = (long)(b->bsys_h[s].fire_iters - it0[s]);
     if (maxForce) maxForce[s] = std::sqrt(b->bsys_h[s].sums[S_FMAX2]);
@@ -1976,6 +2051,13 @@ int cr_batch_autotune(cr_batch* b, long reps, int* lanes_out) {
   }
   if ((rc = cr_batch_set_tile_shape(b, best_l, best_b))) return rc;
   if (lanes_out) *lanes_out = best_l;
+  return CR_OK;
+}
+
+int cr_batch_set_persistent(cr_batch* b, int on) {
+  if (!b) return CR_EINVAL;
+  b->no_persist = !on;
+  drop_graphs(b);
   return CR_OK;
 }
 

@@ -226,6 +226,8 @@ struct DevStatus {
   int pflag[3];
   long long pbase;
   long long steps_left;
+  // persistent batched FIRE: the last launch left with its force op due
+  int bpending;
   // polls a grid-barrier wait makes before it gives up (0: 2^20, about a
   // second; negative: none, the first poll that finds the barrier incomplete
   // gives up)

@@ -197,10 +197,12 @@ __device__ __forceinline__ void smooth_slot_f64(const SysParams& p, const B& bx,
 
 // One step (or force evaluation) of one tile.  pin / pout: positions read
 // and written; step: the integrator step index (Philox stream of the noise).
-// PERSIST (the multi-step kernel): a rebuild due or a non-finite force is
-// reported in *pflag instead of the status block, and the last-block
-// protocol is left to the caller.
-template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH, bool PERSIST>
+// PERSIST: 0 for one op per launch; 1 the multi-step kernel: positions
+// read with plain loads (other CTAs rewrite them between steps), a rebuild
+// due or a non-finite force reported in *pflag instead of the status block,
+// and the last-block protocol left to the caller; 2 the persistent batched
+// FIRE kernel: plain position loads, everything else as for one op.
+template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH, int PERSIST>
 __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a, const StepArgs& s,
                                           const double2* __restrict__ pin, double2* __restrict__ pout,
                                           unsigned long long step, int* pflag) {
@@ -253,7 +255,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
       cp_async_commit();
     }
     const int2 tp = __ldg(a.vtopo + v);
-    s_pos[t] = ld_pos<PERSIST>(pin + v);
+    s_pos[t] = ld_pos<(PERSIST != 0)>(pin + v);
     const double l0v = __ldg(a.l0 + v);
     s_l0[t] = l0v;
     s_il0[t] = 1.0 / l0v;
@@ -384,7 +386,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         double2 nxj = make_double2(0.0, 0.0);
         double nr = 0.0;
         if (sl < cnt) {
-          nxj = ld_pos<PERSIST>(pin + jn);
+          nxj = ld_pos<(PERSIST != 0)>(pin + jn);
           nr = __ldg(a.rad + jn);
         }
         while (sl < cnt) {
@@ -392,7 +394,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
           const double rj = nr;
           sl += L;
           if (sl < cnt) {
-            nxj = ld_pos<PERSIST>(pin + j2);
+            nxj = ld_pos<(PERSIST != 0)>(pin + j2);
             nr = __ldg(a.rad + j2);
             if (sl + L < cnt) j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
           }
@@ -411,9 +413,9 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         double2 nxj = make_double2(0.0, 0.0), nxjq = nxj, nxjqq = nxj;
         double nr = 0.0;
         if (sl < cnt) {
-          nxj = ld_pos<PERSIST>(pin + jn);
-          nxjq = ld_pos<PERSIST>(pin + jn + pq_first(pkn));
-          nxjqq = ld_pos<PERSIST>(pin + jn + pq_second(pkn));
+          nxj = ld_pos<(PERSIST != 0)>(pin + jn);
+          nxjq = ld_pos<(PERSIST != 0)>(pin + jn + pq_first(pkn));
+          nxjqq = ld_pos<(PERSIST != 0)>(pin + jn + pq_second(pkn));
           nr = __ldg(a.rad + jn);
         }
         while (sl < cnt) {
@@ -421,9 +423,9 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
           const double rj = nr;
           sl += L;
           if (sl < cnt) {
-            nxj = ld_pos<PERSIST>(pin + j2);
-            nxjq = ld_pos<PERSIST>(pin + j2 + pq_first(pk2));
-            nxjqq = ld_pos<PERSIST>(pin + j2 + pq_second(pk2));
+            nxj = ld_pos<(PERSIST != 0)>(pin + j2);
+            nxjq = ld_pos<(PERSIST != 0)>(pin + j2 + pq_first(pk2));
+            nxjqq = ld_pos<(PERSIST != 0)>(pin + j2 + pq_second(pk2));
             nr = __ldg(a.rad + j2);
             if (sl + L < cnt) {
               j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
@@ -450,8 +452,8 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
             j1 = __ldg(a.nbr + (size_t)(s0 + L) * stride + i);
             pk1 = __ldg(a.nbr_pq + (size_t)(s0 + L) * stride + i);
           }
-          double2 xj = ld_pos<PERSIST>(pin + j0), xjq = ld_pos<PERSIST>(pin + j0 + pq_first(pk0)),
-                  xjqq = ld_pos<PERSIST>(pin + j0 + pq_second(pk0));
+          double2 xj = ld_pos<(PERSIST != 0)>(pin + j0), xjq = ld_pos<(PERSIST != 0)>(pin + j0 + pq_first(pk0)),
+                  xjqq = ld_pos<(PERSIST != 0)>(pin + j0 + pq_second(pk0));
           double rj = __ldg(a.rad + j0);
           while (true) {
             const int s1 = s0 + L;
@@ -463,9 +465,9 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
                 j2 = __ldg(a.nbr + (size_t)(s1 + L) * stride + i);
                 pk2 = __ldg(a.nbr_pq + (size_t)(s1 + L) * stride + i);
               }
-              nxj = ld_pos<PERSIST>(pin + j1);
-              nxjq = ld_pos<PERSIST>(pin + j1 + pq_first(pk1));
-              nxjqq = ld_pos<PERSIST>(pin + j1 + pq_second(pk1));
+              nxj = ld_pos<(PERSIST != 0)>(pin + j1);
+              nxjq = ld_pos<(PERSIST != 0)>(pin + j1 + pq_first(pk1));
+              nxjqq = ld_pos<(PERSIST != 0)>(pin + j1 + pq_second(pk1));
               nr = __ldg(a.rad + j1);
             }
             if (mixed_slot_f32<POT>(p, bx, xi, seg_i64, seg_i, pseg_i, len2_i, len_i, ri, rj, xj, xjq, xjqq, fi64,
@@ -488,8 +490,8 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
               const int s = base + (__ffsll((long long)late) - 1) * L;
               const int j = __ldg(a.nbr + (size_t)s * stride + i), pk = __ldg(a.nbr_pq + (size_t)s * stride + i);
               smooth_slot_f64<POT>(p, bx, xi, xq, seg_i64, pseg_i64, len2_i64, len_i64, ri, __ldg(a.rad + j),
-                                   ld_pos<PERSIST>(pin + j), ld_pos<PERSIST>(pin + j + pq_first(pk)),
-                                   ld_pos<PERSIST>(pin + j + pq_second(pk)), fi64, fq64, ei);
+                                   ld_pos<(PERSIST != 0)>(pin + j), ld_pos<(PERSIST != 0)>(pin + j + pq_first(pk)),
+                                   ld_pos<(PERSIST != 0)>(pin + j + pq_second(pk)), fi64, fq64, ei);
             }
           }
         }
@@ -649,7 +651,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         if (s.write_out) s.energy[v] = evtx;
         if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
           st->rebuild = 1;
-          if constexpr (PERSIST) atomicOr(pflag, 1);
+          if constexpr (PERSIST == 1) atomicOr(pflag, 1);
           if constexpr (BATCH) s.bsys[sysid].rebuild = 1;
         }
       } else {
@@ -672,7 +674,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
           s.vel[v] = vh2;
           if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
             st->rebuild = 1;
-            if constexpr (PERSIST) atomicOr(pflag, 1);
+            if constexpr (PERSIST == 1) atomicOr(pflag, 1);
             if constexpr (BATCH) s.bsys[sysid].rebuild = 1;
           }
         } else {
@@ -682,11 +684,13 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         }
       }
       if (s.accumulate) {
+        // products and sums rounded as written, so every kernel built on
+        // this body (one op per launch, multi-step, persistent FIRE) sums alike
         sums[S_PE] = evtx + ((INTER == INT_SMOOTH) ? epair : 0.0);
-        sums[S_VV] = vn.x * vn.x + vn.y * vn.y;
-        sums[S_VF] = vn.x * F.x + vn.y * F.y;
-        sums[S_FF] = F.x * F.x + F.y * F.y;
-        sums[S_FMAX2] = fmax(F.x * F.x, F.y * F.y);
+        sums[S_VV] = __fma_rn(vn.y, vn.y, __dmul_rn(vn.x, vn.x));
+        sums[S_VF] = __fma_rn(vn.y, F.y, __dmul_rn(vn.x, F.x));
+        sums[S_FF] = __fma_rn(F.y, F.y, __dmul_rn(F.x, F.x));
+        sums[S_FMAX2] = fmax(__dmul_rn(F.x, F.x), __dmul_rn(F.y, F.y));
       }
       if (!(isfinite(F.x) && isfinite(F.y))) {
         sums[S_NONFINITE] = 1.0;
@@ -707,14 +711,14 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
       // per-CTA partials in a fixed order, compensated
       block_partials<BLOCK>(sums, s_red, s.partials + (size_t)blockIdx.x * NSUM);
     } else if (__syncthreads_or(nonfinite) && t == 0) {
-      if constexpr (PERSIST) {
+      if constexpr (PERSIST == 1) {
         atomicOr(pflag, 2);
       } else {
         st->nonfinite = 1;
         st->abort = 1;
       }
     }
-    if constexpr (PERSIST) return;
+    if constexpr (PERSIST == 1) return;
     if constexpr (BATCH) {
       if (s.accumulate) {
         // the system's last tile reduces the system's partials
@@ -786,7 +790,7 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
     }
     return;
   }
-  tile_body<POT, INTER, MODE, BLOCK, L, PREC, BATCH, false>(p, a, s, a.pos, s.pos_out,
+  tile_body<POT, INTER, MODE, BLOCK, L, PREC, BATCH, 0>(p, a, s, a.pos, s.pos_out,
                                                            (unsigned long long)st->rng_step, nullptr);
 }
 
@@ -873,7 +877,7 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
     if (blockIdx.x == 0 && threadIdx.x == 0) st->pflag[(base + j + 1) % 3] = 0;
     const double2* pin = (j & 1) ? pos1 : pos0;
     double2* pout = (j & 1) ? pos0 : pos1;
-    tile_body<POT, INTER, MODE_STEP, BLOCK, L, PREC, false, true>(p, a, s, pin, pout, step0 + (unsigned long long)j,
+    tile_body<POT, INTER, MODE_STEP, BLOCK, L, PREC, false, 1>(p, a, s, pin, pout, step0 + (unsigned long long)j,
                                                                  slot);
     done = j + 1;
     if (!steps_barrier(st)) {

@@ -515,6 +515,13 @@ int cr_batch_compress(cr_batch* b, const cr_compress_params* params, double* phi
 int cr_batch_compress_stepwise(cr_batch* b, const cr_compress_params* params, double* phi, long* steps, int* state,
                                long* fireIterations);
 int cr_batch_get_launch_count(const cr_batch* b, long long* out);
+/* No reference counterpart.  1 (default): FIRE iterations of batches whose
+ * tiles the GPU holds at once run in a persistent kernel (FP64; tile shapes
+ * (1, 128) and (2, 192)), up to 64 iterations per launch with grid barriers
+ * in place of kernel boundaries, the same iterates as one launch per op; 0:
+ * one launch per op.  A grid-barrier wait that gives up (cr_set_spin_limit
+ * semantics, batch status) switches the batch to one launch per op. */
+int cr_batch_set_persistent(cr_batch* b, int on);
 /* Entries per vertex the batch's neighbour lists hold (grown on overflow). */
 int cr_batch_get_list_capacity(const cr_batch* b, int* out);
 

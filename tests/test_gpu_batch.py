@@ -108,6 +108,50 @@ def test_batch_fire_matches_single(cuda_device):
         d.close()
 
 
+@pytest.mark.parametrize("workload,potential,interaction,lanes", [
+    ("bidisperse_harmonic", "harmonic", "vertexVertex", 1), ("smooth_lj", "lennardJones", "vertexSmooth", 2)])
+def test_batch_fire_persistent_matches_one_launch_per_op(cuda_device, workload, potential, interaction, lanes):
+    # the persistent kernel (up to 64 iterations per launch, grid barriers,
+    # rebuilds between launches) against one launch per op: the same ops in
+    # the same order, so the same iterates bit for bit
+    pks = _systems(workload, [16, 32, 20], 0.40 if workload == "smooth_lj" else 0.70, seed=7,
+                   placement="rsa" if workload == "smooth_lj" else "uniform")
+    kw = dict(potential=potential, interaction=interaction, ea=1.0, el=1.0, eb=0.01, ec=1.0, LJcutoff=2.5)
+    out = []
+    for persistent in (False, True):
+        b = Batch.from_packings(pks, **kw)
+        b.setLanes(lanes)
+        b.setPersistent(persistent)
+        b.setDisplacementCutoff(0.5)
+        sig = b.getMeanParticleSizes()
+        b.initFIRE([0.2, 0.5, 1.1, 0.99, 1e-3, 1e-2, 0.2], 20, dt=1e-3 * sig)
+        n0 = b.getLaunchCount()
+        its, fmax = b.fireMinimize(1e-10 / sig, 3000)
+        out.append((its, fmax, b.getVertexPositions(), b.getVertexVelocities(), b.getLaunchCount() - n0))
+    (i2, f2, x2, v2, l2), (i1, f1, x1, v1, l1) = out
+    assert np.array_equal(i1, i2) and np.array_equal(f1, f2)
+    assert np.array_equal(x1, x2) and np.array_equal(v1, v2)
+    assert i1.max() > 200
+    assert l1 * 10 < l2  # the persistent kernel ran (a few launches per 64 iterations)
+
+
+def test_batch_compress_persistent_matches_one_launch_per_op(cuda_device):
+    pks = batch_packings(4, seed=11, rings=(16, 40))
+    kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
+    prm = dict(dphi=2e-2, min_dphi=2e-3, fire_dt=1e-2, tol0=1e-6, max_fire_iters=400, max_steps=6)
+    out = []
+    for persistent in (True, False):
+        b = Batch.from_packings(pks, **kw)
+        b.setPersistent(persistent)
+        b.setDisplacementCutoff(0.5)
+        res = b.compress(**prm)
+        out.append((res, b.getVertexPositions()))
+    (r1, x1), (r2, x2) = out
+    for k in ("phi", "steps", "state", "fire_iterations"):
+        assert np.array_equal(r1[k], r2[k]), k
+    assert np.array_equal(x1, x2)
+
+
 def test_batch_scale_matches_single(cuda_device):
     pks = _systems("bidisperse_harmonic", [16, 24], 0.40, seed=3)
     kw = dict(potential="harmonic", interaction="vertexVertex", ea=1.0, el=1.0, eb=0.01, ec=1.0)
