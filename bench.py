@@ -77,6 +77,8 @@ def parse(argv=None):
     ap.add_argument("--scale-tiles", type=int, default=8, help="scale-up: k x k copies of the packing")
     ap.add_argument("--scale-steps", type=int, default=200, help="scale-up: MD steps per timed repetition")
     ap.add_argument("--save-state", default=None, help="write the prepared state (npz) after preparation")
+    ap.add_argument("--jam-systems", type=int, default=8,
+                    help="systems of the compression-to-jamming measurement (each also runs through its own context)")
     ap.add_argument("--profile-kernel", action="store_true",
                     help="only time the fused step kernel (few launches; for ncu captures)")
     ap.add_argument("--profile-build", action="store_true",
@@ -572,7 +574,7 @@ def main():
         scale = scale_up_measurement(d, c, args, world, peaks)
 
     batch = None if args.no_batch else batched_fire_measurement(args.batch_systems, world, rank)
-    jam = None if (args.no_batch or rank != 0) else jamming_measurement()
+    jam = None if (args.no_batch or rank != 0) else jamming_measurement(args.jam_systems)
 
     rigid = None
     if rank == 0 and not args.no_rigid:
