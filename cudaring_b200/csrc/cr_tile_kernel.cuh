@@ -205,8 +205,11 @@ __device__ __forceinline__ void smooth_slot_f64(const SysParams& p, const B& bx,
 template <int POT, int INTER, int MODE, int BLOCK, int L, int PREC, bool BATCH, int PERSIST>
 __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a, const StepArgs& s,
                                           const double2* __restrict__ pin, double2* __restrict__ pout,
-                                          unsigned long long step, int* pflag) {
+                                          unsigned long long step, int* pflag, bool reuse = false) {
   constexpr int TV = BLOCK / L;
+  // the multi-step kernel stores no energies and no sums (its ops run with
+  // write_out = accumulate = 0), so its energy terms are left out at compile time
+  constexpr bool kOut = PERSIST != 1;
   constexpr int TS = (MODE == MODE_STEP) ? TV : 1;
   __shared__ double2 s_pos[TV];
   __shared__ double2 s_seg[TV];     // pbc(pos[next] - pos[v])
@@ -223,6 +226,8 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
   __shared__ double2 s_fsh[TV];     // shape force on v, parked across the pair phase
   __shared__ double s_esh[TV];      // shape energy booked on v
   __shared__ int s_lp[TV];
+  __shared__ int2 s_tp[TV];         // topology word (ring, k | nv << 16)
+  __shared__ double s_a0[TV];       // rest area of the vertex's ring
   __shared__ __align__(16) double2 s_vel[TS];
   __shared__ __align__(16) double2 s_last[TS];
   __shared__ double s_red[BLOCK / 32][NSUM];
@@ -249,17 +254,32 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
   double a0r = 1.0;
   if (t < nvt) {
     const int v = v0 + t;
-    if constexpr (MODE == MODE_STEP) {
-      cp_async16(&s_vel[t], s.vel + v);
-      cp_async16(&s_last[t], s.last_pos + v);
-      cp_async_commit();
+    int2 tp;
+    if (PERSIST == 1 && reuse) {
+      // a later step of the multi-step kernel: the CTA holds the same tile,
+      // so its topology, rest lengths and angles, last-build positions and its
+      // own positions and velocities (stored by the last step's tail) are
+      // still in shared memory
+      tp = s_tp[t];
+      a0r = s_a0[t];
+    } else {
+      if constexpr (MODE == MODE_STEP) {
+        cp_async16(&s_vel[t], s.vel + v);
+        cp_async16(&s_last[t], s.last_pos + v);
+        cp_async_commit();
+      }
+      tp = __ldg(a.vtopo + v);
+      s_pos[t] = ld_pos<(PERSIST != 0)>(pin + v);
+      const double l0v = __ldg(a.l0 + v);
+      s_l0[t] = l0v;
+      s_il0[t] = 1.0 / l0v;
+      s_th0[t] = __ldg(a.theta0 + v);
+      a0r = __ldg(a.a0 + tp.x);
+      if constexpr (PERSIST == 1) {
+        s_tp[t] = tp;
+        s_a0[t] = a0r;
+      }
     }
-    const int2 tp = __ldg(a.vtopo + v);
-    s_pos[t] = ld_pos<(PERSIST != 0)>(pin + v);
-    const double l0v = __ldg(a.l0 + v);
-    s_l0[t] = l0v;
-    s_il0[t] = 1.0 / l0v;
-    s_th0[t] = __ldg(a.theta0 + v);
     ring = tp.x;
     k = tp.y & 0xffff;
     nvr = tp.y >> 16;
@@ -267,7 +287,6 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
     ln = lf + (k + 1 == nvr ? 0 : k + 1);
     lp = lf + (k == 0 ? nvr - 1 : k - 1);
     s_lp[t] = lp;
-    a0r = __ldg(a.a0 + ring);
   }
   __syncthreads();
 
@@ -648,7 +667,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         pout[v] = xn;
         s.vel[v] = vn;
         s.force[v] = F;
-        if (s.write_out) s.energy[v] = evtx;
+        if (kOut && s.write_out) s.energy[v] = evtx;
         if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
           st->rebuild = 1;
           if constexpr (PERSIST == 1) atomicOr(pflag, 1);
@@ -672,6 +691,12 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
           }
           pout[v] = xn;
           s.vel[v] = vh2;
+          if constexpr (PERSIST == 1) {
+            // kept for the next step of the multi-step kernel (this thread
+            // alone reads its slots until the barrier between steps)
+            s_pos[t] = xn;
+            s_vel[t] = vh2;
+          }
           if (3.0 * dist_of(pbc2(bx, xn, xl)) > dcut) {
             st->rebuild = 1;
             if constexpr (PERSIST == 1) atomicOr(pflag, 1);
@@ -680,10 +705,10 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         } else {
           s.vel[v] = vn;
           s.force[v] = F;
-          if (s.write_out) s.energy[v] = evtx;
+          if (kOut && s.write_out) s.energy[v] = evtx;
         }
       }
-      if (s.accumulate) {
+      if (kOut && s.accumulate) {
         // products and sums rounded as written, so every kernel built on
         // this body (one op per launch, multi-step, persistent FIRE) sums alike
         sums[S_PE] = evtx + ((INTER == INT_SMOOTH) ? epair : 0.0);
@@ -697,7 +722,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         nonfinite = 1;
       }
     }
-    if (s.write_out && INTER == INT_SMOOTH) {
+    if (kOut && s.write_out && INTER == INT_SMOOTH) {
       __syncthreads();
       if (t < nvt) s_r1[t] = epair;
       for (int stride = 1; stride < TV; stride <<= 1) {
@@ -707,7 +732,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
       __syncthreads();
       if (t < nvt && k == 0) s.p_energy[ring] = s_r1[t];
     }
-    if (s.accumulate) {
+    if (kOut && s.accumulate) {
       // per-CTA partials in a fixed order, compensated
       block_partials<BLOCK>(sums, s_red, s.partials + (size_t)blockIdx.x * NSUM);
     } else if (__syncthreads_or(nonfinite) && t == 0) {
@@ -720,7 +745,7 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
     }
     if constexpr (PERSIST == 1) return;
     if constexpr (BATCH) {
-      if (s.accumulate) {
+      if (kOut && s.accumulate) {
         // the system's last tile reduces the system's partials
         BatchSys& bs = s.bsys[sysid];
         __syncthreads();
@@ -749,11 +774,11 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
       }
     }
     if (is_last_block(st)) {
-      if (!BATCH && s.accumulate) reduce_partials(s.partials, gridDim.x, st->sums);
+      if (!BATCH && kOut && s.accumulate) reduce_partials(s.partials, gridDim.x, st->sums);
       __syncthreads();
       if (t == 0) {
         __threadfence();
-        if (!BATCH && s.accumulate && st->sums[S_NONFINITE] != 0.0) {
+        if (!BATCH && kOut && s.accumulate && st->sums[S_NONFINITE] != 0.0) {
           st->nonfinite = 1;
           st->abort = 1;
         }
@@ -878,7 +903,7 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
     const double2* pin = (j & 1) ? pos1 : pos0;
     double2* pout = (j & 1) ? pos0 : pos1;
     tile_body<POT, INTER, MODE_STEP, BLOCK, L, PREC, false, 1>(p, a, s, pin, pout, step0 + (unsigned long long)j,
-                                                                 slot);
+                                                                 slot, j > 0);
     done = j + 1;
     if (!steps_barrier(st)) {
       stalled = true;
