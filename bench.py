@@ -77,6 +77,9 @@ def parse(argv=None):
     ap.add_argument("--scale-tiles", type=int, default=8, help="scale-up: k x k copies of the packing")
     ap.add_argument("--scale-steps", type=int, default=200, help="scale-up: MD steps per timed repetition")
     ap.add_argument("--save-state", default=None, help="write the prepared state (npz) after preparation")
+    ap.add_argument("--profile-jam", action="store_true",
+                    help="only the device compression of the jamming measurement, inside a profiler range "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--jam-systems", type=int, default=8,
                     help="systems of the compression-to-jamming measurement (each also runs through its own context)")
     ap.add_argument("--profile-kernel", action="store_true",
@@ -349,6 +352,9 @@ def main():
     world, rank, local = dist_setup()
     if world != args.gpus:
         raise SystemExit(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}")
+    if args.profile_jam:
+        print(json.dumps(jamming_measurement(args.jam_systems, profile_only=True)), flush=True)
+        return 0
     if args.plan_only:
         init_group(world)
         print_plan(args, world, rank)
@@ -495,8 +501,8 @@ def main():
             d.setVertexPositions(hpos)
             d.setVertexVelocities(hvel)
             d.NVELoop(M)
-            hpos[:] = d.getVertexPositions()
-            hvel[:] = d.getVertexVelocities()
+            d.getVertexPositions(out=hpos)
+            d.getVertexVelocities(out=hvel)
             _ = d.getPotentialEnergy()
         eb.record(stream)
         torch.cuda.synchronize()
@@ -761,7 +767,7 @@ def batched_fire_measurement(num_systems: int, world: int, rank: int, fire_iters
     return out
 
 
-def jamming_measurement(num_systems: int = 8) -> dict:
+def jamming_measurement(num_systems: int = 8, profile_only: bool = False) -> dict:
     """Compression to jamming of a small batch, three ways: the protocol as
     one graph launch on the device (cr_batch_compress), the same protocol
     driven from the host between steps and FIRE chunks
@@ -783,6 +789,17 @@ def jamming_measurement(num_systems: int = 8) -> dict:
     out = {"workload": f"{num_systems} systems, rings U[16,32] nv 16/22, harmonic, from phi 0.70: dphi 0.02 halved "
                        "on overshoot down to 0.002, FIRE to 1e-6/sigma, at most 40 steps",
            "vertices": int(sum(p.num_vertices for p in pks))}
+    if profile_only:
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        t0 = time.perf_counter()
+        r = b.compress(**prm)
+        torch.cuda.synchronize()
+        out["device"] = {"seconds": time.perf_counter() - t0, "fire_iterations": int(r["fire_iterations"].sum()),
+                         "launches": b.getLaunchCount()}
+        torch.cuda.profiler.stop()
+        b.close()
+        return out
     res = {}
     for mode in ("device", "stepwise"):
         b.setVertexPositions(pos)

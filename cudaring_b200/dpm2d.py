@@ -70,8 +70,13 @@ class DPM2D:
             msg = self._L.cr_last_error(self._h)
             raise CudaRingError(name, rc, msg.decode() if msg else "")
 
-    def _get(self, name, n, dtype=np.float64):
-        out = np.empty(n, dtype=dtype)
+    def _get(self, name, n, dtype=np.float64, out=None):
+        """Download into a new array, or into `out` (n contiguous elements of
+        dtype, e.g. a pinned buffer: the copy then needs no staging)."""
+        if out is None:
+            out = np.empty(n, dtype=dtype)
+        elif out.dtype != dtype or out.size != n or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a contiguous {np.dtype(dtype).name} array of {n} elements")
         self._call(name, out.ctypes.data)
         return out
 
@@ -123,11 +128,12 @@ class DPM2D:
 
     # ----------------------------------------------------------------- state
     def setVertexPositions(self, a): self._call("cr_set_vertex_positions", _f64(a).ctypes.data)
-    def getVertexPositions(self): return self._get("cr_get_vertex_positions", 2 * self.numVertices)
+    def getVertexPositions(self, out=None): return self._get("cr_get_vertex_positions", 2 * self.numVertices, out=out)
     def setVertexVelocities(self, a): self._call("cr_set_vertex_velocities", _f64(a).ctypes.data)
-    def getVertexVelocities(self): return self._get("cr_get_vertex_velocities", 2 * self.numVertices)
+    def getVertexVelocities(self, out=None):
+        return self._get("cr_get_vertex_velocities", 2 * self.numVertices, out=out)
     def setVertexForces(self, a): self._call("cr_set_vertex_forces", _f64(a).ctypes.data)
-    def getVertexForces(self): return self._get("cr_get_vertex_forces", 2 * self.numVertices)
+    def getVertexForces(self, out=None): return self._get("cr_get_vertex_forces", 2 * self.numVertices, out=out)
     def getVertexEnergies(self): return self._get("cr_get_vertex_energies", self.numVertices)
     def getParticleEnergies(self): return self._get("cr_get_particle_energies", self.numParticles)
     def setVertexRadii(self, a): self._call("cr_set_vertex_radii", _f64(a).ctypes.data)

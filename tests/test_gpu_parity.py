@@ -286,3 +286,19 @@ def test_force_is_minus_gradient(cuda_device):
             e.append(d.getPotentialEnergy())
         fd = -(e[0] - e[1]) / (2 * h)
         assert fd == pytest.approx(f[idx], rel=1e-5, abs=1e-6 * max(1.0, np.abs(f).max()))
+
+
+def test_getters_write_into_given_arrays(cuda_device):
+    # out= downloads into the caller's array (a pinned buffer needs no staging)
+    c = synth.workload_config("smooth_lj", 8)
+    pk = synth.make_packing(c["nv"], c["a0"], c["calA0"], 0.40, seed=5, placement="rsa")
+    d = DPM2D.from_packing(pk, **{k: c[k] for k in ("potential", "interaction", "ea", "el", "eb", "ec", "LJcutoff")})
+    d.calcNeighborList(d.setDisplacementCutoff(0.5, 2.0 * d.getMeanVertexRadius()))
+    d.calcForceEnergy()
+    for get in (d.getVertexPositions, d.getVertexVelocities, d.getVertexForces):
+        ref = get()
+        buf = np.full_like(ref, np.nan)
+        assert get(out=buf) is buf and np.array_equal(buf, ref)
+        with pytest.raises(ValueError):
+            get(out=np.empty(ref.size - 1))
+    d.close()
