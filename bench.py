@@ -801,18 +801,20 @@ def jamming_measurement(num_systems: int = 8, profile_only: bool = False) -> dic
         b.close()
         return out
     res = {}
-    for mode in ("device", "stepwise"):
+    for mode in ("device", "stepwise", "one_launch_per_op"):
         b.setVertexPositions(pos)
         b.setVertexVelocities(np.zeros_like(pos))
         b.setVertexRadii(rad)
         b.setRestLengths(l0)
         b.setRestAreas(a0)
+        b.setPersistent(mode != "one_launch_per_op")
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         r = b.compress(stepwise=mode == "stepwise", **prm)
         torch.cuda.synchronize()
         res[mode] = (time.perf_counter() - t0, r)
     b.close()
+    t_op, r_op = res["one_launch_per_op"]
     t_dev, r_dev = res["device"]
     t_host, r_host = res["stepwise"]
     same = all(np.array_equal(r_dev[k], r_host[k]) for k in ("phi", "steps", "state", "fire_iterations"))
@@ -820,6 +822,10 @@ def jamming_measurement(num_systems: int = 8, profile_only: bool = False) -> dic
                      "steps": [int(x) for x in r_dev["steps"]], "state": [int(x) for x in r_dev["state"]],
                      "fire_iterations": int(r_dev["fire_iterations"].sum())}
     out["stepwise"] = {"seconds": t_host, "same_states_as_device": bool(same)}
+    out["device_one_launch_per_op"] = {
+        "seconds": t_op, "note": "the same graph with the persistent FIRE kernel off",
+        "same_states_as_device": bool(all(np.array_equal(r_dev[k], r_op[k])
+                                          for k in ("phi", "steps", "state", "fire_iterations")))}
     # every system through its own context, from the same prepared state
     vo = np.cumsum([0] + [p.num_vertices for p in pks])
     ro = np.cumsum([0] + [p.num_particles for p in pks])
@@ -839,6 +845,7 @@ def jamming_measurement(num_systems: int = 8, profile_only: bool = False) -> dic
                               "note": "the FIRE sums reduce in another order, so decisions at the 2 tol margin can "
                                       "flip and the paths to jamming part"}
     out["device_over_stepwise"] = t_host / t_dev
+    out["persistent_speedup"] = t_op / t_dev
     out["device_over_loop"] = t_loop / t_dev
     return out
 
