@@ -60,3 +60,30 @@ def test_reference_arm_runs_without_the_product_library():
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["config"]["state"] == "bench_state/smooth_lj_1024.npz"
     assert line["config"]["workload"].startswith("1024 deformable rings")
+
+
+def test_clock_sampler_keeps_only_samples_of_the_timed_region(tmp_path, monkeypatch):
+    # a stand-in nvidia-smi: one idle-clock line at start-up, then load clocks
+    # every interval, the power cap active on the third of them
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/usr/bin/env python3\n"
+                    "import sys, time\n"
+                    "print('0, 345, 1965, 80.0, 0x0, Not Active, Not Active, Not Active, Not Active', flush=True)\n"
+                    "k = 0\n"
+                    "while True:\n"
+                    "    time.sleep(0.05)\n"
+                    "    k += 1\n"
+                    "    cap = 'Active' if k == 3 else 'Not Active'\n"
+                    "    print(f'0, 1965, 1965, 900.0, 0x4, Not Active, Not Active, Not Active, {cap}', flush=True)\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}{os.pathsep}{os.environ['PATH']}")
+    monkeypatch.syspath_prepend(ROOT)
+    import importlib
+    import time
+    bench = importlib.import_module("bench")
+    with bench.ClockSampler(0) as cs:
+        time.sleep(0.6)
+    out = cs.summary()
+    assert out["samples"] >= 3
+    assert out["sm_mhz"] == 1965.0 and out["sm_max_mhz"] == 1965.0  # the idle start-up sample is left out
+    assert out["reasons"] == ["sw_power_cap"]
