@@ -222,7 +222,7 @@ struct DevStatus {
   // multi-step kernel (k_tile_steps): barrier arrivals, the rotation base of
   // its three per-step flag slots (bit 1: a rebuild is due, bit 2: a
   // non-finite force), and the middle steps of the sequence still to run
-  unsigned int pbar;
+  unsigned long long pbar;
   int pflag[3];
   long long pbase;
   long long steps_left;

@@ -840,29 +840,33 @@ __global__ void __launch_bounds__(BLOCK, tile_threads_per_sm<PREC, L>() / BLOCK)
 // Every barrier wait is bounded: a CTA that gives up sets stalled and abort
 // and leaves; the others see stalled and leave too.
 
-__device__ __forceinline__ unsigned int pst_ld_acquire(const unsigned int* a) {
-  unsigned int v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+__device__ __forceinline__ unsigned long long pst_ld_acquire(const unsigned long long* a) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
   return v;
 }
 
-__device__ __forceinline__ unsigned int pst_atom_add_release(unsigned int* a, unsigned int x) {
-  unsigned int old;
-  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(a), "r"(x) : "memory");
+// Arrival: acquire-release, so the arrival that completes a barrier has
+// already synchronised with every earlier arrival and needs no poll.
+__device__ __forceinline__ unsigned long long pst_atom_add_acq_rel(unsigned long long* a, unsigned long long x) {
+  unsigned long long old;
+  asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(a), "l"(x) : "memory");
   return old;
 }
 
-// Barrier over the grid on status.pbar (a multiple of gridDim.x at launch).
+// Barrier over the grid on status.pbar (a multiple of gridDim.x at launch; a
+// 64-bit count, so a sequence of any length never wraps it).
 __device__ __forceinline__ bool steps_barrier(DevStatus* st) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned int prev = pst_atom_add_release(&st->pbar, 1u);
-    const unsigned int target = (prev / gridDim.x + 1u) * gridDim.x;
+    const unsigned long long g = gridDim.x;
+    const unsigned long long prev = pst_atom_add_acq_rel(&st->pbar, 1ull);
+    const unsigned long long target = (prev / g + 1ull) * g;
     const long long lim = barrier_poll_limit(st);
     long long it = 0;
-    while (pst_ld_acquire(&st->pbar) < target) {
+    while (prev + 1ull < target && pst_ld_acquire(&st->pbar) < target) {
       if (++it > lim || *(volatile int*)&st->stalled) {
         ok = 0;
         break;
