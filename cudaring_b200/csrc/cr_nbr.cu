@@ -736,30 +736,28 @@ __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* a) {
   return v;
 }
 
-__device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int* a, unsigned int x) {
+__device__ __forceinline__ unsigned int atom_add_release_u32(unsigned int* a, unsigned int x) {
   unsigned int old;
-  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(a), "r"(x) : "memory");
+  asm volatile("atom.add.release.gpu.global.u32 %0, [%1], %2;" : "=r"(old) : "l"(a), "r"(x) : "memory");
   return old;
 }
 
 // Grid barrier on one counter: bar_count is zero when the build starts (the
 // publishing CTA clears it after every CTA has passed the last barrier), and
-// barrier i completes when it reaches i * gridDim.x.  Arrival is an
-// acquire-release add (this CTA's writes, ordered before it by
-// __syncthreads, become visible first); the wait is an acquire load, so what
-// the other CTAs wrote before arriving is visible after it.  The arrival
-// that completes the barrier has synchronised with all the others through
-// the add itself and does not poll.
+// barrier i completes when it reaches i * gridDim.x.  Arrival is a release
+// add (this CTA's writes, ordered before it by __syncthreads, become visible
+// first); the wait is an acquire load, so what the other CTAs wrote before
+// arriving is visible after it.
 __device__ bool grid_barrier(DevStatus* st) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    const unsigned int prev = atom_add_acq_rel_u32(&st->bar_count, 1u);
+    const unsigned int prev = atom_add_release_u32(&st->bar_count, 1u);
     const unsigned int target = (prev / gridDim.x + 1u) * gridDim.x;
     const long long lim = barrier_poll_limit(st);
     long long it = 0;
-    while (prev + 1u < target && ld_acquire_u32(&st->bar_count) < target) {
+    while (ld_acquire_u32(&st->bar_count) < target) {
       if (++it > lim || *(volatile int*)&st->stalled) {
         ok = 0;
         break;

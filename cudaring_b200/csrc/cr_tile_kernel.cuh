@@ -846,11 +846,9 @@ __device__ __forceinline__ unsigned long long pst_ld_acquire(const unsigned long
   return v;
 }
 
-// Arrival: acquire-release, so the arrival that completes a barrier has
-// already synchronised with every earlier arrival and needs no poll.
-__device__ __forceinline__ unsigned long long pst_atom_add_acq_rel(unsigned long long* a, unsigned long long x) {
+__device__ __forceinline__ unsigned long long pst_atom_add_release(unsigned long long* a, unsigned long long x) {
   unsigned long long old;
-  asm volatile("atom.add.acq_rel.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(a), "l"(x) : "memory");
+  asm volatile("atom.add.release.gpu.global.u64 %0, [%1], %2;" : "=l"(old) : "l"(a), "l"(x) : "memory");
   return old;
 }
 
@@ -862,11 +860,11 @@ __device__ __forceinline__ bool steps_barrier(DevStatus* st) {
   if (threadIdx.x == 0) {
     int ok = 1;
     const unsigned long long g = gridDim.x;
-    const unsigned long long prev = pst_atom_add_acq_rel(&st->pbar, 1ull);
+    const unsigned long long prev = pst_atom_add_release(&st->pbar, 1ull);
     const unsigned long long target = (prev / g + 1ull) * g;
     const long long lim = barrier_poll_limit(st);
     long long it = 0;
-    while (prev + 1ull < target && pst_ld_acquire(&st->pbar) < target) {
+    while (pst_ld_acquire(&st->pbar) < target) {
       if (++it > lim || *(volatile int*)&st->stalled) {
         ok = 0;
         break;
