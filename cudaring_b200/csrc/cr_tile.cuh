@@ -348,6 +348,7 @@ __device__ __forceinline__ void smooth_core(const SysParams& p, const B& bx, T2 
   const T proj = (tq.x * seg.x + tq.y * seg.y) * inv_lsq;
   const T pc = tq.x * pseg.x + tq.y * pseg.y;
   const T pl2 = fma(pseg.y, pseg.y, pseg.x * pseg.x);
+  T corner = T(0);  // sign of the corner term at |t - q|: -1, +1 or none
   if (proj >= T(0) && proj < T(1)) {
     T dpx, dpy;
     if constexpr (std::is_same<T, double>::value) {
@@ -379,26 +380,19 @@ __device__ __forceinline__ void smooth_core(const SysParams& p, const B& bx, T2 
       }
       e += (double)ep;
     }
-    if (pc >= -pl2 && pc < T(0)) {
-      // calcVertexVertexInteraction(previousPos, thisPos, ...): delta = q - t
-      T g2, id2, ep2 = T(0);
-      if (pair_eval_t<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != T(0)) {
-        const T s2 = g2 * id2;
-        if constexpr (ROLE1) {
-          ft.x -= s2 * tq.x;
-          ft.y -= s2 * tq.y;
-        } else {
-          fq.x += s2 * tq.x;
-          fq.y += s2 * tq.y;
-        }
-        e -= (double)ep2;
-      }
-    }
+    // calcVertexVertexInteraction(previousPos, thisPos, ...): delta = q - t,
+    // the corner term taken away
+    if (pc >= -pl2 && pc < T(0)) corner = T(-1);
   } else if (proj < T(0) && pc >= T(0)) {
     // calcVertexVertexInteraction(thisPos, previousPos, ...): delta = t - q
+    corner = T(1);
+  }
+  // the two corner cases share one evaluation of the pair term at |t - q|
+  // (a warp whose lanes split between them runs it once), signed by corner
+  if (corner != T(0)) {
     T g2, id2, ep2 = T(0);
     if (pair_eval_t<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != T(0)) {
-      const T s2 = g2 * id2;
+      const T s2 = corner * (g2 * id2);
       if constexpr (ROLE1) {
         ft.x += s2 * tq.x;
         ft.y += s2 * tq.y;
@@ -406,7 +400,7 @@ __device__ __forceinline__ void smooth_core(const SysParams& p, const B& bx, T2 
         fq.x -= s2 * tq.x;
         fq.y -= s2 * tq.y;
       }
-      e += (double)ep2;
+      e += (double)(corner * ep2);
     }
   }
 }
