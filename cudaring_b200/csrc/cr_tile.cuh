@@ -348,59 +348,76 @@ __device__ __forceinline__ void smooth_core(const SysParams& p, const B& bx, T2 
   const T proj = (tq.x * seg.x + tq.y * seg.y) * inv_lsq;
   const T pc = tq.x * pseg.x + tq.y * pseg.y;
   const T pl2 = fma(pseg.y, pseg.y, pseg.x * pseg.x);
-  T corner = T(0);  // sign of the corner term at |t - q|: -1, +1 or none
-  if (proj >= T(0) && proj < T(1)) {
-    T dpx, dpy;
-    if constexpr (std::is_same<T, double>::value) {
-      // FP64: the projection point in box coordinates, as the reference forms
-      // it (pbcDistance(thisPos, previousPos + proj * segment)), so that
-      // near-contact distances carry the same rounding as there
-      const double2 pj = make_double2(qabs.x + proj * seg.x, qabs.y + proj * seg.y);
-      const double2 dpv = pbc2(bx, tabs, pj);
-      dpx = dpv.x;
-      dpy = dpv.y;
-    } else {
-      dpx = fma(-proj, seg.x, tq.x);
-      dpy = fma(-proj, seg.y, tq.y);
+  // One evaluation of the pair term serves the segment term (the foot of the
+  // perpendicular inside the segment) or, before the segment's start, the
+  // corner term at |t - q|: a lane needs at most one of them, so a warp
+  // whose lanes split between the two runs the pair term once.  The corner
+  // term taken away inside the segment's span (concave corners) is the
+  // second, rarer evaluation.
+  const bool on_seg = proj >= T(0) && proj < T(1);
+  const bool before = !on_seg && proj < T(0) && pc >= T(0);
+  if (on_seg || before) {
+    T d2 = tq2;
+    if (on_seg) {
+      T dpx, dpy;
+      if constexpr (std::is_same<T, double>::value) {
+        // FP64: the projection point in box coordinates, as the reference
+        // forms it (pbcDistance(thisPos, previousPos + proj * segment)), so
+        // that near-contact distances carry the same rounding as there
+        const double2 pj = make_double2(qabs.x + proj * seg.x, qabs.y + proj * seg.y);
+        const double2 dpv = pbc2(bx, tabs, pj);
+        dpx = dpv.x;
+        dpy = dpv.y;
+      } else {
+        dpx = fma(-proj, seg.x, tq.x);
+        dpy = fma(-proj, seg.y, tq.y);
+      }
+      d2 = fma(dpy, dpy, dpx * dpx);
     }
     T gm, inv_d, ep = T(0);
-    if (pair_eval_t<POT>(p, fma(dpy, dpy, dpx * dpx), rsum, inv_rsum, gm, inv_d, ep) && gm != T(0)) {
-      const T cross = seg.x * w.y - w.x * seg.y;
-      const T sign = sgn_nan0(cross);
-      const T g = gm * inv_len;
-      if constexpr (ROLE1) {
-        ft.x += g * sign * (-seg.y);
-        ft.y += g * sign * seg.x;
+    if (pair_eval_t<POT>(p, d2, rsum, inv_rsum, gm, inv_d, ep) && gm != T(0)) {
+      if (on_seg) {
+        const T cross = seg.x * w.y - w.x * seg.y;
+        const T sign = sgn_nan0(cross);
+        const T g = gm * inv_len;
+        if constexpr (ROLE1) {
+          ft.x += g * sign * (-seg.y);
+          ft.y += g * sign * seg.x;
+        } else {
+          const T a = fabs(cross) * inv_lsq;
+          fo.x += g * (sign * tq.y - a * seg.x);
+          fo.y += g * (-sign * tq.x - a * seg.y);
+          fq.x += g * (-sign * w.y + a * seg.x);
+          fq.y += g * (sign * w.x + a * seg.y);
+        }
       } else {
-        const T a = fabs(cross) * inv_lsq;
-        fo.x += g * (sign * tq.y - a * seg.x);
-        fo.y += g * (-sign * tq.x - a * seg.y);
-        fq.x += g * (-sign * w.y + a * seg.x);
-        fq.y += g * (sign * w.x + a * seg.y);
+        // calcVertexVertexInteraction(thisPos, previousPos, ...): delta = t - q
+        const T s2 = gm * inv_d;
+        if constexpr (ROLE1) {
+          ft.x += s2 * tq.x;
+          ft.y += s2 * tq.y;
+        } else {
+          fq.x -= s2 * tq.x;
+          fq.y -= s2 * tq.y;
+        }
       }
       e += (double)ep;
     }
+  }
+  if (on_seg && pc >= -pl2 && pc < T(0)) {
     // calcVertexVertexInteraction(previousPos, thisPos, ...): delta = q - t,
     // the corner term taken away
-    if (pc >= -pl2 && pc < T(0)) corner = T(-1);
-  } else if (proj < T(0) && pc >= T(0)) {
-    // calcVertexVertexInteraction(thisPos, previousPos, ...): delta = t - q
-    corner = T(1);
-  }
-  // the two corner cases share one evaluation of the pair term at |t - q|
-  // (a warp whose lanes split between them runs it once), signed by corner
-  if (corner != T(0)) {
     T g2, id2, ep2 = T(0);
     if (pair_eval_t<POT>(p, tq2, rsum, inv_rsum, g2, id2, ep2) && g2 != T(0)) {
-      const T s2 = corner * (g2 * id2);
+      const T s2 = g2 * id2;
       if constexpr (ROLE1) {
-        ft.x += s2 * tq.x;
-        ft.y += s2 * tq.y;
+        ft.x -= s2 * tq.x;
+        ft.y -= s2 * tq.y;
       } else {
-        fq.x -= s2 * tq.x;
-        fq.y -= s2 * tq.y;
+        fq.x += s2 * tq.x;
+        fq.y += s2 * tq.y;
       }
-      e += (double)(corner * ep2);
+      e -= (double)ep2;
     }
   }
 }
