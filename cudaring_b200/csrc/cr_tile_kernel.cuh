@@ -162,6 +162,48 @@ __device__ __forceinline__ bool mixed_slot_f32(const SysParams& p, const B& bx, 
   return false;
 }
 
+// Single-precision test of one smooth unit (tq = t - q, seg = o - q, pseg =
+// q - qq, Rm2 = (range * radSum)^2 with a margin): false only when the unit
+// adds nothing.  A unit contributes only through its segment term (foot of
+// the perpendicular inside the segment, a = tq . seg in [0, |seg|^2), its
+// distance within range), its convex-corner term (a < 0 and tq . pseg >= 0,
+// |tq| within range) or its concave-corner correction (inside the segment's
+// span with |tq| within range, so within the first test).  The margins (1e-3
+// of the scale of each dot product, 1e-4 |tq|^2 and 1% of the squared range)
+// are far above the rounding of offsets formed in FP64 and rounded once.
+__device__ __forceinline__ bool unit_may_contribute(float2 tq, float2 seg, float2 pseg, float Rm2) {
+  const float t2 = fmaf(tq.y, tq.y, tq.x * tq.x);
+  const float l2 = fmaf(seg.y, seg.y, seg.x * seg.x);
+  const float a = fmaf(tq.y, seg.y, tq.x * seg.x);
+  const float ma = 1e-3f * (t2 + l2);
+  const float slack = fmaf(1e-4f, t2, Rm2);
+  if (a >= -ma && a < l2 + ma && t2 * l2 - a * a < slack * l2) return true;
+  if (a < ma && t2 < slack) {
+    const float b = fmaf(tq.y, pseg.y, tq.x * pseg.x);
+    const float pl2 = fmaf(pseg.y, pseg.y, pseg.x * pseg.x);
+    if (b >= -1e-3f * (t2 + pl2)) return true;
+  }
+  return false;
+}
+
+// Whether either smooth unit of a slot (vertex i against neighbour j) may
+// contribute: offsets formed in FP64 as the mixed path forms them, rounded
+// once, then the single-precision unit test.  seg_i64 = x_i - x_q.
+template <int POT, class B>
+__device__ __forceinline__ bool slot_may_contribute(const SysParams& p, const B& bx, double2 xi, double2 seg_i64,
+                                                    float2 seg_i, float2 pseg_i, double ri, double rj, double2 xj,
+                                                    double2 xjq, double2 xjqq) {
+  const float R = pot_range_f<POT>(p) * (float)(ri + rj);
+  const float Rm2 = 1.01f * R * R;
+  const double2 w64 = pbc2(bx, xi, xj);    // x_i - x_j
+  const double2 tq64 = pbc2(bx, xi, xjq);  // x_i - x_jq
+  double2 seg1_64 = make_double2(tq64.x - w64.x, tq64.y - w64.y);  // x_j - x_jq
+  if (fabs(seg1_64.x) > 0.25 * bx.lx || fabs(seg1_64.y) > 0.25 * bx.ly) seg1_64 = pbc2(bx, xj, xjq);
+  if (unit_may_contribute(f2(tq64), f2(seg1_64), f2(pbc2(bx, xjq, xjqq)), Rm2)) return true;
+  const float2 tq2 = f2(make_double2(seg_i64.x - w64.x, seg_i64.y - w64.y));  // x_j - x_q
+  return unit_may_contribute(tq2, seg_i, pseg_i, Rm2);
+}
+
 // FP64 body of one slot, shared by the FP64 path and the mixed path's
 // near-contact slots: the reference's own differences of box coordinates
 // (pbcDistance of each pair of vertices) and the FP64 skip tests.
@@ -429,29 +471,60 @@ __device__ __forceinline__ void tile_body(const SysParams& p, const SysArrays& a
         const double2 pseg_i64 = s_seg[s_lp[lq]];  // x_q - x_qq
         const double len2_i = fma(seg_i64.y, seg_i64.y, seg_i64.x * seg_i64.x);
         const float len_i = sqrtf((float)len2_i);
-        double2 nxj = make_double2(0.0, 0.0), nxjq = nxj, nxjqq = nxj;
-        double nr = 0.0;
-        if (sl < cnt) {
-          nxj = ld_pos<(PERSIST != 0)>(pin + jn);
-          nxjq = ld_pos<(PERSIST != 0)>(pin + jn + pq_first(pkn));
-          nxjqq = ld_pos<(PERSIST != 0)>(pin + jn + pq_second(pkn));
-          nr = __ldg(a.rad + jn);
-        }
-        while (sl < cnt) {
-          const double2 xj = nxj, xjq = nxjq, xjqq = nxjqq;
-          const double rj = nr;
-          sl += L;
-          if (sl < cnt) {
-            nxj = ld_pos<(PERSIST != 0)>(pin + j2);
-            nxjq = ld_pos<(PERSIST != 0)>(pin + j2 + pq_first(pk2));
-            nxjqq = ld_pos<(PERSIST != 0)>(pin + j2 + pq_second(pk2));
-            nr = __ldg(a.rad + j2);
-            if (sl + L < cnt) {
-              j2 = __ldg(a.nbr + (size_t)(sl + L) * stride + i);
-              pk2 = __ldg(a.nbr_pq + (size_t)(sl + L) * stride + i);
-            }
+        const float2 seg_i = f2(seg_i64), pseg_i = f2(pseg_i64);
+        // Most slots add nothing (the foot of the perpendicular past the
+        // segment's end, where the next segment's unit takes over, or out of
+        // range), and a warp issues every slot any of its lanes evaluates.  So
+        // a single-precision pass marks the slots that may contribute (64 lane
+        // slots at a time; a superset, see unit_may_contribute), and only the
+        // marked ones are evaluated in FP64, in slot order: each vertex's sums
+        // are those of evaluating every slot, as an unmarked slot adds nothing.
+        for (int base = lane; base < cnt; base += 64 * L) {
+          const int end = min(cnt, base + 64 * L);
+          unsigned long long need = 0ull;
+          int s0 = base;
+          int j1 = 0, pk1 = 0;
+          const int j0 = __ldg(a.nbr + (size_t)s0 * stride + i), pk0 = __ldg(a.nbr_pq + (size_t)s0 * stride + i);
+          if (s0 + L < end) {
+            j1 = __ldg(a.nbr + (size_t)(s0 + L) * stride + i);
+            pk1 = __ldg(a.nbr_pq + (size_t)(s0 + L) * stride + i);
           }
-          smooth_slot_f64<POT>(p, bx, xi, xq, seg_i64, pseg_i64, len2_i, len_i, ri, rj, xj, xjq, xjqq, fi, fq, ei);
+          double2 xj = ld_pos<(PERSIST != 0)>(pin + j0), xjq = ld_pos<(PERSIST != 0)>(pin + j0 + pq_first(pk0)),
+                  xjqq = ld_pos<(PERSIST != 0)>(pin + j0 + pq_second(pk0));
+          double rj = __ldg(a.rad + j0);
+          while (true) {
+            const int s1 = s0 + L;
+            int jn2 = 0, pkn2 = 0;
+            double2 nxj = xj, nxjq = xjq, nxjqq = xjqq;
+            double nr = rj;
+            if (s1 < end) {
+              if (s1 + L < end) {
+                jn2 = __ldg(a.nbr + (size_t)(s1 + L) * stride + i);
+                pkn2 = __ldg(a.nbr_pq + (size_t)(s1 + L) * stride + i);
+              }
+              nxj = ld_pos<(PERSIST != 0)>(pin + j1);
+              nxjq = ld_pos<(PERSIST != 0)>(pin + j1 + pq_first(pk1));
+              nxjqq = ld_pos<(PERSIST != 0)>(pin + j1 + pq_second(pk1));
+              nr = __ldg(a.rad + j1);
+            }
+            if (slot_may_contribute<POT>(p, bx, xi, seg_i64, seg_i, pseg_i, ri, rj, xj, xjq, xjqq))
+              need |= 1ull << ((s0 - base) / L);
+            if (s1 >= end) break;
+            s0 = s1;
+            xj = nxj;
+            xjq = nxjq;
+            xjqq = nxjqq;
+            rj = nr;
+            j1 = jn2;
+            pk1 = pkn2;
+          }
+          for (; need; need &= need - 1ull) {
+            const int sm = base + (__ffsll((long long)need) - 1) * L;
+            const int j = __ldg(a.nbr + (size_t)sm * stride + i), pk = __ldg(a.nbr_pq + (size_t)sm * stride + i);
+            smooth_slot_f64<POT>(p, bx, xi, xq, seg_i64, pseg_i64, len2_i, len_i, ri, __ldg(a.rad + j),
+                                 ld_pos<(PERSIST != 0)>(pin + j), ld_pos<(PERSIST != 0)>(pin + j + pq_first(pk)),
+                                 ld_pos<(PERSIST != 0)>(pin + j + pq_second(pk)), fi, fq, ei);
+          }
         }
       } else {
         // Smooth units, mixed precision: the lane's slots in FP32, near ones
